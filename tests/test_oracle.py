@@ -1,0 +1,151 @@
+"""The CPU oracle against the fixtures produced by the upstream implementation."""
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle import rgf_oracle as orc
+from quatrex_b200.workloads import make_device
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _blocks_from_dense(dense, sizes, stack):
+    offs = np.hstack(([0], np.cumsum(sizes)))
+    nb = len(sizes)
+    d = [np.broadcast_to(dense[offs[i]:offs[i + 1], offs[i]:offs[i + 1]], (stack, sizes[i], sizes[i])).copy() for i in range(nb)]
+    u = [np.broadcast_to(dense[offs[i]:offs[i + 1], offs[i + 1]:offs[i + 2]], (stack, sizes[i], sizes[i + 1])).copy() for i in range(nb - 1)]
+    lo = [np.broadcast_to(dense[offs[i + 1]:offs[i + 2], offs[i]:offs[i + 1]], (stack, sizes[i + 1], sizes[i])).copy() for i in range(nb - 1)]
+    return d, u, lo
+
+
+@pytest.mark.parametrize("case", ["constant", "mixed"])
+def test_oracle_btd_against_upstream(case):
+    g = np.load(os.path.join(GOLDEN, f"btd_{case}.npz"))
+    sizes = g["block_sizes"]
+    stack = int(g["stack"])
+    offs = np.hstack(([0], np.cumsum(sizes)))
+    mask = g["a"] != 0
+    d, u, lo = _blocks_from_dense(g["a"], sizes, stack)
+    sld, slu, _ = _blocks_from_dense(g["sigma_lesser"], sizes, stack)
+    sgd, sgu, _ = _blocks_from_dense(g["sigma_greater"], sizes, stack)
+    xd, xu, xl_ = orc.selected_inv(d, u, lo, max_batch_size=3)
+    dense = orc.dense_from_blocks(xd, xu, xl_)[0] * mask
+    assert _rel(dense, g["inv"] * mask) < 1e-12
+    res = orc.selected_solve(d, u, lo, sld, slu, sgd, sgu, max_batch_size=3)
+    for key in ("xl", "xg"):
+        got = orc.dense_from_blocks(res[f"{key}_diag"], res[f"{key}_upper"], res[f"{key}_lower"])[0] * mask
+        assert _rel(got, g[key] * mask) < 1e-12
+    ref_r = g["xr"]
+    for i in range(len(sizes)):
+        blk = ref_r[offs[i]:offs[i + 1], offs[i]:offs[i + 1]]
+        m = mask[offs[i]:offs[i + 1], offs[i]:offs[i + 1]]
+        assert _rel(res["xr_diag"][i][0] * m, blk * m) < 1e-12
+    # the reference test criterion: dense inverse / congruence
+    a_inv = np.linalg.inv(g["a"])
+    assert np.allclose(dense, a_inv * mask)
+
+
+def test_oracle_transport_small_against_upstream():
+    g = np.load(os.path.join(GOLDEN, "transport_small.npz"))
+    dev = make_device(num_blocks=4, block_size=8, num_energies=6, seed=7)
+    assert np.array_equal(dev.h_diag, g["h_diag"]) and np.array_equal(dev.h_upper, g["h_upper"])
+    d, u, lo = dev.system_blocks()
+    obc = orc.obc_self_energies(d, u, lo, dev.energies, dev.mu_left, dev.mu_right, dev.kt, dev.sr_tol, dev.sr_max_iter)
+    assert _rel(obc["surface"][0], g["g_surface_left"]) < 1e-12
+    assert _rel(obc["surface"][1], g["g_surface_right"]) < 1e-12
+    for side, k in (("left", 0), ("right", 1)):
+        assert _rel(obc["retarded"][k], g[f"sigma_r_{side}"]) < 1e-12
+        assert _rel(obc["lesser"][k], g[f"sigma_l_{side}"]) < 1e-12
+        assert _rel(obc["greater"][k], g[f"sigma_g_{side}"]) < 1e-12
+    nb = 4
+    obc_r = [obc["retarded"][0], None, None, obc["retarded"][1]]
+    obc_l = [obc["lesser"][0], None, None, obc["lesser"][1]]
+    obc_g = [obc["greater"][0], None, None, obc["greater"][1]]
+    zd = [np.zeros_like(x) for x in d]
+    zu = [np.zeros_like(x) for x in u]
+    res = orc.selected_solve(d, u, lo, zd, zu, zd, zu, obc_r, obc_l, obc_g, return_current=True,
+                             current_stale_coupling=True)
+    for key in ("xl", "xg"):
+        for part in ("diag", "upper", "lower"):
+            got = np.stack(res[f"{key}_{part}"], axis=1)
+            assert _rel(got, g[f"{key}_{part}"]) < 1e-11, (key, part)
+    assert _rel(np.stack(res["xr_diag"], axis=1), g["xr_diag"]) < 1e-11
+    assert _rel(res["current"], g["current"]) < 1e-10
+    xd, xu, xlo = orc.selected_inv(d, u, lo, obc_r)
+    assert _rel(np.stack(xd, axis=1), g["inv_diag"]) < 1e-11
+    assert _rel(np.stack(xu, axis=1), g["inv_upper"]) < 1e-11
+    assert _rel(np.stack(xlo, axis=1), g["inv_lower"]) < 1e-11
+    assert nb == len(d)
+
+
+def test_oracle_transport_cfg_small_subset():
+    g = np.load(os.path.join(GOLDEN, "transport_cfg_small_subset.npz"))
+    dev = make_device(num_blocks=16, block_size=64, num_energies=32, seed=1234)
+    e = dev.energies[g["energy_index"]]
+    d, u, lo = dev.system_blocks(e)
+    obc = orc.obc_self_energies(d, u, lo, e, dev.mu_left, dev.mu_right, dev.kt, dev.sr_tol, dev.sr_max_iter)
+    nb = 16
+    pad = [None] * (nb - 2)
+    res = orc.selected_solve(
+        d, u, lo, [np.zeros_like(x) for x in d], [np.zeros_like(x) for x in u],
+        [np.zeros_like(x) for x in d], [np.zeros_like(x) for x in u],
+        [obc["retarded"][0], *pad, obc["retarded"][1]],
+        [obc["lesser"][0], *pad, obc["lesser"][1]],
+        [obc["greater"][0], *pad, obc["greater"][1]], return_current=True, return_extras=True)
+    for key in ("xl", "xg", "xr"):
+        dd = np.stack(res[f"{key}_diag"], axis=1)
+        assert _rel(np.linalg.norm(dd, axis=(-2, -1)), g[f"{key}_diag_fro"]) < 1e-10
+        assert _rel(orc.block_density(res[f"{key}_diag"]), g[f"{key}_block_density"]) < 1e-10
+        assert _rel(dd[:, 0], g[f"{key}_first_block"]) < 1e-10
+    # upstream reads a stale coupling for every interface but the last
+    assert _rel(res["current"][:, -1], g["current"][:, -1]) < 1e-9
+    # Meir-Wingreen with the interface's own coupling conserves the current
+    # through a ballistic device: every interface carries the left contact
+    # current, up to the leakage of the eta = 1e-6 broadening (< 1e-2 here;
+    # the stale upstream coupling is off by O(1) on these interfaces)
+    for k in range(nb - 1):
+        assert np.allclose(res["current"][:, k], g["i_left"], rtol=1e-2, atol=1e-9 * np.abs(g["i_left"]).max())
+    i_l, i_r = orc.contact_currents(res["xl_diag"][0], res["xg_diag"][0], res["xl_diag"][-1], res["xg_diag"][-1], obc)
+    assert _rel(i_l, g["i_left"]) < 1e-9 and _rel(i_r, g["i_right"]) < 1e-9
+    # Caroli transmission against the contact current (ballistic device)
+    t = orc.caroli_transmission(res["xr_corner"], obc["gamma"][0], obc["gamma"][1])
+    f_l = orc.fermi_dirac(e - dev.mu_left, dev.kt)
+    f_r = orc.fermi_dirac(e - dev.mu_right, dev.kt)
+    sel = np.abs(f_l - f_r) > 1e-3
+    if sel.any():
+        t_cur = (-g["i_left"][sel] / (f_l[sel] - f_r[sel])).real
+        assert np.allclose(t[sel], t_cur, rtol=1e-7, atol=1e-9)
+
+
+def test_oracle_selected_inv_matches_dense_inverse():
+    dev = make_device(num_blocks=5, block_size=6, num_energies=3, seed=3)
+    d, u, lo = dev.system_blocks()
+    xd, xu, xlo = orc.selected_inv(d, u, lo)
+    full = np.linalg.inv(orc.dense_from_blocks(d, u, lo))
+    got = orc.dense_from_blocks(xd, xu, xlo)
+    mask = orc.dense_from_blocks([np.ones_like(x) for x in d], [np.ones_like(x) for x in u], [np.ones_like(x) for x in lo]) != 0
+    assert _rel(got * mask, full * mask) < 1e-10
+
+
+def test_oracle_sancho_rubio_fixed_point():
+    """The upstream SR test criterion: x = inv(a_ii - a_ji x a_ij)."""
+    dev = make_device(num_blocks=2, block_size=10, num_energies=5, seed=5)
+    d, u, lo = dev.system_blocks()
+    x, it = orc.sancho_rubio(d[0], u[0], lo[0], 200, 1e-12)
+    assert it < 200
+    assert _rel(x, np.linalg.inv(d[0] - lo[0] @ x @ u[0])) < 1e-6
+    with pytest.warns(RuntimeWarning):
+        orc.sancho_rubio(d[0], u[0], lo[0], 1, 1e-12)
+
+
+def test_get_batches_matches_upstream_rule():
+    assert orc.get_batches(10, 3)[0] == [4, 3, 3]
+    assert orc.get_batches(10, 100)[0] == [10]
+    assert orc.get_batches(7, 1)[0] == [1] * 7
+    assert list(orc.get_batches(10, 2)[1]) == [0, 2, 4, 6, 8, 10]
