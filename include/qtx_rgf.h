@@ -1,0 +1,205 @@
+/*
+ * qtx_rgf.h -- C ABI of libqtxrgf.so, the B200 (sm_100a) recursive Green's
+ * function (RGF) solver for block-tridiagonal systems
+ *     A(E) = (E + i eta) S - H - Sigma^R_OBC(E)
+ * batched over the energy (stack) axis.
+ *
+ * Every entry point is a drop-in for one call of the upstream qttools /
+ * quatrex Python API (paths relative to the upstream repository):
+ *
+ *   qtx_selected_inv    <- qttools.greens_function_solver.RGF.selected_inv
+ *                          (src/qttools/greens_function_solver/rgf.py:25-113,
+ *                           abstract signature solver.py:34-60)
+ *   qtx_selected_solve  <- qttools.greens_function_solver.RGF.selected_solve
+ *                          (src/qttools/greens_function_solver/rgf.py:115-414,
+ *                           abstract signature solver.py:62-113)
+ *   qtx_sancho_rubio    <- qttools.boundary_conditions.obc.SanchoRubio.__call__
+ *                          (src/qttools/boundary_conditions/obc/sancho_rubio.py:33-86)
+ *   qtx_inv             <- qttools.kernels.linalg.inv
+ *                          (src/qttools/kernels/linalg/inv.py:24-40)
+ *   qtx_obc_assemble    <- the contact part of ElectronSolver._compute_obc
+ *                          (src/quatrex/electron/solver.py:318-337, 372-386)
+ *   qtx_transport_solve <- ElectronSolver.solve for a device whose leads
+ *                          repeat its end cells: A(E) assembly
+ *                          (src/quatrex/electron/solver.py:388-410), both
+ *                          contacts (:305-386), selected_solve (:533-541) and
+ *                          the observables (src/quatrex/core/observables.py:57-189)
+ *
+ * Conventions
+ *  - complex numbers are interleaved (re, im) doubles, layout-identical to
+ *    numpy.complex128 / torch.complex128; every matrix is row-major.
+ *  - A block-tridiagonal matrix is stored in the DSDBSparse layout of qttools
+ *    (src/qttools/datastructures/dsdbsparse.py:109-247): one data row of nnz
+ *    entries per stack element; the entries of block (i, j) form one
+ *    contiguous slice of that row (src/qttools/datastructures/dsdbcoo.py:285-319).
+ *    qtx_btd_desc describes, for each of the 3*nb-2 blocks, where its slice
+ *    starts and how its entries map into the dense block.
+ *  - All data pointers are DEVICE pointers unless QTX_FLAG_HOST_BUFFERS is set,
+ *    in which case they are host pointers (pinned memory is fastest) and the
+ *    library streams the energy batches through the device itself.
+ *  - Nothing is synchronous unless stated: work is enqueued on `stream`.
+ *  - No exception crosses the ABI; every call returns a qtx_status and the
+ *    context keeps a text message (qtx_last_error).
+ */
+#ifndef QTX_RGF_H_
+#define QTX_RGF_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int qtx_status;
+#define QTX_OK 0
+#define QTX_E_INVAL 1          /* invalid argument */
+#define QTX_E_NOMEM 2          /* device memory exhausted / over the admission budget */
+#define QTX_E_SINGULAR 3       /* exact zero pivot in a diagonal-block inverse */
+#define QTX_E_NOT_CONVERGED 4  /* Sancho-Rubio reached max_iterations (results still written) */
+#define QTX_E_TIMEOUT 5        /* a bounded device-side wait gave up */
+#define QTX_E_CUDA 6           /* CUDA runtime error */
+#define QTX_E_UNSUPPORTED 7    /* option not implemented */
+
+/* precision of the bulk block products */
+#define QTX_PREC_FP64 0        /* complex128 throughout */
+#define QTX_PREC_MIXED 1       /* bulk Schur/Keldysh products in 3xTF32 complex FP32 on tcgen05;
+                                  inverses, Sancho-Rubio and the refinement residual in FP64 */
+
+/* flags of qtx_selected_solve */
+#define QTX_FLAG_RETURN_RETARDED 0x1u  /* write diagonal X^R blocks to xr (rgf.py:304-305, 403-404) */
+#define QTX_FLAG_RETURN_CURRENT 0x2u   /* Meir-Wingreen layer current (rgf.py:381-400) */
+#define QTX_FLAG_SYMMETRIC_OUT 0x4u    /* outputs store the upper triangle only (rgf.py:351, 373) */
+#define QTX_FLAG_HOST_BUFFERS 0x8u     /* every data pointer is host memory */
+#define QTX_FLAG_RETARDED_OFFDIAG 0x10u /* also write X^R off-diagonal blocks into xr */
+
+typedef struct qtx_ctx qtx_ctx;
+typedef struct CUstream_st* qtx_stream; /* == cudaStream_t; NULL = legacy default stream */
+
+/* Block map of a block-tridiagonal DSDBSparse matrix.  Block (i, j), |i-j|<=1,
+ * has index k = 2*i + j (order (0,0),(0,1),(1,0),(1,1),(1,2),(2,1),...). */
+typedef struct qtx_btd_desc {
+  int32_t num_blocks;                 /* nb */
+  const int32_t* block_sizes;         /* host [nb] */
+  const int64_t* block_offset;        /* host [3nb-2]: first entry of block k in a data row; -1 = empty block */
+  const int64_t* block_nnz;           /* host [3nb-2]: entries of block k */
+  const int32_t* const* block_index;  /* host [3nb-2] of DEVICE pointers: local linear index r*cols+c of
+                                         each entry of block k; NULL entry = block is dense row-major.
+                                         The array itself may be NULL (all blocks dense). */
+  int64_t stack_size;                 /* number of stack elements (energies), stack flattened */
+  int64_t stack_stride;               /* complex elements between consecutive data rows (>= nnz) */
+} qtx_btd_desc;
+
+/* Boundary blocks: per diagonal block i, NULL or a pointer to a contiguous
+ * (stack_size, b_i, b_i) complex array (OBCBlocks, solver.py:12-28). */
+typedef struct qtx_obc {
+  const void* const* retarded;  /* host [nb] of pointers, or NULL */
+  const void* const* lesser;    /* host [nb] of pointers, or NULL */
+  const void* const* greater;   /* host [nb] of pointers, or NULL */
+} qtx_obc;
+
+qtx_status qtx_ctx_create(int device, qtx_ctx** out);
+qtx_status qtx_ctx_destroy(qtx_ctx* ctx);
+const char* qtx_last_error(const qtx_ctx* ctx);
+/* Device bytes the context may keep for workspaces (0 = no limit). */
+qtx_status qtx_ctx_set_memory_limit(qtx_ctx* ctx, size_t bytes);
+/* Release cached workspaces. */
+qtx_status qtx_ctx_trim(qtx_ctx* ctx);
+/* Library version string. */
+const char* qtx_version(void);
+
+/* Batched inverse of (batch, n, n) complex matrices; x may alias a.
+ * <- qttools.kernels.linalg.inv (src/qttools/kernels/linalg/inv.py:24-40). */
+qtx_status qtx_inv(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a, int64_t stride_a, void* x,
+                   int64_t stride_x, qtx_stream stream);
+
+/* Batched complex GEMM D = alpha op(A) op(B) + beta C, all row-major with
+ * per-matrix strides; op = 0 (none) or 1 (conjugate transpose).  Exposed for
+ * the tests and the autotuner; the solver uses it internally. */
+qtx_status qtx_zgemm(qtx_ctx* ctx, int32_t m, int32_t n, int32_t k, int64_t batch, double alpha_re,
+                     double alpha_im, const void* a, int64_t lda, int64_t stride_a, int32_t op_a,
+                     const void* b, int64_t ldb, int64_t stride_b, int32_t op_b, double beta_re,
+                     double beta_im, const void* c, int64_t ldc, int64_t stride_c, void* d, int64_t ldd,
+                     int64_t stride_d, int32_t precision, qtx_stream stream);
+
+/* Selected inversion: out receives X = A^-1 on the BTD pattern of out_desc.
+ * obc_retarded: NULL or host [nb] of device pointers subtracted from A_ii.
+ * <- RGF.selected_inv(a, obc_blocks, out) (rgf.py:25-113). */
+qtx_status qtx_selected_inv(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const void* a,
+                            const void* const* obc_retarded, const qtx_btd_desc* out_desc, void* out,
+                            int64_t max_batch_size, int32_t precision, uint32_t flags, qtx_stream stream);
+
+/* Selected solve: X^< = A^-1 Sigma^< A^-H, X^> likewise, and (flags) diagonal
+ * X^R and the layer current (stack_size, nb-1) complex.
+ * <- RGF.selected_solve(a, sigma_lesser, sigma_greater, obc_blocks, out,
+ *    return_retarded, return_current) (rgf.py:115-414).  OBC lesser/greater
+ * blocks are ADDED to the diagonal Sigma blocks and the retarded ones
+ * subtracted from A, as in rgf.py:207-255. */
+qtx_status qtx_selected_solve(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const void* a,
+                              const qtx_btd_desc* sl_desc, const void* sigma_lesser,
+                              const qtx_btd_desc* sg_desc, const void* sigma_greater, const qtx_obc* obc,
+                              const qtx_btd_desc* xl_desc, void* xl, const qtx_btd_desc* xg_desc, void* xg,
+                              const qtx_btd_desc* xr_desc, void* xr, void* current, int64_t max_batch_size,
+                              int32_t precision, uint32_t flags, qtx_stream stream);
+
+/* Sancho-Rubio surface Green's function x = inv(a_ii - a_ji x a_ij) for a
+ * batch of (n, n) blocks; each input has its own batch stride (0 = shared).
+ * iterations (device, [batch], may be NULL) receives the iteration count of
+ * each batch entry; converged entries stop iterating (per-entry masks).
+ * Returns QTX_E_NOT_CONVERGED (after writing x) when an entry reached
+ * max_iterations (sancho_rubio.py:81-82 warns in that case).
+ * <- SanchoRubio(max_iterations, convergence_tol)(a_ii, a_ij, a_ji, contact). */
+qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                            const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
+                            double convergence_tol, int32_t max_iterations, void* x, int32_t* iterations,
+                            qtx_stream stream);
+
+/* Contact self-energies from a surface Green's function g (batch, n, n):
+ * sigma_r = m_ji g m_ij, gamma = i (sigma_r - sigma_r^H),
+ * sigma_l = i f gamma, sigma_g = i (f - 1) gamma with f = occupancy[batch]
+ * (src/quatrex/electron/solver.py:318-337). m_ij/m_ji may have stride 0. */
+qtx_status qtx_obc_assemble(qtx_ctx* ctx, int32_t n, int64_t batch, const void* g, const void* m_ji,
+                            int64_t stride_ji, const void* m_ij, int64_t stride_ij, const double* occupancy,
+                            void* sigma_r, void* sigma_l, void* sigma_g, qtx_stream stream);
+
+/* Generator-form transport solve of a device with constant block size b.
+ * H is energy independent and resident on the device; A(E) = (E + i eta) I - H
+ * is built per energy batch on the device, both contacts come from
+ * Sancho-Rubio, and the selected solve writes the requested outputs.  Output
+ * pointers may be NULL (not stored).  Block arrays are dense and contiguous:
+ * diagonal outputs (num_energies, nb, b, b), off-diagonal (num_energies, nb-1, b, b). */
+typedef struct qtx_transport_problem {
+  int32_t num_blocks;
+  int32_t block_size;
+  int64_t num_energies;
+  const void* h_diag;       /* (nb, b, b) */
+  const void* h_upper;      /* (nb-1, b, b): H[i, i+1]; H[i+1, i] = H[i, i+1]^H */
+  const double* energies;   /* (num_energies) device */
+  double eta, mu_left, mu_right, kt;
+  double sr_tol;
+  int32_t sr_max_iterations;
+  int64_t max_batch_size;   /* energies per device batch */
+} qtx_transport_problem;
+
+typedef struct qtx_transport_outputs {
+  void* gr_diag; void* gr_upper; void* gr_lower;   /* G^R */
+  void* gl_diag; void* gl_upper;                   /* G^< (lower = -upper^H) */
+  void* gg_diag; void* gg_upper;                   /* G^> */
+  double* density;       /* (num_energies, nb): sum over each block of Im diag G^< */
+  double* hole_density;  /* (num_energies, nb): sum over each block of -Im diag G^> */
+  double* transmission;  /* (num_energies): Tr[Gamma_L G^R_0N Gamma_R G^R_0N^H] */
+  void* current_left;    /* (num_energies) complex contact current (observables.py:151-157) */
+  void* current_right;   /* (num_energies) complex */
+  int32_t* sr_iterations; /* (num_energies, 2) */
+} qtx_transport_outputs;
+
+qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,
+                               int32_t precision, uint32_t flags, qtx_stream stream);
+
+/* Number of kernel launches this context has issued (for launch accounting). */
+int64_t qtx_launch_count(const qtx_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QTX_RGF_H_ */

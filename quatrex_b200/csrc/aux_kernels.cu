@@ -1,0 +1,411 @@
+// Bandwidth-bound helper kernels of the RGF path: block gather/scatter
+// between dense blocks and DSDBSparse data rows, Hermitian combinations,
+// traces, diagonal sums, Sancho-Rubio convergence norms, A(E) assembly, the
+// contact self-energy assembly and Fermi occupancies.  All are grid-stride
+// loops over (batch, element) with coalesced row-major access; the transposed
+// operands go through 32x32 shared-memory tiles.
+#include "kernels.h"
+
+namespace {
+
+constexpr int TB = 256;
+
+inline unsigned grid_for(int64_t work) {
+  int64_t g = (work + TB - 1) / TB;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+// out = s + w^H - w, square n x n; tiles of 32x32 for the transposed read
+__global__ void skew_combine_kernel(int n, int64_t batch, const cplx* s, int64_t lds, int64_t ss, const cplx* w,
+                                    int64_t ldw, int64_t sw, cplx* out, int64_t ldo, int64_t so) {
+  __shared__ cplx tile[32][33];
+  const int tiles = (n + 31) / 32;
+  const int64_t total = batch * tiles * tiles;
+  for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+    int64_t e = t / (tiles * tiles);
+    int rem = (int)(t % (tiles * tiles));
+    int tr = rem / tiles, tc = rem % tiles;
+    // load w tile (tc, tr) transposed: rows tc*32.., cols tr*32..
+    for (int q = threadIdx.x; q < 32 * 32; q += blockDim.x) {
+      int r = q / 32, c = q % 32;
+      int gr = tc * 32 + r, gc = tr * 32 + c;
+      tile[r][c] = (gr < n && gc < n) ? w[e * sw + (int64_t)gr * ldw + gc] : cmk(0, 0);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 32 * 32; q += blockDim.x) {
+      int r = q / 32, c = q % 32;
+      int gr = tr * 32 + r, gc = tc * 32 + c;
+      if (gr < n && gc < n) {
+        cplx wt = tile[c][r];  // w[gc][gr]
+        cplx wv = w[e * sw + (int64_t)gr * ldw + gc];
+        cplx sv = s[e * ss + (int64_t)gr * lds + gc];
+        out[e * so + (int64_t)gr * ldo + gc] = cmk(sv.x + wt.x - wv.x, sv.y - wt.y - wv.y);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// x <- x - x^H in place: each thread owns the pair (r, c), (c, r) with r <= c
+__global__ void sub_herm_kernel(int n, int64_t batch, cplx* x, int64_t ld, int64_t sx) {
+  const int64_t pairs = (int64_t)n * (n + 1) / 2;
+  const int64_t total = batch * pairs;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t e = t / pairs;
+    int64_t q = t % pairs;
+    // invert q -> (r, c), r <= c, row-major over the upper triangle
+    int r = (int)((2.0 * n + 1 - sqrt((2.0 * n + 1) * (2.0 * n + 1) - 8.0 * q)) / 2);
+    while ((int64_t)r * n - (int64_t)r * (r - 1) / 2 > q) --r;
+    while ((int64_t)(r + 1) * n - (int64_t)(r + 1) * r / 2 <= q) ++r;
+    int c = r + (int)(q - ((int64_t)r * n - (int64_t)r * (r - 1) / 2));
+    cplx* base = x + e * sx;
+    cplx a = base[(int64_t)r * ld + c];
+    cplx b = base[(int64_t)c * ld + r];
+    // new a = a - conj(b); new b = b - conj(a)
+    base[(int64_t)r * ld + c] = cmk(a.x - b.x, a.y + b.y);
+    if (r != c) base[(int64_t)c * ld + r] = cmk(b.x - a.x, b.y + a.y);
+    else base[(int64_t)r * ld + c] = cmk(0.0, 2.0 * a.y);
+  }
+}
+
+__global__ void axpby_kernel(int rows, int cols, int64_t batch, cplx alpha, const cplx* x, int64_t ldx, int64_t sx,
+                             cplx beta, const cplx* y, int64_t ldy, int64_t sy, cplx* out, int64_t ldo, int64_t so,
+                             const int* active) {
+  const int64_t per = (int64_t)rows * cols;
+  const int64_t total = batch * per;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t e = t / per;
+    if (active && !active[e]) continue;
+    int q = (int)(t % per);
+    int r = q / cols, c = q % cols;
+    cplx v = cmul(alpha, x[e * sx + (int64_t)r * ldx + c]);
+    if (y) v = cfma(beta, y[e * sy + (int64_t)r * ldy + c], v);
+    out[e * so + (int64_t)r * ldo + c] = v;
+  }
+}
+
+// scatter dense block -> data slice; mode 0 copy, 1 0.5(X - X^H), 2 -X^H
+// (mode 2: the stored block is cols_out x rows_out = the transpose shape of x;
+// `rows`/`cols` are the shape of the STORED block)
+__global__ void block_scatter_kernel(int rows, int cols, int64_t batch, const cplx* x, int64_t ldx, int64_t sx,
+                                     int mode, cplx* data, int64_t stride, int64_t nnz, const int32_t* index) {
+  const int64_t total = batch * nnz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t e = t / nnz;
+    int64_t q = t % nnz;
+    int lin = index ? index[q] : (int)q;
+    int r = lin / cols, c = lin % cols;
+    const cplx* xb = x + e * sx;
+    cplx v;
+    if (mode == 0) {
+      v = xb[(int64_t)r * ldx + c];
+    } else if (mode == 1) {
+      cplx a = xb[(int64_t)r * ldx + c];
+      cplx b = xb[(int64_t)c * ldx + r];
+      v = cmk(0.5 * (a.x - b.x), 0.5 * (a.y + b.y));
+    } else {
+      cplx b = xb[(int64_t)c * ldx + r];
+      v = cmk(-b.x, b.y);
+    }
+    data[e * stride + q] = v;
+  }
+}
+
+__global__ void block_gather_kernel(int rows, int cols, int64_t batch, const cplx* data, int64_t stride, int64_t nnz,
+                                    const int32_t* index, cplx* out, int64_t ldo, int64_t so) {
+  // zero the dense block first (grid-stride), then scatter the entries
+  const int64_t per = (int64_t)rows * cols;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < batch * per; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t e = t / per;
+    int q = (int)(t % per);
+    out[e * so + (int64_t)(q / cols) * ldo + (q % cols)] = cmk(0, 0);
+  }
+}
+__global__ void block_gather_fill_kernel(int rows, int cols, int64_t batch, const cplx* data, int64_t stride,
+                                         int64_t nnz, const int32_t* index, cplx* out, int64_t ldo, int64_t so) {
+  const int64_t total = batch * nnz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t e = t / nnz;
+    int64_t q = t % nnz;
+    int lin = index ? index[q] : (int)q;
+    int r = lin / cols, c = lin % cols;
+    out[e * so + (int64_t)r * ldo + c] = data[e * stride + q];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// one CTA per batch entry: block reduction of a complex sum
+__device__ cplx block_sum(cplx v) {
+  __shared__ double sre[32], sim[32];
+  double re = warp_sum(v.x), im = warp_sum(v.y);
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sre[warp] = re;
+    sim[warp] = im;
+  }
+  __syncthreads();
+  cplx out = cmk(0, 0);
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      out.x += sre[w];
+      out.y += sim[w];
+    }
+  }
+  __syncthreads();
+  return out;
+}
+
+__global__ void trace_product_kernel(int rows, int cols, int64_t batch, const cplx* x, int64_t ldx, int64_t sx,
+                                     const cplx* y, int64_t ldy, int64_t sy, cplx scale, cplx* tr, int accumulate) {
+  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
+    cplx acc = cmk(0, 0);
+    for (int q = threadIdx.x; q < rows * cols; q += blockDim.x) {
+      int r = q / cols, c = q % cols;
+      acc = cfma(x[e * sx + (int64_t)r * ldx + c], y[e * sy + (int64_t)c * ldy + r], acc);
+    }
+    cplx s = block_sum(acc);
+    if (threadIdx.x == 0) {
+      s = cmul(s, scale);
+      tr[e] = accumulate ? cadd(tr[e], s) : s;
+    }
+  }
+}
+
+__global__ void trace_product_h_kernel(int rows, int cols, int64_t batch, const cplx* x, int64_t ldx, int64_t sx,
+                                       const cplx* y, int64_t ldy, int64_t sy, cplx* tr) {
+  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
+    cplx acc = cmk(0, 0);
+    for (int q = threadIdx.x; q < rows * cols; q += blockDim.x) {
+      int r = q / cols, c = q % cols;
+      acc = cfma(x[e * sx + (int64_t)r * ldx + c], cconj(y[e * sy + (int64_t)r * ldy + c]), acc);
+    }
+    cplx s = block_sum(acc);
+    if (threadIdx.x == 0) tr[e] = s;
+  }
+}
+
+__global__ void diag_imag_sum_kernel(int n, int64_t batch, const cplx* x, int64_t ldx, int64_t sx, double sign,
+                                     double* out, int64_t out_stride, int out_col) {
+  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
+    double acc = 0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) acc += x[e * sx + (int64_t)r * ldx + r].y;
+    cplx s = block_sum(cmk(acc, 0));
+    if (threadIdx.x == 0) out[e * out_stride + out_col] = sign * s.x;
+  }
+}
+
+__global__ void sr_norm_kernel(int n, int64_t batch, const cplx* a, int64_t lda, int64_t sa, const cplx* b,
+                               int64_t ldb, int64_t sb, double tol, int* active, int* iterations, int* num_active) {
+  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
+    if (!active[e]) continue;
+    double acc = 0;
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+      int r = q / n, c = q % n;
+      cplx av = a[e * sa + (int64_t)r * lda + c];
+      cplx bv = b[e * sb + (int64_t)r * ldb + c];
+      double s = hypot(av.x, av.y) + hypot(bv.x, bv.y);
+      acc += s * s;
+    }
+    cplx s = block_sum(cmk(acc, 0));
+    if (threadIdx.x == 0) {
+      double delta = sqrt(s.x) / 2.0;
+      if (iterations) iterations[e] += 1;
+      if (delta < tol) {
+        active[e] = 0;
+      } else {
+        atomicAdd(num_active, 1);
+      }
+    }
+  }
+}
+
+__global__ void assemble_diag_kernel(int n, int64_t batch, const cplx* h, const double* energies, double eta,
+                                     cplx* out, int64_t ldo, int64_t so) {
+  const int64_t per = (int64_t)n * n;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < batch * per; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t e = t / per;
+    int q = (int)(t % per);
+    int r = q / n, c = q % n;
+    cplx hv = h[q];
+    cplx v = cmk(-hv.x, -hv.y);
+    if (r == c) {
+      v.x += energies[e];
+      v.y += eta;
+    }
+    out[e * so + (int64_t)r * ldo + c] = v;
+  }
+}
+
+__global__ void neg_herm_kernel(int n, const cplx* h, cplx* out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n * n; q += gridDim.x * blockDim.x) {
+    int r = q / n, c = q % n;
+    cplx v = h[(int64_t)c * n + r];
+    out[q] = cmk(-v.x, v.y);
+  }
+}
+
+__global__ void obc_lg_kernel(int n, int64_t batch, const cplx* s, int64_t lds, int64_t ss, const double* occ,
+                              cplx* sl, int64_t ldl, int64_t sls, cplx* sg, int64_t ldg, int64_t sgs, cplx* gam,
+                              int64_t ldgam, int64_t sgam) {
+  const int64_t per = (int64_t)n * n;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < batch * per; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t e = t / per;
+    int q = (int)(t % per);
+    int r = q / n, c = q % n;
+    cplx a = s[e * ss + (int64_t)r * lds + c];
+    cplx b = s[e * ss + (int64_t)c * lds + r];
+    // gamma = i (a - conj(b))
+    cplx d = cmk(a.x - b.x, a.y + b.y);
+    cplx g = cmk(-d.y, d.x);
+    double f = occ[e];
+    // i f gamma, i (f - 1) gamma
+    cplx ig = cmk(-g.y, g.x);
+    if (sl) sl[e * sls + (int64_t)r * ldl + c] = cscale(ig, f);
+    if (sg) sg[e * sgs + (int64_t)r * ldg + c] = cscale(ig, f - 1.0);
+    if (gam) gam[e * sgam + (int64_t)r * ldgam + c] = g;
+  }
+}
+
+__global__ void fermi_kernel(int64_t batch, const double* energies, double mu, double kt, double* occ) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < batch; e += (int64_t)gridDim.x * blockDim.x)
+    occ[e] = 1.0 / (1.0 + exp((energies[e] - mu) / kt));
+}
+
+__global__ void fill_int_kernel(int* p, int64_t count, int value) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
+    p[t] = value;
+}
+
+__global__ void real_part_kernel(int64_t count, const cplx* src, double* dst) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
+    dst[t] = src[t].x;
+}
+
+}  // namespace
+
+void launch_skew_combine(int n, int64_t batch, MatView s, MatView w, MutView out, cudaStream_t stream) {
+  int tiles = (n + 31) / 32;
+  skew_combine_kernel<<<grid_for(batch * tiles * tiles * TB), TB, 0, stream>>>(
+      n, batch, s.ptr, s.ld, s.stride, w.ptr, w.ld, w.stride, out.ptr, out.ld, out.stride);
+  qtx_check_launch("skew_combine_kernel");
+}
+
+void launch_sub_herm_inplace(int n, int64_t batch, MutView x, cudaStream_t stream) {
+  sub_herm_kernel<<<grid_for(batch * (int64_t)n * (n + 1) / 2), TB, 0, stream>>>(n, batch, x.ptr, x.ld, x.stride);
+  qtx_check_launch("sub_herm_kernel");
+}
+
+void launch_axpby(int rows, int cols, int64_t batch, cplx alpha, MatView x, cplx beta, MatView y, MutView out,
+                  cudaStream_t stream, const int* active) {
+  axpby_kernel<<<grid_for(batch * (int64_t)rows * cols), TB, 0, stream>>>(
+      rows, cols, batch, alpha, x.ptr, x.ld, x.stride, beta, y.ptr, y.ld, y.stride, out.ptr, out.ld, out.stride,
+      active);
+  qtx_check_launch("axpby_kernel");
+}
+
+namespace {
+__global__ void energy_shift_kernel(int64_t batch, const double* energies, double eta, cplx* shift) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < batch; e += (int64_t)gridDim.x * blockDim.x)
+    shift[e] = cmk(energies[e], eta);
+}
+}  // namespace
+
+void launch_energy_shift(int64_t batch, const double* energies, double eta, cplx* shift, cudaStream_t stream) {
+  energy_shift_kernel<<<grid_for(batch), TB, 0, stream>>>(batch, energies, eta, shift);
+  qtx_check_launch("energy_shift_kernel");
+}
+
+void launch_block_scatter(int rows, int cols, int64_t batch, MatView x, int mode, cplx* data, int64_t stride,
+                          int64_t nnz, const int32_t* index, cudaStream_t stream) {
+  if (nnz <= 0) return;
+  block_scatter_kernel<<<grid_for(batch * nnz), TB, 0, stream>>>(rows, cols, batch, x.ptr, x.ld, x.stride, mode,
+                                                                 data, stride, nnz, index);
+  qtx_check_launch("block_scatter_kernel");
+}
+
+void launch_block_gather(int rows, int cols, int64_t batch, const cplx* data, int64_t stride, int64_t nnz,
+                         const int32_t* index, MutView out, cudaStream_t stream) {
+  block_gather_kernel<<<grid_for(batch * (int64_t)rows * cols), TB, 0, stream>>>(rows, cols, batch, data, stride,
+                                                                                nnz, index, out.ptr, out.ld,
+                                                                                out.stride);
+  qtx_check_launch("block_gather_kernel");
+  if (nnz <= 0) return;
+  block_gather_fill_kernel<<<grid_for(batch * nnz), TB, 0, stream>>>(rows, cols, batch, data, stride, nnz, index,
+                                                                     out.ptr, out.ld, out.stride);
+  qtx_check_launch("block_gather_fill_kernel");
+}
+
+void launch_trace_product(int rows, int cols, int64_t batch, MatView x, MatView y, cplx scale, cplx* tr,
+                          bool accumulate, cudaStream_t stream) {
+  unsigned g = (unsigned)(batch < 65535 ? batch : 65535);
+  trace_product_kernel<<<g, TB, 0, stream>>>(rows, cols, batch, x.ptr, x.ld, x.stride, y.ptr, y.ld, y.stride, scale,
+                                             tr, accumulate ? 1 : 0);
+  qtx_check_launch("trace_product_kernel");
+}
+
+void launch_trace_product_h(int rows, int cols, int64_t batch, MatView x, MatView y, cplx* tr, cudaStream_t stream) {
+  unsigned g = (unsigned)(batch < 65535 ? batch : 65535);
+  trace_product_h_kernel<<<g, TB, 0, stream>>>(rows, cols, batch, x.ptr, x.ld, x.stride, y.ptr, y.ld, y.stride, tr);
+  qtx_check_launch("trace_product_h_kernel");
+}
+
+void launch_diag_imag_sum(int n, int64_t batch, MatView x, double sign, double* out, int64_t out_stride, int out_col,
+                          cudaStream_t stream) {
+  unsigned g = (unsigned)(batch < 65535 ? batch : 65535);
+  diag_imag_sum_kernel<<<g, TB, 0, stream>>>(n, batch, x.ptr, x.ld, x.stride, sign, out, out_stride, out_col);
+  qtx_check_launch("diag_imag_sum_kernel");
+}
+
+void launch_sr_norm_update(int n, int64_t batch, MatView alpha, MatView beta, double tol, int* active,
+                           int* iterations, int* num_active, cudaStream_t stream) {
+  unsigned g = (unsigned)(batch < 65535 ? batch : 65535);
+  sr_norm_kernel<<<g, TB, 0, stream>>>(n, batch, alpha.ptr, alpha.ld, alpha.stride, beta.ptr, beta.ld, beta.stride,
+                                       tol, active, iterations, num_active);
+  qtx_check_launch("sr_norm_kernel");
+}
+
+void launch_assemble_diag(int n, int64_t batch, const cplx* h, const double* energies, double eta, MutView out,
+                          cudaStream_t stream) {
+  assemble_diag_kernel<<<grid_for(batch * (int64_t)n * n), TB, 0, stream>>>(n, batch, h, energies, eta, out.ptr,
+                                                                            out.ld, out.stride);
+  qtx_check_launch("assemble_diag_kernel");
+}
+
+void launch_neg_herm(int n, const cplx* h, cplx* out, cudaStream_t stream) {
+  neg_herm_kernel<<<grid_for((int64_t)n * n), TB, 0, stream>>>(n, h, out);
+  qtx_check_launch("neg_herm_kernel");
+}
+
+void launch_obc_lesser_greater(int n, int64_t batch, MatView sigma_r, const double* occ, MutView sl, MutView sg,
+                               MutView gamma, cudaStream_t stream) {
+  obc_lg_kernel<<<grid_for(batch * (int64_t)n * n), TB, 0, stream>>>(n, batch, sigma_r.ptr, sigma_r.ld,
+                                                                     sigma_r.stride, occ, sl.ptr, sl.ld, sl.stride,
+                                                                     sg.ptr, sg.ld, sg.stride, gamma.ptr, gamma.ld,
+                                                                     gamma.stride);
+  qtx_check_launch("obc_lg_kernel");
+}
+
+void launch_fermi(int64_t batch, const double* energies, double mu, double kt, double* occ, cudaStream_t stream) {
+  fermi_kernel<<<grid_for(batch), TB, 0, stream>>>(batch, energies, mu, kt, occ);
+  qtx_check_launch("fermi_kernel");
+}
+
+void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream) {
+  if (count <= 0) return;
+  fill_int_kernel<<<grid_for(count), TB, 0, stream>>>(p, count, value);
+  qtx_check_launch("fill_int_kernel");
+}
+
+void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t stream) {
+  if (count <= 0) return;
+  real_part_kernel<<<grid_for(count), TB, 0, stream>>>(count, src, dst);
+  qtx_check_launch("real_part_kernel");
+}

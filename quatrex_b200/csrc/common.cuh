@@ -1,0 +1,71 @@
+// Shared device helpers of libqtxrgf: complex double arithmetic on double2,
+// status codes and launch bookkeeping.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/qtx_rgf.h"
+
+typedef double2 cplx;
+
+__host__ __device__ __forceinline__ cplx cmk(double r, double i) { return make_double2(r, i); }
+__host__ __device__ __forceinline__ cplx cadd(cplx a, cplx b) { return cmk(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ cplx csub(cplx a, cplx b) { return cmk(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+  return cmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ cplx cconj(cplx a) { return cmk(a.x, -a.y); }
+__host__ __device__ __forceinline__ cplx cscale(cplx a, double s) { return cmk(a.x * s, a.y * s); }
+// a + b*c
+__host__ __device__ __forceinline__ cplx cfma(cplx b, cplx c, cplx a) {
+  return cmk(fma(b.x, c.x, fma(-b.y, c.y, a.x)), fma(b.x, c.y, fma(b.y, c.x, a.y)));
+}
+// a - b*c
+__host__ __device__ __forceinline__ cplx cfms(cplx b, cplx c, cplx a) {
+  return cmk(fma(-b.x, c.x, fma(b.y, c.y, a.x)), fma(-b.x, c.y, fma(-b.y, c.x, a.y)));
+}
+// 1 / z by Smith's scaled division (R. L. Smith, CACM 5(8), 1962), which avoids
+// overflow of |z|^2 for large or small components.
+__host__ __device__ __forceinline__ cplx crecip(cplx z) {
+  if (fabs(z.x) >= fabs(z.y)) {
+    double r = z.y / z.x;
+    double den = z.x + z.y * r;
+    return cmk(1.0 / den, -r / den);
+  } else {
+    double r = z.x / z.y;
+    double den = z.x * r + z.y;
+    return cmk(r / den, -1.0 / den);
+  }
+}
+__host__ __device__ __forceinline__ double cabs1(cplx z) { return fabs(z.x) + fabs(z.y); }
+
+// Per-context launch counter (host side), incremented by every launch helper.
+extern thread_local int64_t* g_qtx_launch_counter;
+inline void qtx_count_launch() {
+  if (g_qtx_launch_counter) ++*g_qtx_launch_counter;
+}
+
+#define QTX_CUDA_TRY(expr)                                           \
+  do {                                                               \
+    cudaError_t _e = (expr);                                         \
+    if (_e != cudaSuccess) {                                         \
+      throw QtxError(QTX_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    }                                                                \
+  } while (0)
+
+struct QtxError {
+  qtx_status code;
+  std::string msg;
+  QtxError(qtx_status c, std::string m) : code(c), msg(std::move(m)) {}
+};
+
+inline void qtx_check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw QtxError(QTX_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  qtx_count_launch();
+}
+
+inline unsigned ceil_div_u(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }

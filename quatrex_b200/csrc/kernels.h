@@ -1,0 +1,93 @@
+// Host-side launchers of the device kernels of libqtxrgf (all enqueue on `stream`).
+#pragma once
+
+#include "common.cuh"
+
+// A strided batch of row-major complex matrices: element (e, r, c) at
+// ptr[e * stride + r * ld + c].  stride 0 broadcasts one matrix over the batch.
+struct MatView {
+  const cplx* ptr = nullptr;
+  int64_t ld = 0;
+  int64_t stride = 0;
+};
+struct MutView {
+  cplx* ptr = nullptr;
+  int64_t ld = 0;
+  int64_t stride = 0;
+  operator MatView() const { return MatView{ptr, ld, stride}; }
+};
+
+enum Op : int { OP_N = 0, OP_C = 1 };
+
+// D = alpha op(A) op(B) + beta C + gamma C2   (C, C2 optional: ptr == nullptr)
+// op(A) is m x k, op(B) is k x n.  `active` (device, [batch], optional) skips
+// batch entries whose flag is 0.  D may alias C or C2 but not A or B.
+struct GemmCall {
+  int m = 0, n = 0, k = 0;
+  int64_t batch = 0;
+  MatView a; int op_a = OP_N;
+  MatView b; int op_b = OP_N;
+  MatView c; cplx beta = {0, 0};
+  MatView c2; cplx gamma = {0, 0};
+  MutView d; cplx alpha = {1, 0};
+  const int* active = nullptr;
+  // optional per-batch-entry diagonal shift: D[r][r] += diag_shift[e] (e.g. (E + i eta) I)
+  const cplx* diag_shift = nullptr;
+};
+void launch_zgemm(const GemmCall& g, cudaStream_t stream);
+
+// Mixed-precision (3xTF32 on tcgen05) variant of the same contract.
+void launch_zgemm_tf32x3(const GemmCall& g, cudaStream_t stream);
+bool tf32x3_supported(const GemmCall& g);
+
+// Batched in-place-capable Gauss-Jordan inverse with partial pivoting:
+// X = A^-1 for n x n matrices.  info[e] (device, optional) receives 0 or the
+// 1-based column of the first exactly-zero pivot.  X may alias A.
+void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const int* active,
+                 cudaStream_t stream);
+
+// out = s + gamma_s * s2 + w^H - w  (n x n), in place allowed for out == s.
+void launch_skew_combine(int n, int64_t batch, MatView s, MatView w, MutView out, cudaStream_t stream);
+// x = x - x^H in place (n x n).
+void launch_sub_herm_inplace(int n, int64_t batch, MutView x, cudaStream_t stream);
+// out = alpha * x + beta * y (rows x cols); y optional; entries with active[e] == 0 untouched.
+void launch_axpby(int rows, int cols, int64_t batch, cplx alpha, MatView x, cplx beta, MatView y, MutView out,
+                  cudaStream_t stream, const int* active = nullptr);
+// shift[e] = (energies[e] + i eta)
+void launch_energy_shift(int64_t batch, const double* energies, double eta, cplx* shift, cudaStream_t stream);
+
+// Scatter / gather between dense (batch, rows, cols) blocks and a DSDBSparse
+// data slice (entry q of the block at data[e * stride + q], local index
+// index[q] = r * cols + c, or row-major dense when index == nullptr).
+// mode: 0 = copy, 1 = 0.5 (X - X^H) (square), 2 = -X^H (out is cols x rows of x^H)
+void launch_block_scatter(int rows, int cols, int64_t batch, MatView x, int mode, cplx* data, int64_t stride,
+                          int64_t nnz, const int32_t* index, cudaStream_t stream);
+void launch_block_gather(int rows, int cols, int64_t batch, const cplx* data, int64_t stride, int64_t nnz,
+                         const int32_t* index, MutView out, cudaStream_t stream);
+
+// tr[e] (+)= sum_rc x[r][c] * y[c][r] * scale  (trace of x y); x rows x cols, y cols x rows.
+// accumulate: add into tr instead of overwriting.
+void launch_trace_product(int rows, int cols, int64_t batch, MatView x, MatView y, cplx scale, cplx* tr,
+                          bool accumulate, cudaStream_t stream);
+// tr[e] = sum_rc x[r][c] * conj(y[r][c])   (Tr[x y^H])
+void launch_trace_product_h(int rows, int cols, int64_t batch, MatView x, MatView y, cplx* tr,
+                            cudaStream_t stream);
+// out[e * out_stride + out_col] = sign * sum_r Im x[r][r]
+void launch_diag_imag_sum(int n, int64_t batch, MatView x, double sign, double* out, int64_t out_stride,
+                          int out_col, cudaStream_t stream);
+// Sancho-Rubio convergence: delta[e] = || |alpha| + |beta| ||_F / 2 ; then
+// active[e] = active[e] && delta >= tol; iterations[e] += active-before.
+void launch_sr_norm_update(int n, int64_t batch, MatView alpha, MatView beta, double tol, int* active,
+                           int* iterations, int* num_active, cudaStream_t stream);
+// A_ii(E) = (E + i eta) I - H  for energies[batch]; out (batch, n, n).
+void launch_assemble_diag(int n, int64_t batch, const cplx* h, const double* energies, double eta, MutView out,
+                          cudaStream_t stream);
+// out = -H^H for a single matrix (n x n).
+void launch_neg_herm(int n, const cplx* h, cplx* out, cudaStream_t stream);
+// gamma = i (s - s^H); sl = i f gamma; sg = i (f - 1) gamma with f = occ[e]
+void launch_obc_lesser_greater(int n, int64_t batch, MatView sigma_r, const double* occ, MutView sl, MutView sg,
+                               MutView gamma, cudaStream_t stream);
+// occ[e] = 1 / (1 + exp((E_e - mu) / kT))
+void launch_fermi(int64_t batch, const double* energies, double mu, double kt, double* occ, cudaStream_t stream);
+void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream);
+void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t stream);

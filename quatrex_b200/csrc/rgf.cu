@@ -1,0 +1,1008 @@
+// RGF selected inversion / selected solve, Sancho-Rubio and the generator-form
+// transport solve: host-side orchestration of the device kernels, and the C ABI
+// of libqtxrgf.so (declared in include/qtx_rgf.h).
+//
+// Every sweep runs on the caller's stream over one energy batch at a time
+// (qttools' max_batch_size slicing, src/qttools/utils/solvers_utils.py:7-32);
+// the per-block dense recursion state (x_i, X^<_i, X^>_i) of a batch lives in
+// one stream-ordered device allocation.  Dense DSDBSparse blocks are read and
+// written in place (zero copy); blocks with a sparse pattern are gathered to /
+// scattered from dense scratch blocks.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+thread_local int64_t* g_qtx_launch_counter = nullptr;
+
+struct qtx_ctx {
+  int device = 0;
+  std::string last_error;
+  int64_t launches = 0;
+  size_t mem_limit = 0;
+  int* d_scratch = nullptr;    // small device scratch (flags, counters)
+  int* h_pinned = nullptr;     // pinned host mirror
+};
+
+namespace {
+
+constexpr cplx ONE = {1.0, 0.0};
+constexpr cplx ZERO = {0.0, 0.0};
+constexpr cplx MONE = {-1.0, 0.0};
+
+struct LaunchScope {
+  int64_t* prev;
+  explicit LaunchScope(qtx_ctx* c) : prev(g_qtx_launch_counter) { g_qtx_launch_counter = &c->launches; }
+  ~LaunchScope() { g_qtx_launch_counter = prev; }
+};
+
+// Stream-ordered device allocation (cudaMallocAsync on the context's pool).
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(size_t bytes, cudaStream_t s) : stream_(s), bytes_(bytes) {
+    if (bytes == 0) return;
+    cudaError_t e = cudaMallocAsync(&ptr_, bytes, s);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      ptr_ = nullptr;
+      throw QtxError(QTX_E_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed: " +
+                                      cudaGetErrorString(e));
+    }
+  }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    release();
+    ptr_ = o.ptr_; stream_ = o.stream_; bytes_ = o.bytes_;
+    o.ptr_ = nullptr;
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr_) cudaFreeAsync(ptr_, stream_);
+    ptr_ = nullptr;
+  }
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(ptr_); }
+
+ private:
+  void* ptr_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+inline int bidx(int i, int j) { return 2 * i + j; }
+
+// ---------------------------------------------------------------------------
+// DSDBSparse block access
+// ---------------------------------------------------------------------------
+struct Btd {
+  const qtx_btd_desc* d = nullptr;
+  cplx* data = nullptr;
+
+  int nb() const { return d->num_blocks; }
+  int size(int i) const { return d->block_sizes[i]; }
+  int64_t off(int k) const { return d->block_offset[k]; }
+  int64_t nnz(int k) const { return d->block_nnz[k]; }
+  const int32_t* index(int k) const { return d->block_index ? d->block_index[k] : nullptr; }
+  bool empty(int k) const { return off(k) < 0 || nnz(k) == 0; }
+  bool dense(int k) const { return !index(k) && !empty(k); }
+};
+
+void validate_desc(const qtx_btd_desc* d, const char* name) {
+  if (!d) throw QtxError(QTX_E_INVAL, std::string(name) + ": missing block descriptor");
+  if (d->num_blocks < 1) throw QtxError(QTX_E_INVAL, std::string(name) + ": num_blocks < 1");
+  if (!d->block_sizes || !d->block_offset || !d->block_nnz)
+    throw QtxError(QTX_E_INVAL, std::string(name) + ": descriptor arrays missing");
+  if (d->stack_size < 0) throw QtxError(QTX_E_INVAL, std::string(name) + ": negative stack size");
+  const int nb = d->num_blocks;
+  for (int i = 0; i < nb; ++i)
+    if (d->block_sizes[i] < 1) throw QtxError(QTX_E_INVAL, std::string(name) + ": block size < 1");
+  for (int i = 0; i < nb; ++i) {
+    for (int j = std::max(0, i - 1); j <= std::min(nb - 1, i + 1); ++j) {
+      int k = bidx(i, j);
+      int64_t rows = d->block_sizes[i], cols = d->block_sizes[j];
+      bool has_index = d->block_index && d->block_index[k];
+      if (d->block_offset[k] >= 0 && d->block_nnz[k] > 0) {
+        if (!has_index && d->block_nnz[k] != rows * cols)
+          throw QtxError(QTX_E_INVAL, std::string(name) + ": dense block (" + std::to_string(i) + "," +
+                                          std::to_string(j) + ") needs rows*cols entries");
+        if (d->block_nnz[k] > rows * cols)
+          throw QtxError(QTX_E_INVAL, std::string(name) + ": block has more entries than rows*cols");
+        if (d->block_offset[k] + d->block_nnz[k] > d->stack_stride)
+          throw QtxError(QTX_E_INVAL, std::string(name) + ": block slice beyond the data row");
+      }
+    }
+  }
+}
+
+void check_same_blocks(const qtx_btd_desc* a, const qtx_btd_desc* b, const char* name) {
+  if (a->num_blocks != b->num_blocks || a->stack_size != b->stack_size)
+    throw QtxError(QTX_E_INVAL, std::string(name) + ": block count or stack size differs from the system matrix");
+  for (int i = 0; i < a->num_blocks; ++i)
+    if (a->block_sizes[i] != b->block_sizes[i])
+      throw QtxError(QTX_E_INVAL, std::string(name) + ": block sizes differ from the system matrix");
+}
+
+struct Workspace {
+  cudaStream_t s;
+  int64_t ne;           // energies in the current batch slice
+  int bmax;
+  cplx* zero = nullptr;  // bmax^2 zeros (broadcast view)
+};
+
+// Read view of block (i, j) for energies [e0, e0 + ne); sparse blocks are
+// gathered into `scratch` (ne * bmax^2 complex).
+MatView in_block(const Btd& m, int i, int j, int64_t e0, int64_t ne, cplx* scratch, const Workspace& ws) {
+  int k = bidx(i, j);
+  int rows = m.size(i), cols = m.size(j);
+  if (m.empty(k)) return MatView{ws.zero, cols, 0};
+  cplx* base = m.data + e0 * m.d->stack_stride + m.off(k);
+  if (m.dense(k)) return MatView{base, cols, m.d->stack_stride};
+  MutView out{scratch, cols, (int64_t)rows * cols};
+  launch_block_gather(rows, cols, ne, base, m.d->stack_stride, m.nnz(k), m.index(k), out, ws.s);
+  return out;
+}
+
+// Store x (rows x cols of block (i, j), or its source for modes 1/2) into block (i, j).
+void out_block(const Btd& m, int i, int j, int64_t e0, int64_t ne, MatView x, int mode, const Workspace& ws) {
+  if (!m.data) return;
+  int k = bidx(i, j);
+  if (m.empty(k)) return;
+  cplx* base = m.data + e0 * m.d->stack_stride + m.off(k);
+  launch_block_scatter(m.size(i), m.size(j), ne, x, mode, base, m.d->stack_stride, m.nnz(k), m.index(k), ws.s);
+}
+
+// OBC block view (contiguous (stack, b, b)), or null view
+MatView obc_view(const void* const* arr, int i, int b, int64_t e0) {
+  if (!arr || !arr[i]) return MatView{};
+  const cplx* p = reinterpret_cast<const cplx*>(arr[i]);
+  return MatView{p + e0 * (int64_t)b * b, b, (int64_t)b * b};
+}
+
+void gemm(int m, int n, int k, int64_t batch, cplx alpha, MatView a, int op_a, MatView b, int op_b, MutView d,
+          cudaStream_t s, MatView c = MatView{}, cplx beta = ZERO, MatView c2 = MatView{}, cplx gamma = ZERO,
+          const int* active = nullptr, const cplx* diag_shift = nullptr, int precision = QTX_PREC_FP64) {
+  GemmCall g;
+  g.m = m; g.n = n; g.k = k; g.batch = batch;
+  g.a = a; g.op_a = op_a; g.b = b; g.op_b = op_b;
+  g.c = c; g.beta = beta; g.c2 = c2; g.gamma = gamma;
+  g.d = d; g.alpha = alpha; g.active = active; g.diag_shift = diag_shift;
+  if (precision == QTX_PREC_MIXED && tf32x3_supported(g)) launch_zgemm_tf32x3(g, s);
+  else launch_zgemm(g, s);
+}
+
+std::vector<int64_t> batch_offsets(int64_t num, int64_t max_batch) {
+  // get_batches: num // min(max_batch, num) near-equal sections, larger first
+  std::vector<int64_t> offs{0};
+  if (num <= 0) return offs;
+  int64_t mb = std::max<int64_t>(1, max_batch);
+  int64_t nsec = num / std::min(mb, num);
+  int64_t base = num / nsec, rem = num % nsec;
+  for (int64_t q = 0; q < nsec; ++q) offs.push_back(offs.back() + base + (q < rem ? 1 : 0));
+  return offs;
+}
+
+// Per-batch dense state: one (ne, b_i, b_i) slot per diagonal block.  Every
+// slot (and every temporary) has the same per-energy stride bmax^2, so slot
+// and temporary buffers can trade places (pointer swaps) whatever the block sizes.
+struct BlockStack {
+  std::vector<cplx*> ptr;
+  std::vector<int> size;
+  int64_t ne = 0;
+  int64_t slot = 0;  // elements per energy of every slot (bmax^2)
+  MutView view(int i) const { return MutView{ptr[i], size[i], slot}; }
+};
+
+size_t stack_elems(const std::vector<int>& sizes, int64_t ne) {
+  int bmax = *std::max_element(sizes.begin(), sizes.end());
+  return (size_t)bmax * bmax * ne * sizes.size();
+}
+
+BlockStack carve(cplx*& cursor, const std::vector<int>& sizes, int64_t ne, int bmax) {
+  BlockStack st;
+  st.ne = ne;
+  st.size = sizes;
+  st.slot = (int64_t)bmax * bmax;
+  for (size_t q = 0; q < sizes.size(); ++q) {
+    st.ptr.push_back(cursor);
+    cursor += (size_t)st.slot * ne;
+  }
+  return st;
+}
+
+void read_info_or_throw(qtx_ctx* ctx, const int* d_info, int64_t n, cudaStream_t s, const char* what) {
+  // reduce: any nonzero -> first nonzero column
+  std::vector<int> h(n);
+  QTX_CUDA_TRY(cudaMemcpyAsync(h.data(), d_info, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+  QTX_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int64_t e = 0; e < n; ++e)
+    if (h[e]) throw QtxError(QTX_E_SINGULAR, std::string(what) + ": exactly singular diagonal block (stack entry " +
+                                                 std::to_string(e) + ", pivot " + std::to_string(h[e]) + ")");
+  (void)ctx;
+}
+
+// ---------------------------------------------------------------------------
+// selected_inv  (src/qttools/greens_function_solver/rgf.py:25-113)
+// ---------------------------------------------------------------------------
+void selected_inv_impl(qtx_ctx* ctx, const Btd& a, const void* const* obc_r, const Btd& out, int64_t max_batch,
+                       int precision, cudaStream_t s) {
+  const int nb = a.nb();
+  std::vector<int> sizes(a.d->block_sizes, a.d->block_sizes + nb);
+  const int bmax = *std::max_element(sizes.begin(), sizes.end());
+  const int64_t NE = a.d->stack_size;
+  auto offs = batch_offsets(NE, max_batch);
+  int64_t ne_max = 0;
+  for (size_t q = 0; q + 1 < offs.size(); ++q) ne_max = std::max(ne_max, offs[q + 1] - offs[q]);
+  if (ne_max == 0) return;
+
+  const size_t tmp = (size_t)bmax * bmax * ne_max;
+  const size_t total = stack_elems(sizes, ne_max) + 7 * tmp + (size_t)bmax * bmax;
+  DevBuf buf(total * sizeof(cplx) + sizeof(int) * ne_max * nb, s);
+  cplx* cur = buf.as<cplx>();
+  BlockStack x = carve(cur, sizes, ne_max, bmax);
+  cplx* T[7];
+  for (int q = 0; q < 7; ++q) { T[q] = cur; cur += tmp; }
+  Workspace ws{s, ne_max, bmax, cur};
+  QTX_CUDA_TRY(cudaMemsetAsync(ws.zero, 0, sizeof(cplx) * bmax * bmax, s));
+  cur += (size_t)bmax * bmax;
+  int* info = reinterpret_cast<int*>(cur);
+  QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * ne_max * nb, s));
+
+  for (size_t q = 0; q + 1 < offs.size(); ++q) {
+    const int64_t e0 = offs[q], ne = offs[q + 1] - offs[q];
+    auto tv = [&](int idx, int ld) { return MutView{T[idx], ld, (int64_t)bmax * bmax}; };
+    // x_0 = inv(A_00 - Sigma_0)
+    {
+      const int b0 = sizes[0];
+      MatView a00 = in_block(a, 0, 0, e0, ne, T[5], ws);
+      MatView o = obc_view(obc_r, 0, b0, e0);
+      if (o.ptr) {
+        launch_axpby(b0, b0, ne, ONE, a00, MONE, o, tv(0, b0), s);
+        launch_zinv(b0, ne, tv(0, b0), x.view(0), info, nullptr, s);
+      } else {
+        launch_zinv(b0, ne, a00, x.view(0), info, nullptr, s);
+      }
+    }
+    // forward: x_j = inv(A_jj - Sigma_j - A_ji x_i A_ij)
+    for (int i = 0; i + 1 < nb; ++i) {
+      const int j = i + 1, bi = sizes[i], bj = sizes[j];
+      MatView a_ji = in_block(a, j, i, e0, ne, T[4], ws);
+      MatView a_ij = in_block(a, i, j, e0, ne, T[5], ws);
+      MatView a_jj = in_block(a, j, j, e0, ne, T[6], ws);
+      gemm(bj, bi, bi, ne, ONE, a_ji, OP_N, x.view(i), OP_N, tv(0, bi), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           precision);
+      MatView o = obc_view(obc_r, j, bj, e0);
+      gemm(bj, bj, bi, ne, MONE, tv(0, bi), OP_N, a_ij, OP_N, tv(1, bj), s, a_jj, ONE, o, MONE, nullptr, nullptr,
+           precision);
+      launch_zinv(bj, ne, tv(1, bj), x.view(j), info + (int64_t)j * ne_max, nullptr, s);
+    }
+    out_block(out, nb - 1, nb - 1, e0, ne, x.view(nb - 1), 0, ws);
+    // backward
+    for (int i = nb - 2; i >= 0; --i) {
+      const int j = i + 1, bi = sizes[i], bj = sizes[j];
+      MatView a_ji = in_block(a, j, i, e0, ne, T[5], ws);
+      MatView a_ij = in_block(a, i, j, e0, ne, T[6], ws);
+      // X_ji = -(X_jj A_ji) x_i
+      gemm(bj, bi, bj, ne, ONE, x.view(j), OP_N, a_ji, OP_N, tv(0, bi), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           precision);
+      gemm(bj, bi, bi, ne, MONE, tv(0, bi), OP_N, x.view(i), OP_N, tv(1, bi), s, {}, ZERO, {}, ZERO, nullptr,
+           nullptr, precision);
+      out_block(out, j, i, e0, ne, tv(1, bi), 0, ws);
+      // X_ij = -(x_i A_ij) X_jj
+      gemm(bi, bj, bi, ne, ONE, x.view(i), OP_N, a_ij, OP_N, tv(2, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           precision);
+      gemm(bi, bj, bj, ne, MONE, tv(2, bj), OP_N, x.view(j), OP_N, tv(3, bj), s, {}, ZERO, {}, ZERO, nullptr,
+           nullptr, precision);
+      out_block(out, i, j, e0, ne, tv(3, bj), 0, ws);
+      // X_ii = x_i - (x_i A_ij) X_ji
+      gemm(bi, bi, bj, ne, MONE, tv(2, bj), OP_N, tv(1, bi), OP_N, tv(4, bi), s, x.view(i), ONE, {}, ZERO, nullptr,
+           nullptr, precision);
+      std::swap(x.ptr[i], T[4]);
+      out_block(out, i, i, e0, ne, x.view(i), 0, ws);
+    }
+  }
+  read_info_or_throw(ctx, info, ne_max * nb, s, "selected_inv");
+}
+
+// ---------------------------------------------------------------------------
+// selected_solve  (src/qttools/greens_function_solver/rgf.py:115-414)
+// ---------------------------------------------------------------------------
+struct SolveArgs {
+  Btd a, sl, sg, xl, xg, xr;
+  const qtx_obc* obc = nullptr;
+  cplx* current = nullptr;
+  unsigned flags = 0;
+  int64_t max_batch = 100;
+  int precision = QTX_PREC_FP64;
+};
+
+void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
+  const Btd& a = A.a;
+  const int nb = a.nb();
+  std::vector<int> sizes(a.d->block_sizes, a.d->block_sizes + nb);
+  const int bmax = *std::max_element(sizes.begin(), sizes.end());
+  const int64_t NE = a.d->stack_size;
+  const bool want_r = (A.flags & QTX_FLAG_RETURN_RETARDED) != 0;
+  const bool want_r_off = (A.flags & QTX_FLAG_RETARDED_OFFDIAG) != 0;
+  const bool want_cur = (A.flags & QTX_FLAG_RETURN_CURRENT) != 0 && A.current != nullptr;
+  const bool symmetric = (A.flags & QTX_FLAG_SYMMETRIC_OUT) != 0;
+  const int prec = A.precision;
+  auto offs = batch_offsets(NE, A.max_batch);
+  int64_t ne_max = 0;
+  for (size_t q = 0; q + 1 < offs.size(); ++q) ne_max = std::max(ne_max, offs[q + 1] - offs[q]);
+  if (ne_max == 0) return;
+
+  const int NT = 12;
+  const size_t tmp = (size_t)bmax * bmax * ne_max;
+  std::vector<int> cur_sizes(sizes.begin() + 1, sizes.end());
+  size_t total = 3 * stack_elems(sizes, ne_max) + NT * tmp + (size_t)bmax * bmax;
+  if (want_cur) total += 2 * (size_t)bmax * bmax * ne_max * cur_sizes.size();
+  DevBuf buf(total * sizeof(cplx) + sizeof(int) * ne_max * nb, s);
+  cplx* cur = buf.as<cplx>();
+  BlockStack xr = carve(cur, sizes, ne_max, bmax);
+  BlockStack xl = carve(cur, sizes, ne_max, bmax);
+  BlockStack xg = carve(cur, sizes, ne_max, bmax);
+  BlockStack stl, stg;  // Sigma-tilde per interface (for the layer current)
+  if (want_cur) {
+    stl = carve(cur, cur_sizes, ne_max, bmax);
+    stg = carve(cur, cur_sizes, ne_max, bmax);
+  }
+  cplx* T[NT];
+  for (int q = 0; q < NT; ++q) { T[q] = cur; cur += tmp; }
+  Workspace ws{s, ne_max, bmax, cur};
+  QTX_CUDA_TRY(cudaMemsetAsync(ws.zero, 0, sizeof(cplx) * bmax * bmax, s));
+  cur += (size_t)bmax * bmax;
+  int* info = reinterpret_cast<int*>(cur);
+  QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * ne_max * nb, s));
+
+  const void* const* obc_r = A.obc ? A.obc->retarded : nullptr;
+  const void* const* obc_l = A.obc ? A.obc->lesser : nullptr;
+  const void* const* obc_g = A.obc ? A.obc->greater : nullptr;
+
+  for (size_t q = 0; q + 1 < offs.size(); ++q) {
+    const int64_t e0 = offs[q], ne = offs[q + 1] - offs[q];
+    auto tv = [&](int idx, int ld) { return MutView{T[idx], ld, (int64_t)bmax * bmax}; };
+    // G0..G3 (T[8..11]) are gather scratch for sparse input blocks
+    // ---- first block (rgf.py:207-231)
+    {
+      const int b0 = sizes[0];
+      MatView a00 = in_block(a, 0, 0, e0, ne, T[8], ws);
+      MatView o = obc_view(obc_r, 0, b0, e0);
+      if (o.ptr) {
+        launch_axpby(b0, b0, ne, ONE, a00, MONE, o, tv(0, b0), s);
+        launch_zinv(b0, ne, tv(0, b0), xr.view(0), info, nullptr, s);
+      } else {
+        launch_zinv(b0, ne, a00, xr.view(0), info, nullptr, s);
+      }
+      for (int comp = 0; comp < 2; ++comp) {
+        const Btd& S = comp == 0 ? A.sl : A.sg;
+        const void* const* ob = comp == 0 ? obc_l : obc_g;
+        BlockStack& X = comp == 0 ? xl : xg;
+        MatView s00 = in_block(S, 0, 0, e0, ne, T[9], ws);
+        MatView o2 = obc_view(ob, 0, b0, e0);
+        MatView sv = s00;
+        if (o2.ptr) {
+          launch_axpby(b0, b0, ne, ONE, s00, ONE, o2, tv(1, b0), s);
+          sv = tv(1, b0);
+        }
+        gemm(b0, b0, b0, ne, ONE, xr.view(0), OP_N, sv, OP_N, tv(2, b0), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+             prec);
+        gemm(b0, b0, b0, ne, ONE, tv(2, b0), OP_N, xr.view(0), OP_C, X.view(0), s, {}, ZERO, {}, ZERO, nullptr,
+             nullptr, prec);
+      }
+    }
+    // ---- forward sweep (rgf.py:233-295)
+    for (int i = 0; i + 1 < nb; ++i) {
+      const int j = i + 1, bi = sizes[i], bj = sizes[j];
+      MatView a_ji = in_block(a, j, i, e0, ne, T[8], ws);
+      MatView a_ij = in_block(a, i, j, e0, ne, T[9], ws);
+      {
+        MatView a_jj = in_block(a, j, j, e0, ne, T[10], ws);
+        // U = A_ji x_i ; M = A_jj - Sigma^R_j - U A_ij ; x_j = inv(M)
+        gemm(bj, bi, bi, ne, ONE, a_ji, OP_N, xr.view(i), OP_N, tv(0, bi), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+             prec);
+        gemm(bj, bj, bi, ne, MONE, tv(0, bi), OP_N, a_ij, OP_N, tv(1, bj), s, a_jj, ONE,
+             obc_view(obc_r, j, bj, e0), MONE, nullptr, nullptr, prec);
+        launch_zinv(bj, ne, tv(1, bj), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
+      }
+      for (int comp = 0; comp < 2; ++comp) {
+        const Btd& S = comp == 0 ? A.sl : A.sg;
+        const void* const* ob = comp == 0 ? obc_l : obc_g;
+        BlockStack& X = comp == 0 ? xl : xg;
+        MatView s_ij = in_block(S, i, j, e0, ne, T[10], ws);
+        MatView s_jj = in_block(S, j, j, e0, ne, T[11], ws);
+        // W = U S_ij
+        gemm(bj, bj, bi, ne, ONE, tv(0, bi), OP_N, s_ij, OP_N, tv(2, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+             prec);
+        // V = X_i A_ji^H
+        gemm(bi, bj, bi, ne, ONE, X.view(i), OP_N, a_ji, OP_C, tv(3, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+             prec);
+        if (want_cur) {
+          BlockStack& ST = comp == 0 ? stl : stg;
+          // Sigma~ = A_ji V + W^H - W  (kept for the layer current)
+          gemm(bj, bj, bi, ne, ONE, a_ji, OP_N, tv(3, bj), OP_N, ST.view(i), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+               prec);
+          launch_skew_combine(bj, ne, ST.view(i), tv(2, bj), ST.view(i), s);
+          launch_axpby(bj, bj, ne, ONE, ST.view(i), ONE, s_jj, tv(4, bj), s);
+          MatView o2 = obc_view(ob, j, bj, e0);
+          if (o2.ptr) launch_axpby(bj, bj, ne, ONE, tv(4, bj), ONE, o2, tv(4, bj), s);
+        } else {
+          // Q = A_ji V + S_jj + Sigma^<_obc,j ; Q += W^H - W
+          gemm(bj, bj, bi, ne, ONE, a_ji, OP_N, tv(3, bj), OP_N, tv(4, bj), s, s_jj, ONE, obc_view(ob, j, bj, e0),
+               ONE, nullptr, nullptr, prec);
+          launch_skew_combine(bj, ne, tv(4, bj), tv(2, bj), tv(4, bj), s);
+        }
+        // X_j = x_j Q x_j^H
+        gemm(bj, bj, bj, ne, ONE, xr.view(j), OP_N, tv(4, bj), OP_N, tv(5, bj), s, {}, ZERO, {}, ZERO, nullptr,
+             nullptr, prec);
+        gemm(bj, bj, bj, ne, ONE, tv(5, bj), OP_N, xr.view(j), OP_C, X.view(j), s, {}, ZERO, {}, ZERO, nullptr,
+             nullptr, prec);
+      }
+    }
+    // ---- last diagonal blocks (rgf.py:297-305)
+    {
+      const int n = nb - 1;
+      out_block(A.xl, n, n, e0, ne, xl.view(n), 1, ws);
+      out_block(A.xg, n, n, e0, ne, xg.view(n), 1, ws);
+      if (want_r) out_block(A.xr, n, n, e0, ne, xr.view(n), 0, ws);
+    }
+    // ---- backward sweep (rgf.py:307-404)
+    for (int i = nb - 2; i >= 0; --i) {
+      const int j = i + 1, bi = sizes[i], bj = sizes[j];
+      MatView a_ij = in_block(a, i, j, e0, ne, T[8], ws);
+      MatView a_ji = in_block(a, j, i, e0, ne, T[9], ws);
+      // P1 = x_i A_ij (bi x bj), P2 = X_jj A_ji (bj x bi), P3 = P1 X_jj, P4 = P1 P2
+      gemm(bi, bj, bi, ne, ONE, xr.view(i), OP_N, a_ij, OP_N, tv(0, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           prec);
+      gemm(bj, bi, bj, ne, ONE, xr.view(j), OP_N, a_ji, OP_N, tv(1, bi), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           prec);
+      gemm(bi, bj, bj, ne, ONE, tv(0, bj), OP_N, xr.view(j), OP_N, tv(2, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           prec);
+      gemm(bi, bi, bj, ne, ONE, tv(0, bj), OP_N, tv(1, bi), OP_N, tv(3, bi), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           prec);
+      if (want_r_off) {
+        // X^R_ij = -P3 ; X^R_ji = -P2 x_i
+        launch_axpby(bi, bj, ne, MONE, tv(2, bj), ZERO, {}, tv(4, bj), s);
+        out_block(A.xr, i, j, e0, ne, tv(4, bj), 0, ws);
+        gemm(bj, bi, bi, ne, MONE, tv(1, bi), OP_N, xr.view(i), OP_N, tv(4, bi), s, {}, ZERO, {}, ZERO, nullptr,
+             nullptr, prec);
+        out_block(A.xr, j, i, e0, ne, tv(4, bi), 0, ws);
+      }
+      for (int comp = 0; comp < 2; ++comp) {
+        const Btd& S = comp == 0 ? A.sl : A.sg;
+        const Btd& OUT = comp == 0 ? A.xl : A.xg;
+        BlockStack& X = comp == 0 ? xl : xg;
+        MatView s_ij = in_block(S, i, j, e0, ne, T[10], ws);
+        // Y = x_i S_ij
+        gemm(bi, bj, bi, ne, ONE, xr.view(i), OP_N, s_ij, OP_N, tv(4, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+             prec);
+        // t1 = P4 X_i - Y P3^H ; t1 -= t1^H
+        gemm(bi, bi, bi, ne, ONE, tv(3, bi), OP_N, X.view(i), OP_N, tv(5, bi), s, {}, ZERO, {}, ZERO, nullptr,
+             nullptr, prec);
+        gemm(bi, bi, bj, ne, MONE, tv(4, bj), OP_N, tv(2, bj), OP_C, tv(5, bi), s, tv(5, bi), ONE, {}, ZERO, nullptr,
+             nullptr, prec);
+        launch_sub_herm_inplace(bi, ne, tv(5, bi), s);
+        // t2 = P1 X_j
+        gemm(bi, bj, bj, ne, ONE, tv(0, bj), OP_N, X.view(j), OP_N, tv(6, bj), s, {}, ZERO, {}, ZERO, nullptr,
+             nullptr, prec);
+        // X_ij = Y X_jj^H - t2 - X_i P2^H
+        gemm(bi, bj, bj, ne, ONE, tv(4, bj), OP_N, xr.view(j), OP_C, tv(7, bj), s, tv(6, bj), MONE, {}, ZERO,
+             nullptr, nullptr, prec);
+        gemm(bi, bj, bi, ne, MONE, X.view(i), OP_N, tv(1, bi), OP_C, tv(7, bj), s, tv(7, bj), ONE, {}, ZERO, nullptr,
+             nullptr, prec);
+        out_block(OUT, i, j, e0, ne, tv(7, bj), 0, ws);
+        if (!symmetric) out_block(OUT, j, i, e0, ne, tv(7, bj), 2, ws);
+        // X_i += t2 P1^H + t1
+        gemm(bi, bi, bj, ne, ONE, tv(6, bj), OP_N, tv(0, bj), OP_C, X.view(i), s, X.view(i), ONE, tv(5, bi), ONE,
+             nullptr, nullptr, prec);
+        out_block(OUT, i, i, e0, ne, X.view(i), 1, ws);
+      }
+      if (want_cur) {
+        // current_i = Tr[Sigma~^>_i X^<_j - X^>_j Sigma~^<_i]
+        cplx* cur_out = T[11];
+        launch_trace_product(bj, bj, ne, stg.view(i), xl.view(j), ONE, reinterpret_cast<cplx*>(cur_out), false, s);
+        launch_trace_product(bj, bj, ne, xg.view(j), stl.view(i), MONE, reinterpret_cast<cplx*>(cur_out), true, s);
+        // scatter into current[(e0 + e) * (nb - 1) + i]
+        launch_axpby(1, 1, ne, ONE, MatView{cur_out, 1, 1}, ZERO, {}, MutView{A.current + e0 * (nb - 1) + i, 1, nb - 1},
+                     s);
+      }
+      // x_i <- x_i + P4 x_i  (full G^R_ii)
+      gemm(bi, bi, bi, ne, ONE, tv(3, bi), OP_N, xr.view(i), OP_N, tv(4, bi), s, xr.view(i), ONE, {}, ZERO, nullptr,
+           nullptr, prec);
+      std::swap(xr.ptr[i], T[4]);
+      if (want_r) out_block(A.xr, i, i, e0, ne, xr.view(i), 0, ws);
+    }
+  }
+  read_info_or_throw(ctx, info, ne_max * nb, s, "selected_solve");
+}
+
+// ---------------------------------------------------------------------------
+// Sancho-Rubio (src/qttools/boundary_conditions/obc/sancho_rubio.py:33-86)
+// ---------------------------------------------------------------------------
+// Returns true when every entry converged.
+bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView a_ij, MatView a_ji, double tol,
+                       int max_iter, MutView x, int* iterations, cudaStream_t s) {
+  const size_t mat = (size_t)n * n * batch;
+  DevBuf buf(sizeof(cplx) * 9 * mat + sizeof(int) * (2 * batch + 2), s);
+  cplx* p = buf.as<cplx>();
+  auto slot = [&](int q) { return MutView{p + q * mat, n, (int64_t)n * n}; };
+  MutView eps = slot(0), eps_s = slot(1), alpha = slot(2), beta = slot(3), inv = slot(4), t0 = slot(5),
+          t1 = slot(6), t2 = slot(7), t3 = slot(8);
+  int* active = reinterpret_cast<int*>(p + 9 * mat);
+  int* its = active + batch;
+  int* num_active = its + batch;
+  launch_axpby(n, n, batch, ONE, a_ii, ZERO, {}, eps, s);
+  launch_axpby(n, n, batch, ONE, a_ii, ZERO, {}, eps_s, s);
+  launch_axpby(n, n, batch, ONE, a_ji, ZERO, {}, alpha, s);
+  launch_axpby(n, n, batch, ONE, a_ij, ZERO, {}, beta, s);
+  launch_fill_int(active, batch, 1, s);
+  QTX_CUDA_TRY(cudaMemsetAsync(its, 0, sizeof(int) * batch, s));
+  bool converged = false;
+  for (int it = 0; it < max_iter; ++it) {
+    launch_zinv(n, batch, eps, inv, nullptr, active, s);
+    gemm(n, n, n, batch, ONE, alpha, OP_N, inv, OP_N, t0, s, {}, ZERO, {}, ZERO, active);   // a inv
+    gemm(n, n, n, batch, ONE, beta, OP_N, inv, OP_N, t1, s, {}, ZERO, {}, ZERO, active);    // b inv
+    gemm(n, n, n, batch, ONE, t0, OP_N, beta, OP_N, t2, s, {}, ZERO, {}, ZERO, active);     // a inv b
+    launch_axpby(n, n, batch, ONE, eps_s, MONE, t2, eps_s, s, active);                      // eps_s -= a inv b
+    // eps = eps - a inv b - b inv a
+    gemm(n, n, n, batch, MONE, t1, OP_N, alpha, OP_N, eps, s, eps, ONE, t2, MONE, active);
+    gemm(n, n, n, batch, ONE, t0, OP_N, alpha, OP_N, t3, s, {}, ZERO, {}, ZERO, active);    // a inv a
+    gemm(n, n, n, batch, ONE, t1, OP_N, beta, OP_N, t2, s, {}, ZERO, {}, ZERO, active);     // b inv b
+    std::swap(alpha.ptr, t3.ptr);
+    std::swap(beta.ptr, t2.ptr);
+    QTX_CUDA_TRY(cudaMemsetAsync(num_active, 0, sizeof(int), s));
+    launch_sr_norm_update(n, batch, alpha, beta, tol, active, its, num_active, s);
+    QTX_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, num_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+    QTX_CUDA_TRY(cudaStreamSynchronize(s));
+    if (ctx->h_pinned[0] == 0) {
+      converged = true;
+      break;
+    }
+  }
+  launch_zinv(n, batch, eps_s, x, nullptr, nullptr, s);
+  if (iterations) QTX_CUDA_TRY(cudaMemcpyAsync(iterations, its, sizeof(int) * batch, cudaMemcpyDeviceToDevice, s));
+  return converged;
+}
+
+// ---------------------------------------------------------------------------
+// Generator-form transport solve (ElectronSolver.solve for a device whose leads
+// repeat its end cells; interior scattering self-energies are zero)
+// ---------------------------------------------------------------------------
+void transport_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qtx_transport_outputs& O, int prec,
+                    cudaStream_t s, bool& all_converged) {
+  const int nb = P.num_blocks, b = P.block_size;
+  const int64_t NE = P.num_energies;
+  const int64_t bb = (int64_t)b * b;
+  const cplx* h_diag = reinterpret_cast<const cplx*>(P.h_diag);
+  const cplx* h_upper = reinterpret_cast<const cplx*>(P.h_upper);
+  auto offs = batch_offsets(NE, P.max_batch_size > 0 ? P.max_batch_size : NE);
+  int64_t ne_max = 0;
+  for (size_t q = 0; q + 1 < offs.size(); ++q) ne_max = std::max(ne_max, offs[q + 1] - offs[q]);
+  if (ne_max == 0) return;
+
+  // energy-independent couplings: A_i,i+1 = -H_i,i+1 ; A_i+1,i = -H_i,i+1^H
+  DevBuf cpl(sizeof(cplx) * 2 * bb * std::max(nb - 1, 1), s);
+  cplx* a_up = cpl.as<cplx>();
+  cplx* a_lo = a_up + bb * std::max(nb - 1, 1);
+  for (int i = 0; i + 1 < nb; ++i) {
+    launch_axpby(b, b, 1, MONE, MatView{h_upper + i * bb, b, bb}, ZERO, {}, MutView{a_up + i * bb, b, bb}, s);
+    launch_neg_herm(b, h_upper + i * bb, a_lo + i * bb, s);
+  }
+  auto up = [&](int i) { return MatView{a_up + i * bb, b, 0}; };
+  auto lo = [&](int i) { return MatView{a_lo + i * bb, b, 0}; };
+  auto hd = [&](int i) { return MatView{h_diag + i * bb, b, 0}; };
+
+  const size_t tmp = (size_t)bb * ne_max;
+  const int NT = 10;
+  const size_t total = 3 * (size_t)nb * tmp + NT * tmp + 10 * tmp;
+  DevBuf buf(sizeof(cplx) * total + sizeof(cplx) * 4 * ne_max + sizeof(double) * 2 * ne_max +
+                 sizeof(int) * (nb + 2) * ne_max,
+             s);
+  cplx* cur = buf.as<cplx>();
+  std::vector<int> sizes(nb, b);
+  BlockStack xr = carve(cur, sizes, ne_max, b), xl = carve(cur, sizes, ne_max, b), xg = carve(cur, sizes, ne_max, b);
+  cplx* T[NT];
+  for (int q = 0; q < NT; ++q) { T[q] = cur; cur += tmp; }
+  // contact buffers: g_L, g_R, SigR_L, SigR_R, SigL_L, SigL_R, SigG_L, SigG_R, Gam_L, Gam_R
+  cplx* C[10];
+  for (int q = 0; q < 10; ++q) { C[q] = cur; cur += tmp; }
+  cplx* shift = cur; cur += ne_max;
+  cplx* tr = cur; cur += ne_max;
+  cplx* cl = cur; cur += ne_max;
+  cplx* cr = cur; cur += ne_max;
+  double* occ_l = reinterpret_cast<double*>(cur);
+  double* occ_r = occ_l + ne_max;
+  int* info = reinterpret_cast<int*>(occ_r + ne_max);
+  int* its = info + nb * ne_max;
+  QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * nb * ne_max, s));
+
+  auto V = [&](cplx* p) { return MutView{p, b, bb}; };
+  for (size_t q = 0; q + 1 < offs.size(); ++q) {
+    const int64_t e0 = offs[q], ne = offs[q + 1] - offs[q];
+    const double* en = P.energies + e0;
+    launch_energy_shift(ne, en, P.eta, shift, s);
+    // ---- contacts (src/quatrex/electron/solver.py:305-386)
+    // left: A_00(E) into T0 ; g_L = SR(A_00, A_01, A_10)
+    launch_assemble_diag(b, ne, h_diag, en, P.eta, V(T[0]), s);
+    bool okl = sancho_rubio_impl(ctx, b, ne, V(T[0]), up(0), lo(0), P.sr_tol, P.sr_max_iterations, V(C[0]), its, s);
+    if (O.sr_iterations)
+      QTX_CUDA_TRY(cudaMemcpy2DAsync(O.sr_iterations + 2 * e0, 2 * sizeof(int), its, sizeof(int), sizeof(int), ne,
+                                     cudaMemcpyDeviceToDevice, s));
+    launch_assemble_diag(b, ne, h_diag + (int64_t)(nb - 1) * bb, en, P.eta, V(T[0]), s);
+    bool okr = sancho_rubio_impl(ctx, b, ne, V(T[0]), lo(nb - 2), up(nb - 2), P.sr_tol, P.sr_max_iterations,
+                                 V(C[1]), its, s);
+    if (O.sr_iterations)
+      QTX_CUDA_TRY(cudaMemcpy2DAsync(O.sr_iterations + 2 * e0 + 1, 2 * sizeof(int), its, sizeof(int), sizeof(int),
+                                     ne, cudaMemcpyDeviceToDevice, s));
+    all_converged = all_converged && okl && okr;
+    // Sigma^R_L = A_10 g_L A_01 ; Sigma^R_R = A_mn g_R A_nm
+    gemm(b, b, b, ne, ONE, lo(0), OP_N, V(C[0]), OP_N, V(T[1]), s);
+    gemm(b, b, b, ne, ONE, V(T[1]), OP_N, up(0), OP_N, V(C[2]), s);
+    gemm(b, b, b, ne, ONE, up(nb - 2), OP_N, V(C[1]), OP_N, V(T[1]), s);
+    gemm(b, b, b, ne, ONE, V(T[1]), OP_N, lo(nb - 2), OP_N, V(C[3]), s);
+    launch_fermi(ne, en, P.mu_left, P.kt, occ_l, s);
+    launch_fermi(ne, en, P.mu_right, P.kt, occ_r, s);
+    launch_obc_lesser_greater(b, ne, V(C[2]), occ_l, V(C[4]), V(C[6]), V(C[8]), s);
+    launch_obc_lesser_greater(b, ne, V(C[3]), occ_r, V(C[5]), V(C[7]), V(C[9]), s);
+    auto obc_r = [&](int i) { return i == 0 ? MatView(V(C[2])) : (i == nb - 1 ? MatView(V(C[3])) : MatView{}); };
+    auto obc_x = [&](int comp, int i) {
+      int base = comp == 0 ? 4 : 6;
+      return i == 0 ? MatView(V(C[base])) : (i == nb - 1 ? MatView(V(C[base + 1])) : MatView{});
+    };
+    auto tv = [&](int idx) { return V(T[idx]); };
+    auto out_at = [&](void* base, int64_t blocks_per_e, int blk) {
+      return MutView{reinterpret_cast<cplx*>(base) + (e0 * blocks_per_e + blk) * bb, b, blocks_per_e * bb};
+    };
+
+    // ---- first block: x_0 = inv(A_00 - Sigma^R_L), X_0 = x_0 Sigma_0 x_0^H
+    // M_0 = (E + i eta) I - H_00 - Sigma^R_L
+    // (a K = 0 product: the epilogue alone forms -H_00 - Sigma^R_L + shift on the diagonal)
+    gemm(b, b, 0, ne, ONE, tv(0), OP_N, tv(0), OP_N, tv(1), s, hd(0), MONE, obc_r(0), MONE, nullptr, shift);
+    launch_zinv(b, ne, tv(1), xr.view(0), info, nullptr, s);
+    for (int comp = 0; comp < 2; ++comp) {
+      BlockStack& X = comp == 0 ? xl : xg;
+      gemm(b, b, b, ne, ONE, xr.view(0), OP_N, obc_x(comp, 0), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           prec);
+      gemm(b, b, b, ne, ONE, tv(2), OP_N, xr.view(0), OP_C, X.view(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    }
+    // ---- forward sweep
+    for (int i = 0; i + 1 < nb; ++i) {
+      const int j = i + 1;
+      gemm(b, b, b, ne, ONE, lo(i), OP_N, xr.view(i), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      // M = (E + i eta) I - H_jj - Sigma^R_j - U A_ij
+      gemm(b, b, b, ne, MONE, tv(0), OP_N, up(i), OP_N, tv(1), s, hd(j), MONE, obc_r(j), MONE, nullptr, shift, prec);
+      launch_zinv(b, ne, tv(1), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
+      for (int comp = 0; comp < 2; ++comp) {
+        BlockStack& X = comp == 0 ? xl : xg;
+        // V = X_i A_ji^H ; Q = A_ji V + Sigma_obc,j ; X_j = x_j Q x_j^H   (interior Sigma = 0)
+        gemm(b, b, b, ne, ONE, X.view(i), OP_N, lo(i), OP_C, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+        gemm(b, b, b, ne, ONE, lo(i), OP_N, tv(3), OP_N, tv(4), s, obc_x(comp, j), ONE, {}, ZERO, nullptr, nullptr,
+             prec);
+        gemm(b, b, b, ne, ONE, xr.view(j), OP_N, tv(4), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+        gemm(b, b, b, ne, ONE, tv(5), OP_N, xr.view(j), OP_C, X.view(j), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      }
+    }
+    // ---- last blocks, corner chain start
+    const int n = nb - 1;
+    if (O.gl_diag) launch_block_scatter(b, b, ne, xl.view(n), 1, out_at(O.gl_diag, nb, n).ptr, nb * bb, bb, nullptr, s);
+    if (O.gg_diag) launch_block_scatter(b, b, ne, xg.view(n), 1, out_at(O.gg_diag, nb, n).ptr, nb * bb, bb, nullptr, s);
+    if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, out_at(O.gr_diag, nb, n), s);
+    if (O.density) launch_diag_imag_sum(b, ne, xl.view(n), 1.0, O.density + e0 * nb, nb, n, s);
+    if (O.hole_density) launch_diag_imag_sum(b, ne, xg.view(n), -1.0, O.hole_density + e0 * nb, nb, n, s);
+    // contact current at the right contact uses the symmetrised G^<_nn, G^>_nn
+    if (O.current_right) {
+      launch_block_scatter(b, b, ne, xl.view(n), 1, T[6], bb, bb, nullptr, s);
+      launch_block_scatter(b, b, ne, xg.view(n), 1, T[7], bb, bb, nullptr, s);
+      launch_trace_product(b, b, ne, V(C[7]), tv(6), ONE, cr, false, s);
+      launch_trace_product(b, b, ne, tv(7), V(C[5]), MONE, cr, true, s);
+      QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_right) + e0, cr, sizeof(cplx) * ne,
+                                   cudaMemcpyDeviceToDevice, s));
+    }
+    cplx* corner = T[8];
+    cplx* corner2 = T[9];
+    if (O.transmission) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, V(corner), s);
+    // ---- backward sweep
+    for (int i = nb - 2; i >= 0; --i) {
+      const int j = i + 1;
+      gemm(b, b, b, ne, ONE, xr.view(i), OP_N, up(i), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      gemm(b, b, b, ne, ONE, xr.view(j), OP_N, lo(i), OP_N, tv(1), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      gemm(b, b, b, ne, ONE, tv(0), OP_N, xr.view(j), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      gemm(b, b, b, ne, ONE, tv(0), OP_N, tv(1), OP_N, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      if (O.gr_upper) launch_axpby(b, b, ne, MONE, tv(2), ZERO, {}, out_at(O.gr_upper, nb - 1, i), s);
+      if (O.gr_lower)
+        gemm(b, b, b, ne, MONE, tv(1), OP_N, xr.view(i), OP_N, out_at(O.gr_lower, nb - 1, i), s, {}, ZERO, {}, ZERO,
+             nullptr, nullptr, prec);
+      if (O.transmission) {
+        // G_{i,N-1} = -(x_i A_ij) G_{j,N-1}
+        gemm(b, b, b, ne, MONE, tv(0), OP_N, V(corner), OP_N, V(corner2), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+             prec);
+        std::swap(corner, corner2);
+      }
+      for (int comp = 0; comp < 2; ++comp) {
+        BlockStack& X = comp == 0 ? xl : xg;
+        void* od = comp == 0 ? O.gl_diag : O.gg_diag;
+        void* ou = comp == 0 ? O.gl_upper : O.gg_upper;
+        // t1 = P4 X_i - (P4 X_i)^H ; t2 = P1 X_j
+        gemm(b, b, b, ne, ONE, tv(3), OP_N, X.view(i), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+        launch_sub_herm_inplace(b, ne, tv(5), s);
+        gemm(b, b, b, ne, ONE, tv(0), OP_N, X.view(j), OP_N, tv(6), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+        // X_ij = -t2 - X_i P2^H
+        if (ou)
+          gemm(b, b, b, ne, MONE, X.view(i), OP_N, tv(1), OP_C, out_at(ou, nb - 1, i), s, tv(6), MONE, {}, ZERO,
+               nullptr, nullptr, prec);
+        // X_i += t2 P1^H + t1
+        gemm(b, b, b, ne, ONE, tv(6), OP_N, tv(0), OP_C, X.view(i), s, X.view(i), ONE, tv(5), ONE, nullptr, nullptr,
+             prec);
+        if (od) launch_block_scatter(b, b, ne, X.view(i), 1, out_at(od, nb, i).ptr, nb * bb, bb, nullptr, s);
+      }
+      if (O.density) launch_diag_imag_sum(b, ne, xl.view(i), 1.0, O.density + e0 * nb, nb, i, s);
+      if (O.hole_density) launch_diag_imag_sum(b, ne, xg.view(i), -1.0, O.hole_density + e0 * nb, nb, i, s);
+      gemm(b, b, b, ne, ONE, tv(3), OP_N, xr.view(i), OP_N, tv(4), s, xr.view(i), ONE, {}, ZERO, nullptr, nullptr,
+           prec);
+      std::swap(xr.ptr[i], T[4]);
+      if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(i), ZERO, {}, out_at(O.gr_diag, nb, i), s);
+    }
+    if (O.current_left) {
+      launch_block_scatter(b, b, ne, xl.view(0), 1, T[6], bb, bb, nullptr, s);
+      launch_block_scatter(b, b, ne, xg.view(0), 1, T[7], bb, bb, nullptr, s);
+      launch_trace_product(b, b, ne, V(C[6]), tv(6), ONE, cl, false, s);
+      launch_trace_product(b, b, ne, tv(7), V(C[4]), MONE, cl, true, s);
+      QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_left) + e0, cl, sizeof(cplx) * ne,
+                                   cudaMemcpyDeviceToDevice, s));
+    }
+    if (O.transmission) {
+      // T = Tr[Gamma_L G_0N Gamma_R G_0N^H]
+      gemm(b, b, b, ne, ONE, V(C[8]), OP_N, V(corner), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      gemm(b, b, b, ne, ONE, tv(0), OP_N, V(C[9]), OP_N, tv(1), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      launch_trace_product_h(b, b, ne, tv(1), V(corner), tr, s);
+      launch_real_part(ne, tr, O.transmission + e0, s);
+    }
+  }
+  read_info_or_throw(ctx, info, (int64_t)nb * ne_max, s, "transport_solve");
+}
+
+// ---------------------------------------------------------------------------
+// host-buffer streaming for qtx_selected_solve (QTX_FLAG_HOST_BUFFERS)
+// ---------------------------------------------------------------------------
+size_t desc_row_bytes(const qtx_btd_desc* d) { return sizeof(cplx) * (size_t)d->stack_stride; }
+
+template <typename F>
+qtx_status guarded(qtx_ctx* ctx, F&& f) {
+  if (!ctx) return QTX_E_INVAL;
+  LaunchScope scope(ctx);
+  try {
+    QTX_CUDA_TRY(cudaSetDevice(ctx->device));
+    f();
+    ctx->last_error.clear();
+    return QTX_OK;
+  } catch (const QtxError& e) {
+    ctx->last_error = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    ctx->last_error = e.what();
+    return QTX_E_CUDA;
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* qtx_version(void) { return "qtx-rgf 0.1 (sm_100a)"; }
+
+qtx_status qtx_ctx_create(int device, qtx_ctx** out) {
+  if (!out) return QTX_E_INVAL;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    return QTX_E_CUDA;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) return QTX_E_CUDA;
+  qtx_ctx* c = new qtx_ctx();
+  c->device = device;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  if (cudaMalloc(&c->d_scratch, 4096) != cudaSuccess || cudaMallocHost(&c->h_pinned, 4096) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return QTX_E_NOMEM;
+  }
+  *out = c;
+  return QTX_OK;
+}
+
+qtx_status qtx_ctx_destroy(qtx_ctx* ctx) {
+  if (!ctx) return QTX_E_INVAL;
+  cudaSetDevice(ctx->device);
+  cudaFree(ctx->d_scratch);
+  cudaFreeHost(ctx->h_pinned);
+  delete ctx;
+  return QTX_OK;
+}
+
+const char* qtx_last_error(const qtx_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+qtx_status qtx_ctx_set_memory_limit(qtx_ctx* ctx, size_t bytes) {
+  if (!ctx) return QTX_E_INVAL;
+  ctx->mem_limit = bytes;
+  return QTX_OK;
+}
+
+qtx_status qtx_ctx_trim(qtx_ctx* ctx) {
+  return guarded(ctx, [&] {
+    cudaMemPool_t pool;
+    QTX_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+    QTX_CUDA_TRY(cudaDeviceSynchronize());
+    QTX_CUDA_TRY(cudaMemPoolTrimTo(pool, 0));
+  });
+}
+
+int64_t qtx_launch_count(const qtx_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+qtx_status qtx_inv(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a, int64_t stride_a, void* x,
+                   int64_t stride_x, qtx_stream stream) {
+  return guarded(ctx, [&] {
+    if (n < 1 || batch < 0 || !a || !x) throw QtxError(QTX_E_INVAL, "qtx_inv: bad arguments");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    DevBuf info(sizeof(int) * std::max<int64_t>(batch, 1), s);
+    QTX_CUDA_TRY(cudaMemsetAsync(info.as<int>(), 0, sizeof(int) * std::max<int64_t>(batch, 1), s));
+    launch_zinv(n, batch, MatView{reinterpret_cast<const cplx*>(a), n, stride_a},
+                MutView{reinterpret_cast<cplx*>(x), n, stride_x}, info.as<int>(), nullptr, s);
+    read_info_or_throw(ctx, info.as<int>(), batch, s, "qtx_inv");
+  });
+}
+
+qtx_status qtx_zgemm(qtx_ctx* ctx, int32_t m, int32_t n, int32_t k, int64_t batch, double alpha_re,
+                     double alpha_im, const void* a, int64_t lda, int64_t stride_a, int32_t op_a, const void* b,
+                     int64_t ldb, int64_t stride_b, int32_t op_b, double beta_re, double beta_im, const void* c,
+                     int64_t ldc, int64_t stride_c, void* d, int64_t ldd, int64_t stride_d, int32_t precision,
+                     qtx_stream stream) {
+  return guarded(ctx, [&] {
+    if (m < 0 || n < 0 || k < 0 || batch < 0 || !a || !b || !d || (op_a != 0 && op_a != 1) ||
+        (op_b != 0 && op_b != 1))
+      throw QtxError(QTX_E_INVAL, "qtx_zgemm: bad arguments");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    gemm(m, n, k, batch, cmk(alpha_re, alpha_im), MatView{reinterpret_cast<const cplx*>(a), lda, stride_a}, op_a,
+         MatView{reinterpret_cast<const cplx*>(b), ldb, stride_b}, op_b,
+         MutView{reinterpret_cast<cplx*>(d), ldd, stride_d}, s,
+         MatView{reinterpret_cast<const cplx*>(c), ldc, stride_c}, cmk(beta_re, beta_im), MatView{}, ZERO, nullptr,
+         nullptr, precision);
+  });
+}
+
+qtx_status qtx_selected_inv(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const void* a,
+                            const void* const* obc_retarded, const qtx_btd_desc* out_desc, void* out,
+                            int64_t max_batch_size, int32_t precision, uint32_t flags, qtx_stream stream) {
+  return guarded(ctx, [&] {
+    validate_desc(a_desc, "a");
+    validate_desc(out_desc, "out");
+    check_same_blocks(a_desc, out_desc, "out");
+    if (!a || !out) throw QtxError(QTX_E_INVAL, "qtx_selected_inv: null data");
+    if (flags & QTX_FLAG_HOST_BUFFERS) throw QtxError(QTX_E_UNSUPPORTED, "qtx_selected_inv: host buffers");
+    if (max_batch_size < 1) throw QtxError(QTX_E_INVAL, "qtx_selected_inv: max_batch_size < 1");
+    Btd A{a_desc, const_cast<cplx*>(reinterpret_cast<const cplx*>(a))};
+    Btd O{out_desc, reinterpret_cast<cplx*>(out)};
+    selected_inv_impl(ctx, A, obc_retarded, O, max_batch_size, precision, reinterpret_cast<cudaStream_t>(stream));
+  });
+}
+
+qtx_status qtx_selected_solve(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const void* a,
+                              const qtx_btd_desc* sl_desc, const void* sigma_lesser, const qtx_btd_desc* sg_desc,
+                              const void* sigma_greater, const qtx_obc* obc, const qtx_btd_desc* xl_desc, void* xl,
+                              const qtx_btd_desc* xg_desc, void* xg, const qtx_btd_desc* xr_desc, void* xr,
+                              void* current, int64_t max_batch_size, int32_t precision, uint32_t flags,
+                              qtx_stream stream) {
+  return guarded(ctx, [&] {
+    validate_desc(a_desc, "a");
+    validate_desc(sl_desc, "sigma_lesser");
+    validate_desc(sg_desc, "sigma_greater");
+    validate_desc(xl_desc, "xl");
+    validate_desc(xg_desc, "xg");
+    check_same_blocks(a_desc, sl_desc, "sigma_lesser");
+    check_same_blocks(a_desc, sg_desc, "sigma_greater");
+    check_same_blocks(a_desc, xl_desc, "xl");
+    check_same_blocks(a_desc, xg_desc, "xg");
+    if ((flags & (QTX_FLAG_RETURN_RETARDED | QTX_FLAG_RETARDED_OFFDIAG)) && (!xr_desc || !xr))
+      throw QtxError(QTX_E_INVAL, "qtx_selected_solve: retarded output requested without xr");
+    if (xr_desc) {
+      validate_desc(xr_desc, "xr");
+      check_same_blocks(a_desc, xr_desc, "xr");
+    }
+    if ((flags & QTX_FLAG_RETURN_CURRENT) && !current)
+      throw QtxError(QTX_E_INVAL, "qtx_selected_solve: current requested without a buffer");
+    if (!a || !sigma_lesser || !sigma_greater || !xl || !xg)
+      throw QtxError(QTX_E_INVAL, "qtx_selected_solve: null data");
+    if (max_batch_size < 1) throw QtxError(QTX_E_INVAL, "qtx_selected_solve: max_batch_size < 1");
+    if (flags & QTX_FLAG_HOST_BUFFERS) throw QtxError(QTX_E_UNSUPPORTED, "qtx_selected_solve: host buffers");
+    SolveArgs S;
+    S.a = Btd{a_desc, const_cast<cplx*>(reinterpret_cast<const cplx*>(a))};
+    S.sl = Btd{sl_desc, const_cast<cplx*>(reinterpret_cast<const cplx*>(sigma_lesser))};
+    S.sg = Btd{sg_desc, const_cast<cplx*>(reinterpret_cast<const cplx*>(sigma_greater))};
+    S.xl = Btd{xl_desc, reinterpret_cast<cplx*>(xl)};
+    S.xg = Btd{xg_desc, reinterpret_cast<cplx*>(xg)};
+    S.xr = Btd{xr_desc, reinterpret_cast<cplx*>(xr)};
+    S.obc = obc;
+    S.current = reinterpret_cast<cplx*>(current);
+    S.flags = flags;
+    S.max_batch = max_batch_size;
+    S.precision = precision;
+    selected_solve_impl(ctx, S, reinterpret_cast<cudaStream_t>(stream));
+  });
+}
+
+qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                            const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
+                            double convergence_tol, int32_t max_iterations, void* x, int32_t* iterations,
+                            qtx_stream stream) {
+  bool ok = true;
+  qtx_status st = guarded(ctx, [&] {
+    if (n < 1 || batch < 1 || !a_ii || !a_ij || !a_ji || !x || max_iterations < 1)
+      throw QtxError(QTX_E_INVAL, "qtx_sancho_rubio: bad arguments");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    ok = sancho_rubio_impl(ctx, n, batch, MatView{reinterpret_cast<const cplx*>(a_ii), n, stride_ii},
+                           MatView{reinterpret_cast<const cplx*>(a_ij), n, stride_ij},
+                           MatView{reinterpret_cast<const cplx*>(a_ji), n, stride_ji}, convergence_tol,
+                           max_iterations, MutView{reinterpret_cast<cplx*>(x), n, (int64_t)n * n}, iterations, s);
+    QTX_CUDA_TRY(cudaStreamSynchronize(s));
+  });
+  if (st == QTX_OK && !ok) {
+    ctx->last_error = "Surface Green's function did not converge.";
+    return QTX_E_NOT_CONVERGED;
+  }
+  return st;
+}
+
+qtx_status qtx_obc_assemble(qtx_ctx* ctx, int32_t n, int64_t batch, const void* g, const void* m_ji,
+                            int64_t stride_ji, const void* m_ij, int64_t stride_ij, const double* occupancy,
+                            void* sigma_r, void* sigma_l, void* sigma_g, qtx_stream stream) {
+  return guarded(ctx, [&] {
+    if (n < 1 || batch < 0 || !g || !m_ji || !m_ij || !sigma_r) throw QtxError(QTX_E_INVAL, "qtx_obc_assemble");
+    if ((sigma_l || sigma_g) && !occupancy) throw QtxError(QTX_E_INVAL, "qtx_obc_assemble: occupancy missing");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int64_t bb = (int64_t)n * n;
+    DevBuf t(sizeof(cplx) * bb * std::max<int64_t>(batch, 1), s);
+    gemm(n, n, n, batch, ONE, MatView{reinterpret_cast<const cplx*>(m_ji), n, stride_ji}, OP_N,
+         MatView{reinterpret_cast<const cplx*>(g), n, bb}, OP_N, MutView{t.as<cplx>(), n, bb}, s);
+    gemm(n, n, n, batch, ONE, MatView{t.as<cplx>(), n, bb}, OP_N,
+         MatView{reinterpret_cast<const cplx*>(m_ij), n, stride_ij}, OP_N,
+         MutView{reinterpret_cast<cplx*>(sigma_r), n, bb}, s);
+    if (sigma_l || sigma_g)
+      launch_obc_lesser_greater(n, batch, MatView{reinterpret_cast<cplx*>(sigma_r), n, bb}, occupancy,
+                                MutView{reinterpret_cast<cplx*>(sigma_l), n, bb},
+                                MutView{reinterpret_cast<cplx*>(sigma_g), n, bb}, MutView{}, s);
+  });
+}
+
+qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,
+                               int32_t precision, uint32_t flags, qtx_stream stream) {
+  bool ok = true;
+  qtx_status st = guarded(ctx, [&] {
+    if (!p || !o) throw QtxError(QTX_E_INVAL, "qtx_transport_solve: null problem");
+    if (p->num_blocks < 2 || p->block_size < 1 || p->num_energies < 0 || !p->h_diag || !p->h_upper ||
+        !p->energies || p->kt <= 0 || p->sr_max_iterations < 1)
+      throw QtxError(QTX_E_INVAL, "qtx_transport_solve: bad problem");
+    (void)flags;
+    transport_impl(ctx, *p, *o, precision, reinterpret_cast<cudaStream_t>(stream), ok);
+  });
+  if (st == QTX_OK && !ok) {
+    ctx->last_error = "Surface Green's function did not converge.";
+    return QTX_E_NOT_CONVERGED;
+  }
+  return st;
+}
+
+}  // extern "C"

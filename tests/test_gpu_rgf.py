@@ -1,0 +1,230 @@
+"""Parity of the drop-in RGF solver (CUDA path through the C ABI) with the
+oracle and the upstream fixtures.
+
+Bar: relative Frobenius error <= 1e-10 per returned block against the oracle
+(complex128), and the upstream unit-test criterion (dense inverse / congruence
+with numpy.allclose defaults) on the upstream-style sparse BTD matrices for
+every combination the upstream conftest parametrises: constant and mixed block
+sizes, batching 1 / 2 / 100, out on/off, return_retarded on/off, stack shapes
+(10,), (7, 2), (9, 2, 4).
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+from scipy import sparse
+
+from oracle import rgf_oracle as orc
+from quatrex_b200.datastructures import DSDBCOO
+from quatrex_b200.greens_function_solver import RGF, OBCBlocks
+from quatrex_b200.workloads import make_device
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-10
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _bt_dense(rng, block_sizes):
+    """Seeded upstream-style random BTD matrix (50 % dense blocks, diagonally dominant)."""
+    offs = np.hstack(([0], np.cumsum(block_sizes)))
+    n = offs[-1]
+    arr = np.zeros((n, n), dtype=np.complex128)
+
+    def blk(m, k):
+        mask = rng.random((m, k)) < 0.5
+        return mask * (rng.random((m, k)) + 1j * rng.random((m, k)))
+
+    for i in range(len(block_sizes)):
+        arr[offs[i]:offs[i + 1], offs[i]:offs[i + 1]] = blk(block_sizes[i], block_sizes[i]) + np.eye(block_sizes[i])
+        if i > 0:
+            arr[offs[i]:offs[i + 1], offs[i - 1]:offs[i]] = blk(block_sizes[i], block_sizes[i - 1])
+            arr[offs[i - 1]:offs[i], offs[i]:offs[i + 1]] = blk(block_sizes[i - 1], block_sizes[i])
+    for i in range(n):
+        arr[i, i] = (1 + 1j) + complex(np.sum(arr[i, :]))
+    return arr
+
+
+BLOCK_SIZES = [np.array([2] * 10), np.array([2] * 3 + [4] * 2 + [2] * 3)]
+STACKS = [(10,), (7, 2), (9, 2, 4)]
+
+
+@pytest.mark.parametrize("block_sizes", BLOCK_SIZES, ids=["constant", "mixed"])
+@pytest.mark.parametrize("max_batch_size", [1, 2, 100])
+@pytest.mark.parametrize("use_out", [True, False])
+@pytest.mark.parametrize("stack", STACKS, ids=["1D", "2D", "3D"])
+@pytest.mark.parametrize("on_device", [True, False])
+def test_selected_inv_upstream_criterion(block_sizes, max_batch_size, use_out, stack, on_device):
+    rng = np.random.default_rng(len(block_sizes) * 7 + max_batch_size)
+    bt = _bt_dense(rng, block_sizes)
+    mask = bt.astype(bool)
+    ref = np.linalg.inv(bt) * mask
+    a = DSDBCOO.from_sparray(sparse.coo_matrix(bt), block_sizes, stack, device="cuda" if on_device else None)
+    solver = RGF(max_batch_size=max_batch_size)
+    if use_out:
+        x = DSDBCOO.zeros_like(a)
+        assert solver.selected_inv(a, out=x) is None
+    else:
+        x = solver.selected_inv(a)
+    got = x.to_dense() * mask
+    assert np.allclose(np.broadcast_to(ref, stack + ref.shape), got)
+    assert _rel(got, np.broadcast_to(ref, got.shape)) < 1e-12
+
+
+@pytest.mark.parametrize("block_sizes", BLOCK_SIZES, ids=["constant", "mixed"])
+@pytest.mark.parametrize("max_batch_size", [1, 2, 100])
+@pytest.mark.parametrize("use_out", [True, False])
+@pytest.mark.parametrize("return_retarded", [True, False])
+@pytest.mark.parametrize("stack", STACKS, ids=["1D", "2D", "3D"])
+def test_selected_solve_upstream_criterion(block_sizes, max_batch_size, use_out, return_retarded, stack):
+    rng = np.random.default_rng(len(block_sizes) * 11 + max_batch_size)
+    bt = _bt_dense(rng, block_sizes)
+    bl = bt - bt.conj().T
+    bg = bt - bt.conj().T
+    ref_r = np.linalg.inv(bt)
+    ref_l = ref_r @ bl @ ref_r.conj().T
+    ref_g = ref_r @ bg @ ref_r.conj().T
+    A = DSDBCOO.from_sparray(sparse.coo_matrix(bt), block_sizes, stack, device="cuda")
+    BL = DSDBCOO.from_sparray(sparse.coo_matrix(bl), block_sizes, stack, device="cuda")
+    BG = DSDBCOO.from_sparray(sparse.coo_matrix(bg), block_sizes, stack, device="cuda")
+    solver = RGF(max_batch_size=max_batch_size)
+    if use_out:
+        XR, XL, XG = (DSDBCOO.zeros_like(A) for _ in range(3))
+        assert solver.selected_solve(A, BL, BG, out=[XL, XG, XR], return_retarded=return_retarded) is None
+    elif return_retarded:
+        XL, XG, XR = solver.selected_solve(A, BL, BG, return_retarded=True)
+    else:
+        XL, XG = solver.selected_solve(A, BL, BG)
+    if return_retarded:
+        m = XR.to_dense().astype(bool)
+        assert np.allclose(np.broadcast_to(ref_r, stack + ref_r.shape) * m, XR.to_dense() * m)
+    for X, ref in ((XL, ref_l), (XG, ref_g)):
+        m = X.to_dense().astype(bool)
+        assert np.allclose(np.broadcast_to(ref, stack + ref.shape) * m, X.to_dense() * m)
+
+
+def test_selected_solve_wrong_out_length_raises():
+    bt = _bt_dense(np.random.default_rng(0), BLOCK_SIZES[0])
+    A = DSDBCOO.from_sparray(sparse.coo_matrix(bt), BLOCK_SIZES[0], (2,), device="cuda")
+    with pytest.raises(ValueError):
+        RGF().selected_solve(A, A, A, out=[DSDBCOO.zeros_like(A), DSDBCOO.zeros_like(A)], return_retarded=True)
+
+
+@pytest.mark.parametrize("case", ["constant", "mixed"])
+def test_against_upstream_fixture(case):
+    g = np.load(os.path.join(GOLDEN, f"btd_{case}.npz"))
+    sizes = g["block_sizes"]
+    stack = int(g["stack"])
+    mask = g["a"] != 0
+    A = DSDBCOO.from_sparray(sparse.coo_matrix(g["a"]), sizes, (stack,), device="cuda")
+    BL = DSDBCOO.from_sparray(sparse.coo_matrix(g["sigma_lesser"]), sizes, (stack,), device="cuda")
+    BG = DSDBCOO.from_sparray(sparse.coo_matrix(g["sigma_greater"]), sizes, (stack,), device="cuda")
+    solver = RGF(max_batch_size=2)
+    x = solver.selected_inv(A).to_dense()[3] * mask
+    assert _rel(x, g["inv"] * mask) < 1e-12
+    xl, xg, xr = solver.selected_solve(A, BL, BG, return_retarded=True)
+    for key, got in (("xl", xl), ("xg", xg)):
+        m = g[key] != 0
+        assert _rel(got.to_dense()[0] * m, g[key] * m) < 1e-12
+    m = g["xr"] != 0
+    assert _rel(xr.to_dense()[0] * m, g["xr"] * m) < 1e-12
+
+
+def _transport_inputs(dev, energies=None, device="cuda"):
+    e = dev.energies if energies is None else energies
+    d, u, lo = dev.system_blocks(e)
+    obc = orc.obc_self_energies(d, u, lo, e, dev.mu_left, dev.mu_right, dev.kt, dev.sr_tol, dev.sr_max_iter)
+    nb = len(d)
+    A = DSDBCOO.from_blocks(d, u, lo, device=device)
+    z = DSDBCOO.from_blocks([np.zeros_like(x) for x in d], [np.zeros_like(x) for x in u],
+                            [np.zeros_like(x) for x in lo], device=device)
+    ob = OBCBlocks(nb)
+    ob.retarded[0], ob.retarded[-1] = obc["retarded"]
+    ob.lesser[0], ob.lesser[-1] = obc["lesser"]
+    ob.greater[0], ob.greater[-1] = obc["greater"]
+    return d, u, lo, obc, A, z, ob
+
+
+def _blocks(m, nb):
+    return ([m.blocks[i, i] for i in range(nb)], [m.blocks[i, i + 1] for i in range(nb - 1)],
+            [m.blocks[i + 1, i] for i in range(nb - 1)])
+
+
+def test_transport_small_against_upstream_fixture():
+    g = np.load(os.path.join(GOLDEN, "transport_small.npz"))
+    dev = make_device(num_blocks=4, block_size=8, num_energies=6, seed=7)
+    d, u, lo, obc, A, Z, ob = _transport_inputs(dev)
+    xl, xg, xr, cur = RGF().selected_solve(A, Z, Z, obc_blocks=ob, return_retarded=True, return_current=True)
+    nb = 4
+    for key, X in (("xl", xl), ("xg", xg)):
+        dd, uu, ll = _blocks(X, nb)
+        assert _rel(np.stack(dd, 1), g[f"{key}_diag"]) < TOL
+        assert _rel(np.stack(uu, 1), g[f"{key}_upper"]) < TOL
+        assert _rel(np.stack(ll, 1), g[f"{key}_lower"]) < TOL
+    assert _rel(np.stack(_blocks(xr, nb)[0], 1), g["xr_diag"]) < TOL
+    cur = cur.cpu().numpy()
+    # the last interface is where upstream reads the right coupling
+    assert _rel(cur[:, -1], g["current"][:, -1]) < 1e-9
+    x = RGF().selected_inv(A, obc_blocks=ob)
+    dd, uu, ll = _blocks(x, nb)
+    assert _rel(np.stack(dd, 1), g["inv_diag"]) < TOL
+    assert _rel(np.stack(uu, 1), g["inv_upper"]) < TOL
+    assert _rel(np.stack(ll, 1), g["inv_lower"]) < TOL
+
+
+@pytest.mark.parametrize("max_batch_size", [1, 3, 100])
+def test_transport_per_block_against_oracle(max_batch_size):
+    dev = make_device(num_blocks=6, block_size=24, num_energies=7, seed=21)
+    d, u, lo, obc, A, Z, ob = _transport_inputs(dev)
+    nb = 6
+    pad = [None] * (nb - 2)
+    ref = orc.selected_solve(d, u, lo, [np.zeros_like(x) for x in d], [np.zeros_like(x) for x in u],
+                             [np.zeros_like(x) for x in d], [np.zeros_like(x) for x in u],
+                             [obc["retarded"][0], *pad, obc["retarded"][1]], [obc["lesser"][0], *pad, obc["lesser"][1]],
+                             [obc["greater"][0], *pad, obc["greater"][1]], return_current=True)
+    xl, xg, xr, cur = RGF(max_batch_size=max_batch_size).selected_solve(
+        A, Z, Z, obc_blocks=ob, return_retarded=True, return_current=True)
+    for key, X in (("xl", xl), ("xg", xg)):
+        dd, uu, ll = _blocks(X, nb)
+        for i in range(nb):
+            assert _rel(dd[i], ref[f"{key}_diag"][i]) < TOL, (key, i)
+        for i in range(nb - 1):
+            assert _rel(uu[i], ref[f"{key}_upper"][i]) < TOL
+            assert _rel(ll[i], ref[f"{key}_lower"][i]) < TOL
+    for i in range(nb):
+        assert _rel(xr.blocks[i, i], ref["xr_diag"][i]) < TOL
+    assert _rel(cur.cpu().numpy(), ref["current"]) < 1e-9
+
+
+def test_host_numpy_inputs_roundtrip():
+    """NumPy (host) matrices: copied to the device and the outputs written back."""
+    dev = make_device(num_blocks=4, block_size=16, num_energies=3, seed=4)
+    d, u, lo, obc, A, Z, ob = _transport_inputs(dev, device=None)
+    assert isinstance(A.data, np.ndarray)
+    xl, xg = RGF().selected_solve(A, Z, Z, obc_blocks=ob)
+    assert isinstance(xl.data, np.ndarray)
+    pad = [None] * 2
+    ref = orc.selected_solve(d, u, lo, [np.zeros_like(x) for x in d], [np.zeros_like(x) for x in u],
+                             [np.zeros_like(x) for x in d], [np.zeros_like(x) for x in u],
+                             [obc["retarded"][0], *pad, obc["retarded"][1]], [obc["lesser"][0], *pad, obc["lesser"][1]],
+                             [obc["greater"][0], *pad, obc["greater"][1]])
+    assert _rel(xl.blocks[2, 2], ref["xl_diag"][2]) < TOL
+
+
+def test_single_block_device():
+    """nb = 1: no sweep, x_0 = inv(A_00 - Sigma_0)."""
+    rng = np.random.default_rng(9)
+    a = rng.standard_normal((5, 5)) + 1j * rng.standard_normal((5, 5)) + 5 * np.eye(5)
+    A = DSDBCOO.from_sparray(sparse.coo_matrix(a), np.array([5]), (2,), device="cuda")
+    x = RGF().selected_inv(A)
+    assert _rel(x.to_dense()[0], np.linalg.inv(a)) < 1e-12
+    sl = a - a.conj().T
+    SL = DSDBCOO.from_sparray(sparse.coo_matrix(sl), np.array([5]), (2,), device="cuda")
+    xl, xg = RGF().selected_solve(A, SL, SL)
+    ref = np.linalg.inv(a) @ sl @ np.linalg.inv(a).conj().T
+    assert _rel(xl.to_dense()[1], 0.5 * (ref - ref.conj().T)) < 1e-12

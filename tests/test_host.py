@@ -1,0 +1,108 @@
+"""Host-side logic that needs no GPU: library exports, block maps, batching."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+from scipy import sparse
+
+from quatrex_b200 import _lib
+from quatrex_b200.datastructures import DSDBCOO, block_sort_index, btd_layout_from_coords
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _header_symbols():
+    text = open(os.path.join(ROOT, "include", "qtx_rgf.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:qtx_status|const char\*|int64_t)\s+(qtx_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    names = _header_symbols()
+    assert len(names) >= 12
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _lib.SIGNATURES, n
+    assert set(_lib.SIGNATURES) == set(names)
+    assert b"sm_100a" in lib.qtx_version()
+
+
+def test_library_without_device_reports_error():
+    lib = _lib.load()
+    p = ctypes.c_void_p()
+    # on a machine without a usable CUDA device the context cannot be created
+    st = lib.qtx_ctx_create(0, ctypes.byref(p))
+    try:
+        import torch
+
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if not has_gpu:
+        assert st != _lib.QTX_OK
+    else:
+        assert st == _lib.QTX_OK
+        lib.qtx_ctx_destroy(p)
+
+
+def _bt_pattern(sizes, density, rng):
+    offs = np.hstack(([0], np.cumsum(sizes)))
+    n = offs[-1]
+    a = np.zeros((n, n), dtype=np.complex128)
+    for i in range(len(sizes)):
+        for j in range(max(0, i - 1), min(len(sizes), i + 2)):
+            blk = (rng.random((sizes[i], sizes[j])) < density) * (rng.standard_normal((sizes[i], sizes[j])) + 1j)
+            a[offs[i]:offs[i + 1], offs[j]:offs[j + 1]] = blk
+    return a
+
+
+@pytest.mark.parametrize("sizes", [[2] * 10, [2, 2, 2, 4, 4, 2, 2, 2], [5, 3, 7]])
+@pytest.mark.parametrize("density", [0.5, 1.0])
+def test_layout_roundtrip(sizes, density):
+    rng = np.random.default_rng(1)
+    dense = _bt_pattern(sizes, density, rng)
+    m = DSDBCOO.from_sparray(sparse.coo_matrix(dense), np.array(sizes), (3,))
+    assert np.allclose(m.to_dense()[1], dense)
+    lay = m.layout
+    nb = len(sizes)
+    offs = np.hstack(([0], np.cumsum(sizes)))
+    for i in range(nb):
+        for j in range(max(0, i - 1), min(nb, i + 2)):
+            k = 2 * i + j
+            blk = m.blocks[i, j][0]
+            assert np.allclose(blk, dense[offs[i]:offs[i + 1], offs[j]:offs[j + 1]])
+            if density == 1.0:
+                assert lay.local_index[k] is None  # dense row-major slice, read in place
+    # blocks are contiguous and in (0,0),(0,1),(1,0),(1,1),... order
+    starts = [s for s in lay.block_offset if s >= 0]
+    assert starts == sorted(starts)
+
+
+def test_layout_rejects_non_btd():
+    rows = np.array([0, 5])
+    cols = np.array([5, 0])
+    with pytest.raises(ValueError):
+        btd_layout_from_coords(rows, cols, [2, 2, 2])
+
+
+def test_block_sort_matches_upstream_rule():
+    # upstream: block row by block row, inside a block row by block column,
+    # stable inside a block (compute_block_sort_index)
+    rows = np.array([0, 0, 1, 2, 2, 3, 3])
+    cols = np.array([0, 2, 1, 0, 3, 2, 3])
+    order = block_sort_index(rows, cols, [2, 2])
+    assert list(zip(rows[order], cols[order])) == [(0, 0), (1, 1), (0, 2), (2, 0), (2, 3), (3, 2), (3, 3)]
+
+
+def test_set_get_block_and_zeros_like():
+    dense = _bt_pattern([3, 3, 3], 1.0, np.random.default_rng(2))
+    m = DSDBCOO.from_sparray(sparse.coo_matrix(dense), np.array([3, 3, 3]), (4,))
+    z = DSDBCOO.zeros_like(m)
+    assert np.all(z.to_dense() == 0)
+    val = np.arange(9).reshape(3, 3) * (1 + 1j)
+    z.blocks[1, 2] = val
+    assert np.allclose(z.blocks[1, 2], val)
+    assert np.allclose(z.to_dense()[2][3:6, 6:9], val)
