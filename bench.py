@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""RGF transport benchmark: energy-point solves/s on one or more B200s.
+
+Workload (the single-GPU scale-up): a seeded block-tridiagonal device with
+nb = 64 blocks of b = 256 orbitals, 1024 energies on [-2, 2], complex128.
+One step = one batch of energies (default 128) through the full hot path:
+A(E) = (E + i eta) I - H formed on the device, Sancho-Rubio for both contacts
+(tol 1e-12), contact self-energies, the RGF selected solve returning the
+diagonal and first off-diagonal blocks of G^R, G^< and G^>, per-block density,
+contact currents and the Caroli transmission.  With the defaults
+(--steps 8, 128 energies per step) the timed region covers all 1024 energies.
+
+value: whole-job solves/s with H resident in HBM; e2e: the same through the
+public API with H and the energies copied from pinned host memory and the
+step's observables (density, currents, transmission) read back every step.
+Under torchrun each rank solves its own energies (weak scaling, no collective
+on the data path); the time is the maximum over ranks.
+
+--impl reference times the CPU implementation of the same path (the NumPy
+restatement of the upstream algorithm in oracle/) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FP64_DMMA_PEAK_TFLOPS = 37.0  # measured on this pool's B200s: mma.sync m8n8k4 f64 issue-rate probe
+FP64_PEAK_SOURCE = "measured: DMMA issue-rate probe on B200 (profiles/fp64_peak_b200.md)"
+
+
+def _workload(args):
+    from quatrex_b200.workloads import CONFIG_LARGE, CONFIG_SMALL
+
+    cfg = dict(CONFIG_LARGE if args.workload == "large" else CONFIG_SMALL)
+    return cfg
+
+
+def _flops_per_energy(nb, b, sr_iterations):
+    """Algorithmic flops of one energy solve of the generator form (zero interior
+    self-energies), in units of one b x b complex product (8 b^3 flops; a block
+    inverse counts as one):
+      first block: inverse + 2 x 2 Keldysh products            =  5
+      forward step: A_ji x_i, Schur update, inverse, 2 x 4       = 11 per step
+      backward step: P1..P4, G^R_ji, corner chain, 2 x 4, x_i    = 15 per step
+      contacts: Sigma^R 2 x 2; transmission: 2                   =  6
+      Sancho-Rubio: 7 per iteration + final inverse, per contact"""
+    units = 5 + (nb - 1) * (11 + 15) + 6 + sum(7 * it + 1 for it in sr_iterations)
+    return 8.0 * b ** 3 * units
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_index: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        ids = [v.strip() for v in vis.split(",")] if vis else []
+        self.index = ids[local_index] if local_index < len(ids) else str(local_index)
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(cfg, sample_energies: int, threads_note: dict):
+    """The oracle (NumPy restatement of the upstream path) on a bounded sample."""
+    from oracle import rgf_oracle as orc
+    from quatrex_b200.workloads import make_device
+
+    dev = make_device(**cfg)
+    idx = np.linspace(0, cfg["num_energies"] - 1, sample_energies).round().astype(int)
+    e = dev.energies[idx]
+    t0 = time.perf_counter()
+    for k in range(len(e)):
+        ek = e[k:k + 1]
+        d, u, lo = dev.system_blocks(ek)
+        obc = orc.obc_self_energies(d, u, lo, ek, dev.mu_left, dev.mu_right, dev.kt, dev.sr_tol, dev.sr_max_iter)
+        nb = len(d)
+        pad = [None] * (nb - 2)
+        z = [np.zeros_like(x) for x in d]
+        zu = [np.zeros_like(x) for x in u]
+        ref = orc.selected_solve(d, u, lo, z, zu, z, zu, [obc["retarded"][0], *pad, obc["retarded"][1]],
+                                 [obc["lesser"][0], *pad, obc["lesser"][1]],
+                                 [obc["greater"][0], *pad, obc["greater"][1]], return_extras=True)
+        orc.caroli_transmission(ref["xr_corner"], obc["gamma"][0], obc["gamma"][1])
+        orc.block_density(ref["xl_diag"])
+    dt = time.perf_counter() - t0
+    return len(e) / dt, dt, idx
+
+
+def blas_threads() -> dict:
+    try:
+        from threadpoolctl import threadpool_info
+
+        info = threadpool_info()
+        blas = [i for i in info if i.get("user_api") == "blas"]
+        if blas:
+            return {"threads": int(blas[0].get("num_threads", 1)), "library": blas[0].get("internal_api", "?")}
+    except Exception:
+        pass
+    return {"threads": os.cpu_count() or 1, "library": "?"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cfg = _workload(args)
+    bt = blas_threads()
+    total = 0.0
+    solves = 0
+    # warm-up: one energy each
+    for _ in range(args.warmup):
+        cpu_baseline(cfg, 1, bt)
+    for _ in range(args.steps):
+        rate, dt, _ = cpu_baseline(cfg, args.ref_energies_per_step, bt)
+        total += dt
+        solves += args.ref_energies_per_step
+    value = solves / total
+    sample = (f"{args.ref_energies_per_step} energy solve(s) per step of nb={cfg['num_blocks']}, "
+              f"b={cfg['block_size']} (Sancho-Rubio both contacts + selected solve + transmission)")
+    line = {
+        "impl": "reference", "metric": "rgf_energy_solves_per_s", "value": value, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"transport nb={cfg['num_blocks']} b={cfg['block_size']} "
+                               f"E={cfg['num_energies']} complex128", "energies_per_step": args.ref_energies_per_step},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": bt["threads"], "kind": "port",
+                         "sample": sample, "blas": bt["library"]},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from quatrex_b200 import _lib
+    from quatrex_b200.transport import TransportSolver
+    from quatrex_b200.workloads import make_device
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device(f"cuda:{local}"))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    cfg = _workload(args)
+    dev = make_device(**cfg)
+    E = args.energies_per_step
+    nb, b = cfg["num_blocks"], cfg["block_size"]
+    solver = TransportSolver(dev, max_batch_size=E, precision=args.precision, cuda_device=local)
+    energies_all = torch.from_numpy(dev.energies).to(f"cuda:{local}")
+    out = solver.allocate_outputs(E)
+    n_all = len(dev.energies)
+
+    def step_energies(k):
+        g = (k * world + rank) * E
+        idx = (torch.arange(E, device=f"cuda:{local}") + g) % n_all
+        return energies_all[idx].contiguous()
+
+    stream = torch.cuda.current_stream()
+    step_e = [step_energies(k) for k in range(args.steps)]
+    for k in range(args.warmup):
+        solver.solve(step_energies(k), out)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region
+    ctx_launch0 = _lib.launch_count(local)
+    _lib.set_timing(True, local)
+    sr_its = []
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for k in range(args.steps):
+            solver.solve(step_e[k], out)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    launches = _lib.launch_count(local) - ctx_launch0
+    gemm = _lib.timing_report(0, local)
+    inv = _lib.timing_report(1, local)
+    _lib.set_timing(False, local)
+    sr_its = out["sr_iterations"].cpu().numpy()
+    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_ms = float(t.item())
+    value = world * args.steps * E / (elapsed_ms / 1000.0)
+
+    # ---- end to end through the public API: H and energies from pinned host memory,
+    # observables back to pinned host memory, every step
+    e2e = None
+    if not args.no_e2e:
+        h_diag_host = torch.from_numpy(dev.h_diag).pin_memory()
+        h_upper_host = torch.from_numpy(dev.h_upper).pin_memory()
+        e_host = [step_energies(k).cpu().pin_memory() for k in range(args.steps)]
+        obs_keys = ("density", "hole_density", "transmission", "current_left", "current_right", "sr_iterations")
+        host_obs = {k: torch.empty(out[k].shape, dtype=out[k].dtype).pin_memory() for k in obs_keys}
+        h_diag_dev = torch.empty_like(solver.h_diag)
+        h_upper_dev = torch.empty_like(solver.h_upper)
+        e_dev = torch.empty(E, dtype=torch.float64, device=f"cuda:{local}")
+        s2 = TransportSolver(dev, max_batch_size=E, precision=args.precision, cuda_device=local,
+                             h_diag=h_diag_dev, h_upper=h_upper_dev)
+        h2d = h_diag_host.numel() * 16 + h_upper_host.numel() * 16 + E * 8
+        d2h = sum(v.numel() * v.element_size() for v in host_obs.values())
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for k in range(args.steps):
+            h_diag_dev.copy_(h_diag_host, non_blocking=True)
+            h_upper_dev.copy_(h_upper_host, non_blocking=True)
+            e_dev.copy_(e_host[k], non_blocking=True)
+            s2.solve(e_dev, out)
+            for key in obs_keys:
+                host_obs[key].copy_(out[key], non_blocking=True)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device=f"cuda:{local}")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * args.steps * E / (float(t.item()) / 1000.0), "unit": "solves/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    # ---- roofline of the dominant kernel (batched complex FP64 GEMM on DMMA)
+    gemm_tflops = gemm["flops"] / (gemm["ms"] / 1000.0) / 1e12 if gemm["ms"] > 0 else 0.0
+    roofline = {
+        "kernel": "zgemm_dmma_kernel", "bound": "tensor", "achieved": round(gemm_tflops, 3),
+        "peak": FP64_DMMA_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": round(gemm_tflops / FP64_DMMA_PEAK_TFLOPS, 4),
+        "peak_source": FP64_PEAK_SOURCE,
+        "traffic": None,
+        "gemm_launches": gemm["launches"], "gemm_ms": round(gemm["ms"], 3),
+        "gemm_share_of_step": round(gemm["ms"] / elapsed_ms, 4) if elapsed_ms > 0 else None,
+        "inverse_ms": round(inv["ms"], 3), "inverse_launches": inv["launches"],
+        "inverse_tflops": round(inv["flops"] / (inv["ms"] / 1000.0) / 1e12, 3) if inv["ms"] > 0 else None,
+    }
+    alg = _flops_per_energy(nb, b, [float(np.mean(sr_its[:, 0])), float(np.mean(sr_its[:, 1]))])
+    whole_tflops = alg * args.steps * E / (elapsed_ms / 1000.0) / 1e12
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        bt = blas_threads()
+        rate, dt, idx = cpu_baseline(cfg, args.cpu_energies, bt)
+        cpu = {"value": rate, "unit": "solves/s", "cores": bt["threads"], "kind": "port",
+               "sample": f"{args.cpu_energies} energies of the same workload ({dt:.1f} s, oracle NumPy path)",
+               "blas": bt["library"]}
+
+    if rank == 0:
+        line = {
+            "metric": "rgf_energy_solves_per_s", "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "data": "synthetic (seeded Hamiltonian generator)",
+            "config": {
+                "workload": f"transport nb={nb} b={b} E={cfg['num_energies']} complex128, "
+                            f"{args.precision}", "energies_per_step": E, "precision": args.precision,
+                "l2": "inputs larger than L2 (per-step state >= 24 GB)", "parallelism": f"energy shards x{world}"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "whole_step_tflops_fp64_equiv": round(whole_tflops, 3),
+            "sr_iterations_mean": [float(np.mean(sr_its[:, 0])), float(np.mean(sr_its[:, 1]))],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["large", "small"], default="large")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--energies-per-step", type=int, default=128)
+    ap.add_argument("--cpu-energies", type=int, default=3)
+    ap.add_argument("--ref-energies-per-step", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

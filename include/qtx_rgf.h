@@ -199,6 +199,17 @@ qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, con
 /* Number of kernel launches this context has issued (for launch accounting). */
 int64_t qtx_launch_count(const qtx_ctx* ctx);
 
+/* Launch timing (the counterpart of qttools.profiling.Profiler,
+ * src/qttools/profiling/profiler.py:187-429, which times code regions): when
+ * enabled, every complex-GEMM (kind 0) and block-inverse (kind 1) launch of
+ * this context is bracketed by CUDA events on its stream.  Enabling or
+ * disabling resets the totals.  The report synchronises on the recorded events
+ * and returns the summed device time, the algorithmic flops (8 m n k per
+ * complex product, 8 n^3 per inverse) and the number of launches. */
+qtx_status qtx_ctx_set_timing(qtx_ctx* ctx, int enable);
+qtx_status qtx_ctx_timing_report(qtx_ctx* ctx, int32_t kind, double* total_ms, double* total_flops,
+                                 int64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -107,6 +107,9 @@ SIGNATURES = {
     "qtx_ctx_set_memory_limit": (c_int32, [c_void_p, ctypes.c_size_t]),
     "qtx_ctx_trim": (c_int32, [c_void_p]),
     "qtx_launch_count": (c_int64, [c_void_p]),
+    "qtx_ctx_set_timing": (c_int32, [c_void_p, ctypes.c_int]),
+    "qtx_ctx_timing_report": (
+        c_int32, [c_void_p, c_int32, ctypes.POINTER(c_double), ctypes.POINTER(c_double), ctypes.POINTER(c_int64)]),
     "qtx_inv": (c_int32, [c_void_p, c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p]),
     "qtx_zgemm": (
         c_int32,
@@ -213,3 +216,18 @@ def check(status: int, ctx: int, what: str) -> None:
 
 def launch_count(device: int = 0) -> int:
     return int(load().qtx_launch_count(context(device)))
+
+
+def set_timing(enable: bool, device: int = 0) -> None:
+    ctx = context(device)
+    check(load().qtx_ctx_set_timing(ctx, 1 if enable else 0), ctx, "qtx_ctx_set_timing")
+
+
+def timing_report(kind: int, device: int = 0) -> dict:
+    """Summed device time (ms), algorithmic flops and launches of one kernel class
+    (0 = complex GEMM, 1 = block inverse) since timing was enabled."""
+    ctx = context(device)
+    ms, fl, n = c_double(), c_double(), c_int64()
+    check(load().qtx_ctx_timing_report(ctx, kind, ctypes.byref(ms), ctypes.byref(fl), ctypes.byref(n)), ctx,
+          "qtx_ctx_timing_report")
+    return {"ms": ms.value, "flops": fl.value, "launches": n.value}

@@ -19,6 +19,14 @@
 
 thread_local int64_t* g_qtx_launch_counter = nullptr;
 
+// Per-kernel-class CUDA-event timing of the launches a context issues
+// (enabled by qtx_ctx_set_timing): 0 = complex GEMM, 1 = inverse.
+struct TimedLaunch {
+  cudaEvent_t start, stop;
+  int kind;
+  double flops;
+};
+
 struct qtx_ctx {
   int device = 0;
   std::string last_error;
@@ -26,7 +34,60 @@ struct qtx_ctx {
   size_t mem_limit = 0;
   int* d_scratch = nullptr;    // small device scratch (flags, counters)
   int* h_pinned = nullptr;     // pinned host mirror
+  bool timing = false;
+  std::vector<TimedLaunch> timed;
+  std::vector<cudaEvent_t> event_pool;
+  double acc_ms[2] = {0, 0};
+  double acc_flops[2] = {0, 0};
+  int64_t acc_launches[2] = {0, 0};
 };
+
+thread_local qtx_ctx* g_timing_ctx = nullptr;
+
+static cudaEvent_t pool_event(qtx_ctx* c) {
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Bracket one launch with events when timing is on.
+struct TimedScope {
+  qtx_ctx* c;
+  cudaStream_t s;
+  TimedLaunch t;
+  TimedScope(int kind, double flops, cudaStream_t stream) : c(g_timing_ctx), s(stream) {
+    if (!c || !c->timing) { c = nullptr; return; }
+    t.kind = kind;
+    t.flops = flops;
+    t.start = pool_event(c);
+    t.stop = pool_event(c);
+    cudaEventRecord(t.start, s);
+  }
+  ~TimedScope() {
+    if (!c) return;
+    cudaEventRecord(t.stop, s);
+    c->timed.push_back(t);
+  }
+};
+
+static void drain_timing(qtx_ctx* c) {
+  for (auto& t : c->timed) {
+    cudaEventSynchronize(t.stop);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t.start, t.stop);
+    c->acc_ms[t.kind] += ms;
+    c->acc_flops[t.kind] += t.flops;
+    c->acc_launches[t.kind] += 1;
+    c->event_pool.push_back(t.start);
+    c->event_pool.push_back(t.stop);
+  }
+  c->timed.clear();
+}
 
 namespace {
 
@@ -36,8 +97,15 @@ constexpr cplx MONE = {-1.0, 0.0};
 
 struct LaunchScope {
   int64_t* prev;
-  explicit LaunchScope(qtx_ctx* c) : prev(g_qtx_launch_counter) { g_qtx_launch_counter = &c->launches; }
-  ~LaunchScope() { g_qtx_launch_counter = prev; }
+  qtx_ctx* prev_ctx;
+  explicit LaunchScope(qtx_ctx* c) : prev(g_qtx_launch_counter), prev_ctx(g_timing_ctx) {
+    g_qtx_launch_counter = &c->launches;
+    g_timing_ctx = c;
+  }
+  ~LaunchScope() {
+    g_qtx_launch_counter = prev;
+    g_timing_ctx = prev_ctx;
+  }
 };
 
 // Stream-ordered device allocation (cudaMallocAsync on the context's pool).
@@ -174,8 +242,15 @@ void gemm(int m, int n, int k, int64_t batch, cplx alpha, MatView a, int op_a, M
   g.a = a; g.op_a = op_a; g.b = b; g.op_b = op_b;
   g.c = c; g.beta = beta; g.c2 = c2; g.gamma = gamma;
   g.d = d; g.alpha = alpha; g.active = active; g.diag_shift = diag_shift;
+  TimedScope ts(0, 8.0 * m * n * (double)k * batch, s);
   if (precision == QTX_PREC_MIXED && tf32x3_supported(g)) launch_zgemm_tf32x3(g, s);
   else launch_zgemm(g, s);
+}
+
+// Block inverse with timing (8 n^3 algorithmic flops per matrix: getrf + getri).
+void zinv(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t s) {
+  TimedScope ts(1, 8.0 * n * (double)n * n * batch, s);
+  launch_zinv(n, batch, a, x, info, active, s);
 }
 
 std::vector<int64_t> batch_offsets(int64_t num, int64_t max_batch) {
@@ -265,9 +340,9 @@ void selected_inv_impl(qtx_ctx* ctx, const Btd& a, const void* const* obc_r, con
       MatView o = obc_view(obc_r, 0, b0, e0);
       if (o.ptr) {
         launch_axpby(b0, b0, ne, ONE, a00, MONE, o, tv(0, b0), s);
-        launch_zinv(b0, ne, tv(0, b0), x.view(0), info, nullptr, s);
+        zinv(b0, ne, tv(0, b0), x.view(0), info, nullptr, s);
       } else {
-        launch_zinv(b0, ne, a00, x.view(0), info, nullptr, s);
+        zinv(b0, ne, a00, x.view(0), info, nullptr, s);
       }
     }
     // forward: x_j = inv(A_jj - Sigma_j - A_ji x_i A_ij)
@@ -281,7 +356,7 @@ void selected_inv_impl(qtx_ctx* ctx, const Btd& a, const void* const* obc_r, con
       MatView o = obc_view(obc_r, j, bj, e0);
       gemm(bj, bj, bi, ne, MONE, tv(0, bi), OP_N, a_ij, OP_N, tv(1, bj), s, a_jj, ONE, o, MONE, nullptr, nullptr,
            precision);
-      launch_zinv(bj, ne, tv(1, bj), x.view(j), info + (int64_t)j * ne_max, nullptr, s);
+      zinv(bj, ne, tv(1, bj), x.view(j), info + (int64_t)j * ne_max, nullptr, s);
     }
     out_block(out, nb - 1, nb - 1, e0, ne, x.view(nb - 1), 0, ws);
     // backward
@@ -377,9 +452,9 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
       MatView o = obc_view(obc_r, 0, b0, e0);
       if (o.ptr) {
         launch_axpby(b0, b0, ne, ONE, a00, MONE, o, tv(0, b0), s);
-        launch_zinv(b0, ne, tv(0, b0), xr.view(0), info, nullptr, s);
+        zinv(b0, ne, tv(0, b0), xr.view(0), info, nullptr, s);
       } else {
-        launch_zinv(b0, ne, a00, xr.view(0), info, nullptr, s);
+        zinv(b0, ne, a00, xr.view(0), info, nullptr, s);
       }
       for (int comp = 0; comp < 2; ++comp) {
         const Btd& S = comp == 0 ? A.sl : A.sg;
@@ -410,7 +485,7 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
              prec);
         gemm(bj, bj, bi, ne, MONE, tv(0, bi), OP_N, a_ij, OP_N, tv(1, bj), s, a_jj, ONE,
              obc_view(obc_r, j, bj, e0), MONE, nullptr, nullptr, prec);
-        launch_zinv(bj, ne, tv(1, bj), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
+        zinv(bj, ne, tv(1, bj), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
       }
       for (int comp = 0; comp < 2; ++comp) {
         const Btd& S = comp == 0 ? A.sl : A.sg;
@@ -546,7 +621,7 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
   QTX_CUDA_TRY(cudaMemsetAsync(its, 0, sizeof(int) * batch, s));
   bool converged = false;
   for (int it = 0; it < max_iter; ++it) {
-    launch_zinv(n, batch, eps, inv, nullptr, active, s);
+    zinv(n, batch, eps, inv, nullptr, active, s);
     gemm(n, n, n, batch, ONE, alpha, OP_N, inv, OP_N, t0, s, {}, ZERO, {}, ZERO, active);   // a inv
     gemm(n, n, n, batch, ONE, beta, OP_N, inv, OP_N, t1, s, {}, ZERO, {}, ZERO, active);    // b inv
     gemm(n, n, n, batch, ONE, t0, OP_N, beta, OP_N, t2, s, {}, ZERO, {}, ZERO, active);     // a inv b
@@ -566,7 +641,7 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
       break;
     }
   }
-  launch_zinv(n, batch, eps_s, x, nullptr, nullptr, s);
+  zinv(n, batch, eps_s, x, nullptr, nullptr, s);
   if (iterations) QTX_CUDA_TRY(cudaMemcpyAsync(iterations, its, sizeof(int) * batch, cudaMemcpyDeviceToDevice, s));
   return converged;
 }
@@ -665,7 +740,7 @@ void transport_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qtx_tran
     // M_0 = (E + i eta) I - H_00 - Sigma^R_L
     // (a K = 0 product: the epilogue alone forms -H_00 - Sigma^R_L + shift on the diagonal)
     gemm(b, b, 0, ne, ONE, tv(0), OP_N, tv(0), OP_N, tv(1), s, hd(0), MONE, obc_r(0), MONE, nullptr, shift);
-    launch_zinv(b, ne, tv(1), xr.view(0), info, nullptr, s);
+    zinv(b, ne, tv(1), xr.view(0), info, nullptr, s);
     for (int comp = 0; comp < 2; ++comp) {
       BlockStack& X = comp == 0 ? xl : xg;
       gemm(b, b, b, ne, ONE, xr.view(0), OP_N, obc_x(comp, 0), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
@@ -678,7 +753,7 @@ void transport_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qtx_tran
       gemm(b, b, b, ne, ONE, lo(i), OP_N, xr.view(i), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
       // M = (E + i eta) I - H_jj - Sigma^R_j - U A_ij
       gemm(b, b, b, ne, MONE, tv(0), OP_N, up(i), OP_N, tv(1), s, hd(j), MONE, obc_r(j), MONE, nullptr, shift, prec);
-      launch_zinv(b, ne, tv(1), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
+      zinv(b, ne, tv(1), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
       for (int comp = 0; comp < 2; ++comp) {
         BlockStack& X = comp == 0 ? xl : xg;
         // V = X_i A_ji^H ; Q = A_ji V + Sigma_obc,j ; X_j = x_j Q x_j^H   (interior Sigma = 0)
@@ -853,6 +928,29 @@ qtx_status qtx_ctx_trim(qtx_ctx* ctx) {
 
 int64_t qtx_launch_count(const qtx_ctx* ctx) { return ctx ? ctx->launches : -1; }
 
+qtx_status qtx_ctx_set_timing(qtx_ctx* ctx, int enable) {
+  if (!ctx) return QTX_E_INVAL;
+  cudaSetDevice(ctx->device);
+  drain_timing(ctx);
+  ctx->timing = enable != 0;
+  for (int k = 0; k < 2; ++k) {
+    ctx->acc_ms[k] = ctx->acc_flops[k] = 0;
+    ctx->acc_launches[k] = 0;
+  }
+  return QTX_OK;
+}
+
+qtx_status qtx_ctx_timing_report(qtx_ctx* ctx, int32_t kind, double* total_ms, double* total_flops,
+                                 int64_t* launches) {
+  if (!ctx || kind < 0 || kind > 1) return QTX_E_INVAL;
+  cudaSetDevice(ctx->device);
+  drain_timing(ctx);
+  if (total_ms) *total_ms = ctx->acc_ms[kind];
+  if (total_flops) *total_flops = ctx->acc_flops[kind];
+  if (launches) *launches = ctx->acc_launches[kind];
+  return QTX_OK;
+}
+
 qtx_status qtx_inv(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a, int64_t stride_a, void* x,
                    int64_t stride_x, qtx_stream stream) {
   return guarded(ctx, [&] {
@@ -860,7 +958,7 @@ qtx_status qtx_inv(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a, int64_
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     DevBuf info(sizeof(int) * std::max<int64_t>(batch, 1), s);
     QTX_CUDA_TRY(cudaMemsetAsync(info.as<int>(), 0, sizeof(int) * std::max<int64_t>(batch, 1), s));
-    launch_zinv(n, batch, MatView{reinterpret_cast<const cplx*>(a), n, stride_a},
+    zinv(n, batch, MatView{reinterpret_cast<const cplx*>(a), n, stride_a},
                 MutView{reinterpret_cast<cplx*>(x), n, stride_x}, info.as<int>(), nullptr, s);
     read_info_or_throw(ctx, info.as<int>(), batch, s, "qtx_inv");
   });

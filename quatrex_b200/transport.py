@@ -1,0 +1,86 @@
+"""Generator-form transport solve on the device (qtx_transport_solve).
+
+The energy-independent Hamiltonian blocks stay resident on the GPU; for each
+energy batch the library forms A(E) = (E + i eta) I - H on the fly (inside the
+GEMM epilogues), computes both contact self-energies by Sancho-Rubio, runs
+the selected solve and writes the requested Green's-function blocks and
+observables.  This is the device-resident form of
+``ElectronSolver.solve`` (``src/quatrex/electron/solver.py:456-604``) for a
+device whose leads repeat its end cells and whose interior scattering
+self-energies vanish.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from quatrex_b200 import _lib
+from quatrex_b200.workloads import TransportDevice
+
+_PRECISIONS = {"fp64": _lib.QTX_PREC_FP64, "mixed": _lib.QTX_PREC_MIXED}
+
+OUTPUT_KEYS = ("gr_diag", "gr_upper", "gr_lower", "gl_diag", "gl_upper", "gg_diag", "gg_upper", "density",
+               "hole_density", "transmission", "current_left", "current_right", "sr_iterations")
+
+
+class TransportSolver:
+    """Device-resident transport solver for one ``TransportDevice``."""
+
+    def __init__(self, device: TransportDevice, max_batch_size: int = 128, precision: str = "fp64",
+                 cuda_device: int | None = None, h_diag=None, h_upper=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("quatrex_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
+        self.dev = device
+        self.cuda = torch.cuda.current_device() if cuda_device is None else cuda_device
+        self.max_batch_size = int(max_batch_size)
+        self.precision = precision
+        self.nb = device.num_blocks
+        self.b = device.block_size
+        # H may be handed in already on the device (e.g. shared by several solvers)
+        self.h_diag = h_diag if h_diag is not None else torch.from_numpy(device.h_diag).to(f"cuda:{self.cuda}")
+        self.h_upper = h_upper if h_upper is not None else torch.from_numpy(device.h_upper).to(f"cuda:{self.cuda}")
+
+    def allocate_outputs(self, num_energies: int, keys=OUTPUT_KEYS) -> dict:
+        nb, b, ne = self.nb, self.b, int(num_energies)
+        dev = f"cuda:{self.cuda}"
+        shapes = {
+            "gr_diag": (ne, nb, b, b), "gr_upper": (ne, nb - 1, b, b), "gr_lower": (ne, nb - 1, b, b),
+            "gl_diag": (ne, nb, b, b), "gl_upper": (ne, nb - 1, b, b),
+            "gg_diag": (ne, nb, b, b), "gg_upper": (ne, nb - 1, b, b),
+        }
+        out = {}
+        for k in keys:
+            if k in shapes:
+                out[k] = torch.empty(shapes[k], dtype=torch.complex128, device=dev)
+            elif k in ("density", "hole_density"):
+                out[k] = torch.empty((ne, nb), dtype=torch.float64, device=dev)
+            elif k == "transmission":
+                out[k] = torch.empty((ne,), dtype=torch.float64, device=dev)
+            elif k in ("current_left", "current_right"):
+                out[k] = torch.empty((ne,), dtype=torch.complex128, device=dev)
+            elif k == "sr_iterations":
+                out[k] = torch.empty((ne, 2), dtype=torch.int32, device=dev)
+        return out
+
+    def solve(self, energies, outputs: dict | None = None, keys=OUTPUT_KEYS, stream=None) -> dict:
+        """Solve at the given energies (device or host array); returns the output dict."""
+        e = energies if isinstance(energies, torch.Tensor) else torch.as_tensor(np.asarray(energies, dtype=np.float64))
+        e = e.to(device=f"cuda:{self.cuda}", dtype=torch.float64).contiguous()
+        ne = int(e.shape[0])
+        if outputs is None:
+            outputs = self.allocate_outputs(ne, keys)
+        lib = _lib.load()
+        ctx = _lib.context(self.cuda)
+        p = _lib.TransportProblem(
+            num_blocks=self.nb, block_size=self.b, num_energies=ne, h_diag=self.h_diag.data_ptr(),
+            h_upper=self.h_upper.data_ptr(), energies=e.data_ptr(), eta=self.dev.eta, mu_left=self.dev.mu_left,
+            mu_right=self.dev.mu_right, kt=self.dev.kt, sr_tol=self.dev.sr_tol,
+            sr_max_iterations=self.dev.sr_max_iter, max_batch_size=self.max_batch_size)
+        o = _lib.TransportOutputs(**{k: (outputs[k].data_ptr() if k in outputs else None) for k in OUTPUT_KEYS})
+        s = stream if stream is not None else torch.cuda.current_stream(self.cuda).cuda_stream
+        st = lib.qtx_transport_solve(ctx, ctypes.byref(p), ctypes.byref(o), _PRECISIONS[self.precision], 0, s)
+        _lib.check(st, ctx, "transport_solve")
+        return outputs
