@@ -154,6 +154,24 @@ qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
                             double convergence_tol, int32_t max_iterations, void* x, int32_t* iterations,
                             qtx_stream stream);
 
+/* Sancho-Rubio that allocates nothing -- no counterpart in the upstream code.
+ * For callers that cannot let a library allocate device memory (an
+ * application allocator that owns all device memory, a plugin host that
+ * forbids library allocations, a latency-critical loop where cudaMalloc /
+ * cudaFree would synchronise the device).  Same contract as qtx_sancho_rubio
+ * (x, iterations and the QTX_E_NOT_CONVERGED status), without a context: the
+ * work space is one fixed 16 MiB device array inside the library, held by
+ * every GPU that loads it until the process exits.  A call needs about
+ * 9 * 16 * n^2 * batch bytes of it; larger requests return QTX_E_INVAL with the
+ * reason in `err` (optional caller buffer of err_len bytes).  The first call on
+ * a device looks up the array's device address; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race, so
+ * serialise them.  The call synchronises `stream` (convergence checks). */
+qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                                    const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
+                                    double convergence_tol, int32_t max_iterations, void* x, int32_t* iterations,
+                                    qtx_stream stream, char* err, int32_t err_len);
+
 /* Contact self-energies from a surface Green's function g (batch, n, n):
  * sigma_r = m_ji g m_ij, gamma = i (sigma_r - sigma_r^H),
  * sigma_l = i f gamma, sigma_g = i (f - 1) gamma with f = occupancy[batch]
