@@ -214,6 +214,12 @@ typedef struct qtx_transport_outputs {
 qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,
                                int32_t precision, uint32_t flags, qtx_stream stream);
 
+/* FP64 roofline probe -- no counterpart in the upstream code.  Measures the
+ * issue-rate ceiling of the FP64 tensor path (kind 0: DMMA mma.sync m8n8k4)
+ * or of scalar DFMA (kind 1) on the current device, in TFLOP/s; the roofline
+ * denominator of the FP64 kernels.  Synchronous. */
+qtx_status qtx_probe_fp64_peak(int32_t kind, double* tflops);
+
 /* Number of kernel launches this context has issued (for launch accounting). */
 int64_t qtx_launch_count(const qtx_ctx* ctx);
 

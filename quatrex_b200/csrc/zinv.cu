@@ -1,55 +1,96 @@
 // Batched complex FP64 inverse: blocked in-place Gauss-Jordan elimination with
-// partial (row) pivoting, one CTA per matrix.
+// partial (row) pivoting, one CTA per matrix, bulk work on the FP64 tensor path.
 //
 // Replaces qttools.kernels.linalg.inv (src/qttools/kernels/linalg/inv.py:6-40,
-// LAPACK getrf/getri or getrf/getrs on the GPU there).  Pivot choice follows
-// the LAPACK izamax rule: the first row of maximal |Re| + |Im|.
+// LAPACK getrf/getri, or getrf/getrs on the GPU).  Pivot choice follows the
+// LAPACK izamax rule: the first row (in the current row order) of maximal
+// |Re| + |Im|.
 //
-// Algorithm (for an n x n matrix X, panel width W):
+// Algorithm for an n x n matrix X (a copy of A), panel width w:
 //   for each panel of columns [k0, k0 + w):
-//     1. stage the n x w panel in shared memory and run unblocked in-place
-//        Gauss-Jordan on it: pivot search, row swap (recorded), scale the
-//        pivot row, eliminate the pivot column from every other row;
-//     2. the other columns receive the same row operations at once: with the
-//        composite row permutation sigma of the panel and the final panel
-//        P, for every row i
-//          X[i, c] <- [i not a pivot row] X[sigma(i), c]
-//                     + sum_j P[i, j] X[sigma(k0 + j), c]
-//        (a rank-w update, the bulk of the n^3 complex multiply-adds);
+//     1. stage the n x w panel in shared memory (rows in the current order of
+//        X) and eliminate it column by column without moving rows: pick the
+//        pivot row among the rows not yet used, eliminate the column from all
+//        other rows, scale the pivot row (two barriers per column);
+//     2. turn the pivot sequence into the row permutation sigma that the
+//        classic row-swapping Gauss-Jordan would apply (position k0 + j takes
+//        pivot row p_j, the displaced row goes to p_j's position), and record
+//        each swap for the final column unscrambling;
+//     3. apply the panel's row operations to every other column at once, a
+//        rank-w update on DMMA (mma.sync m16n8k4 f64) tiles:
+//          X[i, c] <- [i not in panel] X[sigma(i), c]
+//                     + sum_j P[sigma(i), j] X[p_j, c]
+//        in column slabs of CW, the k0 + j pivot rows staged in shared memory;
 //   finally undo the row interchanges as column interchanges in reverse order.
-// The matrix itself stays in global memory (L2 resident for the working set of
-// one wave); the panel (n x (W+1) complex, padded against bank conflicts), one
-// row slab of the update and the permutation live in shared memory.
+// The matrix itself stays in global memory (L2 resident for a wave of
+// matrices); shared memory holds the panel (n x Wp, XOR-swizzled so that both
+// row-per-thread access and DMMA fragment loads are conflict-free), two slabs
+// of pivot rows and the permutation arrays.
 #include "kernels.h"
 
 namespace {
 
 constexpr int THREADS = 256;
-constexpr int CPT = 4;      // columns per thread in the rank-w update
-constexpr int MAX_RPT = 8;  // rows per thread in the rank-w update
+constexpr int NWARPS = THREADS / 32;
+constexpr int MAX_CPT = 32;  // panel columns per thread in the elimination
+constexpr int MAX_RPT = 2;   // panel rows per thread in the elimination
 
 struct InvShape {
-  int W;    // panel width
-  int CW;   // columns per update slab
+  int w;    // panel width
+  int wp;   // panel storage width (multiple of 8)
+  int cw;   // columns per update slab (multiple of 32)
+  int tpr;  // threads per panel row in the elimination
 };
 
 __host__ __device__ inline InvShape inv_shape(int n) {
   InvShape s;
-  if (n <= 64) s.W = n;
-  else if (n <= 256) s.W = 32;
-  else s.W = 16;
-  s.CW = (n <= 256) ? 32 : 16;
+  s.w = n <= 64 ? n : (n <= 256 ? 32 : 16);
+  s.wp = (s.w + 7) / 8 * 8;
+  int row_tiles = (n + 31) / 32;
+  int col_tiles = row_tiles >= NWARPS ? 1 : NWARPS / row_tiles;
+  s.cw = 32 * col_tiles;
+  int tpr = 1;
+  while (tpr * 2 * n <= THREADS && tpr * 2 <= s.w) tpr *= 2;
+  s.tpr = tpr;
   return s;
+}
+
+// complex elements of the update slabs: pivot rows and panel rows, double
+// buffered (none when one panel covers the matrix)
+__host__ __device__ inline int slab_elems(int n, const InvShape& s) { return s.w >= n ? 0 : 4 * s.w * (s.cw + 2); }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool pred) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  int bytes = pred ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
 inline size_t inv_smem_bytes(int n) {
   InvShape s = inv_shape(n);
-  size_t panel = (size_t)n * (s.W + 1) * sizeof(cplx);
-  size_t slab = (size_t)s.W * s.CW * sizeof(cplx);
-  size_t fcol = (size_t)n * sizeof(cplx);
-  size_t ints = (size_t)(2 * n) * sizeof(int);
-  size_t red = 2 * (THREADS / 32) * sizeof(double) * 2;
-  return panel + slab + fcol + ints + red + 64;
+  size_t panel = (size_t)n * s.wp * sizeof(cplx);
+  size_t slabs = (size_t)slab_elems(n, s) * sizeof(cplx);
+  size_t ints = (size_t)(3 * n + 4) * sizeof(int);
+  size_t red = 2 * NWARPS * (sizeof(double) + sizeof(int));
+  size_t pivrow = (size_t)s.wp * sizeof(cplx);
+  return panel + slabs + ints + red + pivrow + 256;
+}
+
+// swizzled panel index: row r, column c (c < wp, wp multiple of 8)
+__device__ __forceinline__ int pidx(int r, int c, int wp) {
+  int sw = ((r & 1) << 2) | ((r >> 1) & 3);
+  return r * wp + (c ^ sw);
+}
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
 }
 
 __device__ __forceinline__ void argmax_combine(double& v, int& i, double v2, int i2) {
@@ -64,17 +105,27 @@ __global__ void __launch_bounds__(THREADS, 1)
                    cplx* x_base, int64_t ldx, int64_t sx, int* info, const int* active) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const InvShape shp = inv_shape(n);
-  const int W = shp.W, CW = shp.CW, LDP = W + 1;
+  const int W = shp.w, WP = shp.wp, CW = shp.cw, TPR = shp.tpr;
+  const int LDR = CW + 2;
   cplx* P = reinterpret_cast<cplx*>(smem_raw);
-  cplx* R = P + (size_t)n * LDP;
-  cplx* fcol = R + (size_t)W * CW;
-  int* sigma = reinterpret_cast<int*>(fcol + n);
-  int* perm = sigma + n;
-  double* red_v = reinterpret_cast<double*>(perm + n);
-  int* red_i = reinterpret_cast<int*>(red_v + THREADS / 32);
-  __shared__ int s_piv;
+  cplx* Rs = P + (size_t)n * WP;                 // two slabs of W x LDR (pivot rows, panel rows)
+  int* pos2row = reinterpret_cast<int*>(Rs + slab_elems(n, shp));
+  int* row2pos = pos2row + n;
+  int* perm = row2pos + n;                       // swap partner of each column (final unscramble)
+  // doubles after the int arrays: round the offset up to 16 bytes (3n ints is
+  // not a multiple of 8 bytes for odd n)
+  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(perm + n) + 15) & ~uintptr_t(15));
+  int* red_i = reinterpret_cast<int*>(red_v + 2 * NWARPS);
+  cplx* pbuf = reinterpret_cast<cplx*>(red_i + 2 * NWARPS + 2);  // copy of the pivot row (16-byte aligned below)
+  pbuf = reinterpret_cast<cplx*>((reinterpret_cast<uintptr_t>(pbuf) + 15) & ~uintptr_t(15));
+  __shared__ int s_rowflag[1024];                // row already a pivot (n <= 1024)
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  // elimination ownership: thread -> (rows r0 + q * rstride, columns cl + j * TPR)
+  const int rstride = THREADS / TPR;
+  const int r_own = tid / TPR;
+  const int c_own = tid % TPR;
 
   for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
     if (active && !active[e]) continue;
@@ -87,158 +138,240 @@ __global__ void __launch_bounds__(THREADS, 1)
         int r = idx / n, c = idx % n;
         X[(int64_t)r * ldx + c] = A[(int64_t)r * lda + c];
       }
-      __syncthreads();
     }
+    for (int r = tid; r < n; r += THREADS) s_rowflag[r] = 0;
+    __syncthreads();
 
     for (int k0 = 0; k0 < n; k0 += W) {
       const int w = min(W, n - k0);
+      // ---- 1. stage the panel (rows in the current order of X)
       for (int idx = tid; idx < n * w; idx += THREADS) {
         int r = idx / w, c = idx % w;
-        P[r * LDP + c] = X[(int64_t)r * ldx + k0 + c];
+        P[pidx(r, c, WP)] = X[(int64_t)r * ldx + k0 + c];
       }
-      for (int r = tid; r < n; r += THREADS) sigma[r] = r;
+      for (int r = tid; r < n; r += THREADS) {
+        pos2row[r] = r;
+        row2pos[r] = r;
+      }
       __syncthreads();
 
       for (int kk = 0; kk < w; ++kk) {
         const int k = k0 + kk;
-        // 1. pivot search over rows k..n-1 of panel column kk
+        // pivot search: the owner of (r, kk) looks at row r if it is not a pivot yet
         double bv = -1.0;
         int bi = n;
-        for (int r = k + tid; r < n; r += THREADS) argmax_combine(bv, bi, cabs1(P[r * LDP + kk]), r);
+        if (c_own == (kk % TPR)) {
+          for (int q = 0; q < MAX_RPT; ++q) {
+            int r = r_own + q * rstride;
+            if (r < n && !s_rowflag[r]) argmax_combine(bv, bi, cabs1(P[pidx(r, kk, WP)]), r);
+          }
+        }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
           double v2 = __shfl_down_sync(0xffffffffu, bv, off);
           int i2 = __shfl_down_sync(0xffffffffu, bi, off);
           argmax_combine(bv, bi, v2, i2);
         }
+        const int slot = (kk & 1) * NWARPS;
         if (lane == 0) {
-          red_v[warp] = bv;
-          red_i[warp] = bi;
+          red_v[slot + warp] = bv;
+          red_i[slot + warp] = bi;
         }
-        __syncthreads();
-        if (tid == 0) {
-          double v = red_v[0];
-          int i = red_i[0];
-          for (int q = 1; q < THREADS / 32; ++q) argmax_combine(v, i, red_v[q], red_i[q]);
-          if (i >= n) i = k;
-          s_piv = i;
-          perm[k] = i;
-          int t = sigma[k];
-          sigma[k] = sigma[i];
-          sigma[i] = t;
-        }
-        __syncthreads();
-        const int p = s_piv;
-        // 2. swap panel rows k and p
-        if (p != k) {
-          for (int c = tid; c < w; c += THREADS) {
-            cplx t = P[k * LDP + c];
-            P[k * LDP + c] = P[p * LDP + c];
-            P[p * LDP + c] = t;
-          }
-        }
-        __syncthreads();
-        // 3. scale the pivot row; keep the pivot column for the elimination
-        const cplx piv = P[k * LDP + kk];
-        if (piv.x == 0.0 && piv.y == 0.0) zero_pivot = zero_pivot ? zero_pivot : k + 1;
+        __syncthreads();  // S1: partial maxima and the previous column's writes are visible
+        double v = red_v[slot];
+        int p = red_i[slot];
+        for (int q = 1; q < NWARPS; ++q) argmax_combine(v, p, red_v[slot + q], red_i[slot + q]);
+        const cplx piv = P[pidx(p, kk, WP)];
+        if (piv.x == 0.0 && piv.y == 0.0 && !zero_pivot) zero_pivot = k + 1;
         const cplx d = crecip(piv);
-        for (int r = tid; r < n; r += THREADS) fcol[r] = P[r * LDP + kk];
-        __syncthreads();
-        for (int c = tid; c < w; c += THREADS) P[k * LDP + c] = (c == kk) ? d : cmul(P[k * LDP + c], d);
-        __syncthreads();
-        // 4. eliminate column kk from all other rows
-        for (int idx = tid; idx < n * w; idx += THREADS) {
-          int r = idx / w, c = idx % w;
-          if (r == k) continue;
-          cplx f = fcol[r];
-          P[r * LDP + c] = (c == kk) ? cmul(cmk(-f.x, -f.y), d) : cfms(f, P[k * LDP + c], P[r * LDP + c]);
+        // read phase: the owners of the pivot row copy it aside; every thread
+        // reads the factors of its rows
+        cplx f[MAX_RPT];
+#pragma unroll
+        for (int q = 0; q < MAX_RPT; ++q) {
+          int r = r_own + q * rstride;
+          f[q] = (r < n) ? P[pidx(r, kk, WP)] : cmk(0, 0);
         }
-        __syncthreads();
-      }
-
-      // write the finished panel back
-      for (int idx = tid; idx < n * w; idx += THREADS) {
-        int r = idx / w, c = idx % w;
-        X[(int64_t)r * ldx + k0 + c] = P[r * LDP + c];
-      }
-
-      // rank-w update of all other columns, CW columns per slab
-      const int tx = tid % (CW / CPT);
-      const int ty = tid / (CW / CPT);
-      const int TY = THREADS / (CW / CPT);
-      for (int cs = 0; cs < n; cs += CW) {
-        // (the panel columns themselves are skipped by the `ok` predicates)
-        cplx y[MAX_RPT][CPT];
-        // phase a: gather this thread's (permuted) rows and the pivot rows R
-#pragma unroll
-        for (int i = 0; i < MAX_RPT; ++i) {
-          int r = ty + i * TY;
-#pragma unroll
-          for (int q = 0; q < CPT; ++q) {
-            int c = cs + tx + q * (CW / CPT);
-            bool ok = r < n && c < n && (c < k0 || c >= k0 + w);
-            y[i][q] = ok ? X[(int64_t)sigma[r] * ldx + c] : cmk(0, 0);
-          }
+        for (int c = tid; c < w; c += THREADS) pbuf[c] = P[pidx(p, c, WP)];
+        // the flag is read by the next column's pivot search, which follows S2
+        if (tid == 0) s_rowflag[p] = 1;
+        __syncthreads();  // S2: all reads of this column done
+        if (tid == 0) {
+          // classic row-swap semantics: position k receives row p
+          int qpos = row2pos[p];
+          int rk = pos2row[k];
+          pos2row[k] = p;
+          row2pos[p] = k;
+          pos2row[qpos] = rk;
+          row2pos[rk] = qpos;
+          perm[k] = qpos;
         }
-        for (int idx = tid; idx < w * CW; idx += THREADS) {
-          int j = idx / CW, cc = idx % CW;
-          int c = cs + cc;
-          bool ok = c < n && (c < k0 || c >= k0 + w);
-          R[j * CW + cc] = ok ? X[(int64_t)sigma[k0 + j] * ldx + c] : cmk(0, 0);
-        }
-        __syncthreads();
-        // phase b: X[r, c] = [r not pivot] y + sum_j P[r, j] R[j, c]
 #pragma unroll
-        for (int i = 0; i < MAX_RPT; ++i) {
-          int r = ty + i * TY;
-          if (r >= k0 && r < k0 + w) {
-#pragma unroll
-            for (int q = 0; q < CPT; ++q) y[i][q] = cmk(0, 0);
-          }
-        }
-        for (int j = 0; j < w; ++j) {
-          cplx rv[CPT];
-#pragma unroll
-          for (int q = 0; q < CPT; ++q) rv[q] = R[j * CW + tx + q * (CW / CPT)];
-#pragma unroll
-          for (int i = 0; i < MAX_RPT; ++i) {
-            int r = ty + i * TY;
-            if (r < n) {
-              cplx pv = P[r * LDP + j];
-#pragma unroll
-              for (int q = 0; q < CPT; ++q) y[i][q] = cfma(pv, rv[q], y[i][q]);
+        for (int q = 0; q < MAX_RPT; ++q) {
+          int r = r_own + q * rstride;
+          if (r >= n) continue;
+          if (r == p) {
+#pragma unroll 8
+            for (int j = 0; j < MAX_CPT; ++j) {
+              int c = c_own + j * TPR;
+              if (c < w) P[pidx(r, c, WP)] = (c == kk) ? d : cmul(pbuf[c], d);
+            }
+          } else {
+            const cplx fd = cmul(f[q], d);
+#pragma unroll 8
+            for (int j = 0; j < MAX_CPT; ++j) {
+              int c = c_own + j * TPR;
+              if (c < w) {
+                cplx* pp = &P[pidx(r, c, WP)];
+                *pp = (c == kk) ? cmk(-fd.x, -fd.y) : cfms(fd, pbuf[c], *pp);
+              }
             }
           }
         }
+      }
+      __syncthreads();
+
+      // ---- 3. rank-w update of the other columns, slabs of CW columns.
+      // Output position i reads X[sigma(i)], and sigma(i) is either i itself or
+      // a row of [k0, k0 + w) (a row displaced by a pivot swap); the pivot rows
+      // X[p_j] and the rows of [k0, k0 + w) of the slab are staged in shared
+      // memory first, so afterwards every thread reads and writes only its own
+      // positions of X and one barrier per slab suffices.
+      const int row_tiles = (n + 31) / 32;
+      const int col_tiles = CW / 32;
+      const int nslab = (n + CW - 1) / CW;
+      // slabs with at least one column outside the panel, staged double buffered
+      auto next_slab = [&](int from) {
+        int sl = from;
+        while (sl < nslab && (sl * CW >= k0 && min(sl * CW + CW, n) <= k0 + w)) ++sl;
+        return sl;
+      };
+      auto stage = [&](int sl, int buf) {
+        cplx* Rb = Rs + (size_t)buf * 2 * W * LDR;
+        cplx* Db = Rb + (size_t)W * LDR;
+        const int cs = sl * CW;
+        for (int idx = tid; idx < w * CW; idx += THREADS) {
+          int j = idx / CW, cc = idx % CW;
+          int c = cs + cc;
+          bool ok = c < n;
+          cp_async16(&Rb[j * LDR + cc], ok ? &X[(int64_t)pos2row[k0 + j] * ldx + c] : X, ok);
+          cp_async16(&Db[j * LDR + cc], ok ? &X[(int64_t)(k0 + j) * ldx + c] : X, ok);
+        }
+        cp_async_commit();
+      };
+      int slab = next_slab(0);
+      int buf = 0;
+      if (slab < nslab) stage(slab, 0);
+      while (slab < nslab) {
+        const int c0 = slab * CW;
+        const int nxt = next_slab(slab + 1);
+        // the other buffer was last read before the barrier that ended the
+        // previous slab, so it can be refilled now
+        if (nxt < nslab) stage(nxt, buf ^ 1);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        cplx* R = Rs + (size_t)buf * 2 * W * LDR;  // pivot rows p_j      (w x CW)
+        cplx* D = R + (size_t)W * LDR;             // rows k0 + j         (w x CW)
+        for (int tile = warp; tile < row_tiles * col_tiles; tile += NWARPS) {
+          const int rt = tile / col_tiles, ct = tile % col_tiles;
+          const int row0 = rt * 32, col0 = ct * 32;
+          double acc_re[2][4][4], acc_im[2][4][4];
 #pragma unroll
-        for (int i = 0; i < MAX_RPT; ++i) {
-          int r = ty + i * TY;
+          for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-          for (int q = 0; q < CPT; ++q) {
-            int c = cs + tx + q * (CW / CPT);
-            bool ok = r < n && c < n && (c < k0 || c >= k0 + w);
-            if (ok) X[(int64_t)r * ldx + c] = y[i][q];
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                int i = row0 + mi * 16 + g + ((q >> 1) << 3);
+                int cc = col0 + ni * 8 + 2 * t + (q & 1);
+                int c = c0 + cc;
+                cplx y = cmk(0, 0);
+                if (i < n && c < n && !(i >= k0 && i < k0 + w)) {
+                  int src = pos2row[i];
+                  y = (src == i) ? X[(int64_t)i * ldx + c] : D[(src - k0) * LDR + cc];
+                }
+                acc_re[mi][ni][q] = y.x;
+                acc_im[mi][ni][q] = y.y;
+              }
+          int prow_idx[2][2];
+#pragma unroll
+          for (int mi = 0; mi < 2; ++mi) {
+            int i0 = row0 + mi * 16 + g, i1 = i0 + 8;
+            prow_idx[mi][0] = i0 < n ? pos2row[i0] : -1;
+            prow_idx[mi][1] = i1 < n ? pos2row[i1] : -1;
           }
+          for (int kk = 0; kk < w; kk += 4) {
+            const int kc = kk + t;
+            cplx af[2][2], bf[4];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                int pr = prow_idx[mi][h];
+                af[mi][h] = (pr >= 0 && kc < w) ? P[pidx(pr, kc, WP)] : cmk(0, 0);
+              }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) bf[ni] = (kc < w) ? R[kc * LDR + col0 + ni * 8 + g] : cmk(0, 0);
+            // real parts first, then imaginary: 16 independent accumulators
+            // separate the two products that feed the same accumulator
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+              for (int ni = 0; ni < 4; ++ni) {
+                dmma(acc_re[mi][ni], af[mi][0].x, af[mi][1].x, bf[ni].x);
+                dmma(acc_im[mi][ni], af[mi][0].x, af[mi][1].x, bf[ni].y);
+              }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+              for (int ni = 0; ni < 4; ++ni) {
+                dmma(acc_re[mi][ni], -af[mi][0].y, -af[mi][1].y, bf[ni].y);
+                dmma(acc_im[mi][ni], af[mi][0].y, af[mi][1].y, bf[ni].x);
+              }
+          }
+#pragma unroll
+          for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                int i = row0 + mi * 16 + g + ((q >> 1) << 3);
+                int c = c0 + col0 + ni * 8 + 2 * t + (q & 1);
+                if (i < n && c < n && !(c >= k0 && c < k0 + w))
+                  X[(int64_t)i * ldx + c] = cmk(acc_re[mi][ni][q], acc_im[mi][ni][q]);
+              }
         }
         __syncthreads();
+        slab = nxt;
+        buf ^= 1;
       }
+      cp_async_wait<0>();
+      // ---- panel columns: final panel values in the new row order
+      for (int idx = tid; idx < n * w; idx += THREADS) {
+        int i = idx / w, c = idx % w;
+        X[(int64_t)i * ldx + k0 + c] = P[pidx(pos2row[i], c, WP)];
+      }
+      // rows are now in the new order: the pivot rows so far sit at positions < k0 + w
+      for (int r = tid; r < n; r += THREADS) s_rowflag[r] = (r < k0 + w) ? 1 : 0;
+      __syncthreads();
     }
 
-    // undo the row interchanges as column interchanges, in reverse order
-    for (int c = tid; c < n; c += THREADS) sigma[c] = c;
+    // ---- undo the row interchanges as column interchanges, in reverse order
+    int* colsrc = pos2row;  // reuse: column permutation
+    for (int c = tid; c < n; c += THREADS) colsrc[c] = c;
     __syncthreads();
     if (tid == 0) {
       for (int k = n - 1; k >= 0; --k) {
-        int p = perm[k];
-        int t = sigma[k];
-        sigma[k] = sigma[p];
-        sigma[p] = t;
+        int q = perm[k];
+        int tmp = colsrc[k];
+        colsrc[k] = colsrc[q];
+        colsrc[q] = tmp;
       }
     }
     __syncthreads();
     {
-      // rows in slabs through the (now free) panel buffer
-      const int rows_per_slab = max(1, (n * LDP) / n);
+      const int rows_per_slab = max(1, (int)((size_t)n * WP / n));
       for (int r0 = 0; r0 < n; r0 += rows_per_slab) {
         int nr = min(rows_per_slab, n - r0);
         for (int idx = tid; idx < nr * n; idx += THREADS) {
@@ -248,7 +381,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         __syncthreads();
         for (int idx = tid; idx < nr * n; idx += THREADS) {
           int r = idx / n, c = idx % n;
-          X[(int64_t)(r0 + r) * ldx + c] = P[r * n + sigma[c]];
+          X[(int64_t)(r0 + r) * ldx + c] = P[r * n + colsrc[c]];
         }
         __syncthreads();
       }
@@ -262,7 +395,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
 void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t stream) {
   if (n <= 0 || batch <= 0) return;
-  if (n > 1024) throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size above 1024");
+  if (n > 512) throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size above 512");
   size_t smem = inv_smem_bytes(n);
   static size_t configured = 0;
   if (smem > configured) {
@@ -270,9 +403,11 @@ void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const in
     configured = smem;
   }
   InvShape s = inv_shape(n);
-  // every row of the update must be owned: rows per thread <= MAX_RPT
-  int ty = THREADS / (s.CW / CPT);
-  if ((n + ty - 1) / ty > MAX_RPT) throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size too large");
+  // every panel row / column must be owned by the elimination mapping
+  int rows_per_thread = (n + (THREADS / s.tpr) - 1) / (THREADS / s.tpr);
+  int cols_per_thread = (s.w + s.tpr - 1) / s.tpr;
+  if (rows_per_thread > MAX_RPT || cols_per_thread > MAX_CPT)
+    throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size outside the supported shapes");
   int grid = (int)(batch < 65535 ? batch : 65535);
   zinv_gj_kernel<<<grid, THREADS, smem, stream>>>(n, batch, a.ptr, a.ld, a.stride, x.ptr, x.ld, x.stride, info,
                                                   active);

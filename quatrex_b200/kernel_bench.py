@@ -1,0 +1,148 @@
+"""Fixed-shape launches of the hot kernels, timed with CUDA events.
+
+``python -m quatrex_b200.kernel_bench gemm --b 256 --batch 128 --launches 5``
+runs the batched complex GEMM of one RGF block product (b x b x b, ``batch``
+energies) ``launches`` times after one warm-up launch and prints the mean
+device time and TFLOP/s (8 b^3 flops per complex product).  ``inv`` does the
+same for the batched block inverse (8 b^3 flops per block), ``sr`` for one
+Sancho-Rubio solve.  The same invocations are the targets of the ncu captures
+summarised under profiles/.  Inputs are seeded, in HBM, and larger than L2 for
+the default shapes (3 x 128 MiB operands at b = 256).
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import sys
+
+import numpy as np
+import torch
+
+from quatrex_b200 import _lib
+
+
+def _rand(g, *shape):
+    return torch.complex(torch.randn(*shape, generator=g, dtype=torch.float64),
+                         torch.randn(*shape, generator=g, dtype=torch.float64)).cuda()
+
+
+def bench_gemm(b: int, batch: int, launches: int, op_b: int = 0, precision: int = 0) -> dict:
+    g = torch.Generator().manual_seed(1)
+    a = _rand(g, batch, b, b)
+    bb = _rand(g, batch, b, b)
+    d = torch.empty_like(a)
+    lib = _lib.load()
+    ctx = _lib.context(torch.cuda.current_device())
+    s = torch.cuda.current_stream().cuda_stream
+
+    def run():
+        st = lib.qtx_zgemm(ctx, b, b, b, batch, 1.0, 0.0, a.data_ptr(), b, b * b, 0, bb.data_ptr(), b, b * b, op_b,
+                           0.0, 0.0, None, b, b * b, d.data_ptr(), b, b * b, precision, s)
+        _lib.check(st, ctx, "zgemm")
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(launches):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    flops = 8.0 * b ** 3 * batch
+    ref = a[:2] @ (bb[:2] if op_b == 0 else bb[:2].conj().transpose(-1, -2))
+    err = float(torch.linalg.norm(d[:2] - ref) / torch.linalg.norm(ref))
+    return {"kernel": "zgemm", "b": b, "batch": batch, "ms": ms, "tflops": flops / ms / 1e9, "rel_err": err,
+            "bytes_min": 3 * batch * b * b * 16}
+
+
+def bench_inv(b: int, batch: int, launches: int) -> dict:
+    rng = np.random.default_rng(2)
+    a = rng.standard_normal((batch, b, b)) + 1j * rng.standard_normal((batch, b, b)) + np.sqrt(b) * np.eye(b)
+    ta = torch.from_numpy(a).cuda()
+    x = torch.empty_like(ta)
+    lib = _lib.load()
+    ctx = _lib.context(torch.cuda.current_device())
+    s = torch.cuda.current_stream().cuda_stream
+
+    def run():
+        _lib.check(lib.qtx_inv(ctx, b, batch, ta.data_ptr(), b * b, x.data_ptr(), b * b, s), ctx, "inv")
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(launches):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    err = float(np.linalg.norm(x[:2].cpu().numpy() @ a[:2] - np.eye(b)) / np.sqrt(2 * b))
+    return {"kernel": "zinv", "b": b, "batch": batch, "ms": ms, "tflops": 8.0 * b ** 3 * batch / ms / 1e9,
+            "residual": err}
+
+
+def bench_sr(b: int, batch: int, launches: int) -> dict:
+    from quatrex_b200.obc import SanchoRubio
+    from quatrex_b200.workloads import make_device
+
+    dev = make_device(num_blocks=2, block_size=b, num_energies=batch, seed=5)
+    d, u, lo = dev.system_blocks()
+    tii = torch.from_numpy(d[0]).cuda()
+    tij = torch.from_numpy(u[0][0]).cuda()
+    tji = torch.from_numpy(lo[0][0]).cuda()
+    sr = SanchoRubio(200, 1e-12)
+    sr(tii, tij, tji)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(launches):
+        sr(tii, tij, tji)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    it = float(np.mean(sr.last_iterations))
+    return {"kernel": "sancho_rubio", "b": b, "batch": batch, "ms": ms, "mean_iterations": it,
+            "tflops": 8.0 * b ** 3 * batch * (7 * it + 1) / ms / 1e9}
+
+
+def probe_fp64_peak() -> dict:
+    lib = _lib.load()
+    out = {}
+    for kind, name in ((0, "dmma_m8n8k4_tflops"), (1, "dfma_tflops")):
+        v = ctypes.c_double()
+        torch.cuda.init()
+        st = lib.qtx_probe_fp64_peak(kind, ctypes.byref(v))
+        if st != _lib.QTX_OK:
+            raise RuntimeError(f"qtx_probe_fp64_peak failed with status {st}")
+        out[name] = v.value
+    return {"kernel": "fp64_peak_probe", **out}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description="fixed-shape kernel timing")
+    ap.add_argument("kernel", choices=["gemm", "gemm_h", "inv", "sr", "fp64peak"])
+    ap.add_argument("--b", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=128)
+    ap.add_argument("--launches", type=int, default=5)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    args = ap.parse_args(argv)
+    prec = 0 if args.precision == "fp64" else 1
+    if args.kernel == "fp64peak":
+        r = probe_fp64_peak()
+    elif args.kernel == "gemm":
+        r = bench_gemm(args.b, args.batch, args.launches, 0, prec)
+    elif args.kernel == "gemm_h":
+        r = bench_gemm(args.b, args.batch, args.launches, 1, prec)
+    elif args.kernel == "inv":
+        r = bench_inv(args.b, args.batch, args.launches)
+    else:
+        r = bench_sr(args.b, args.batch, args.launches)
+    print(json.dumps(r), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
