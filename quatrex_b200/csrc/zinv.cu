@@ -44,7 +44,7 @@ struct InvShape {
 
 __host__ __device__ inline InvShape inv_shape(int n) {
   InvShape s;
-  s.w = n <= 64 ? n : (n <= 256 ? 32 : 16);
+  s.w = n <= 32 ? n : (n <= 256 ? (n <= 96 ? 16 : 32) : 16);
   s.wp = (s.w + 7) / 8 * 8;
   int row_tiles = (n + 31) / 32;
   int col_tiles = row_tiles >= NWARPS ? 1 : NWARPS / row_tiles;
