@@ -196,6 +196,7 @@ def run_ours(args):
     import torch.distributed as dist
 
     from quatrex_b200 import _lib
+    from quatrex_b200.energy_shards import max_over_ranks
     from quatrex_b200.transport import TransportSolver
     from quatrex_b200.workloads import make_device
 
@@ -253,10 +254,7 @@ def run_ours(args):
     inv = _lib.timing_report(1, local)
     _lib.set_timing(False, local)
     sr_its = out["sr_iterations"].cpu().numpy()
-    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, device=f"cuda:{local}")
     value = world * args.steps * E / (elapsed_ms / 1000.0)
 
     # ---- end to end through the public API: H and energies from pinned host memory,
@@ -288,10 +286,8 @@ def run_ours(args):
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device=f"cuda:{local}")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * args.steps * E / (float(t.item()) / 1000.0), "unit": "solves/s",
+        e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), device=f"cuda:{local}")
+        e2e = {"value": world * args.steps * E / (e2e_ms / 1000.0), "unit": "solves/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
     # ---- roofline of the dominant kernel (batched complex FP64 GEMM on DMMA)

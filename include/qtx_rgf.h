@@ -172,6 +172,15 @@ qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const void* a_ii, 
                                     double convergence_tol, int32_t max_iterations, void* x, int32_t* iterations,
                                     qtx_stream stream, char* err, int32_t err_len);
 
+/* One fixed-point step of the surface Green's function and its residuals:
+ * x_ref = inv(a_ii - a_ji x a_ij), abs_res = ||x_ref - x||_F,
+ * rel_res = abs_res / ||x_ref||_F per batch entry (device arrays, may be NULL).
+ * <- OBCSystem._fixed_point_step / _get_residuals
+ *    (src/qttools/boundary_conditions/obc/obc.py:105-130, 156-202). */
+qtx_status qtx_obc_fixed_point(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                               const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
+                               const void* x, void* x_ref, double* abs_res, double* rel_res, qtx_stream stream);
+
 /* Contact self-energies from a surface Green's function g (batch, n, n):
  * sigma_r = m_ji g m_ij, gamma = i (sigma_r - sigma_r^H),
  * sigma_l = i f gamma, sigma_g = i (f - 1) gamma with f = occupancy[batch]

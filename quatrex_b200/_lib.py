@@ -139,6 +139,11 @@ SIGNATURES = {
         [c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_double, c_int32, c_void_p,
          c_void_p, c_void_p, ctypes.c_char_p, c_int32],
     ),
+    "qtx_obc_fixed_point": (
+        c_int32,
+        [c_void_p, c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p,
+         c_void_p, c_void_p, c_void_p],
+    ),
     "qtx_obc_assemble": (
         c_int32,
         [c_void_p, c_int32, c_int64, c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p,

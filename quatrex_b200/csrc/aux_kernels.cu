@@ -291,6 +291,34 @@ __global__ void real_part_kernel(int64_t count, const cplx* src, double* dst) {
 
 }  // namespace
 
+namespace {
+// abs_res[e] = ||x_ref - x||_F, rel_res[e] = abs_res[e] / ||x_ref||_F
+__global__ void residual_norm_kernel(int n, int64_t batch, const cplx* xr, int64_t sr, const cplx* x, int64_t sx,
+                                     double* abs_res, double* rel_res) {
+  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
+    double d2 = 0, r2 = 0;
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+      cplx a = xr[e * sr + q], b = x[e * sx + q];
+      double dx = a.x - b.x, dy = a.y - b.y;
+      d2 += dx * dx + dy * dy;
+      r2 += a.x * a.x + a.y * a.y;
+    }
+    cplx s = block_sum(cmk(d2, r2));
+    if (threadIdx.x == 0) {
+      abs_res[e] = sqrt(s.x);
+      rel_res[e] = s.y > 0 ? sqrt(s.x) / sqrt(s.y) : INFINITY;
+    }
+  }
+}
+}  // namespace
+
+void launch_residual_norm(int n, int64_t batch, MatView x_ref, MatView x, double* abs_res, double* rel_res,
+                          cudaStream_t stream) {
+  unsigned g = (unsigned)(batch < 65535 ? batch : 65535);
+  residual_norm_kernel<<<g, TB, 0, stream>>>(n, batch, x_ref.ptr, x_ref.stride, x.ptr, x.stride, abs_res, rel_res);
+  qtx_check_launch("residual_norm_kernel");
+}
+
 void launch_skew_combine(int n, int64_t batch, MatView s, MatView w, MutView out, cudaStream_t stream) {
   int tiles = (n + 31) / 32;
   skew_combine_kernel<<<grid_for(batch * tiles * tiles * TB), TB, 0, stream>>>(

@@ -1064,6 +1064,31 @@ qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
   return st;
 }
 
+qtx_status qtx_obc_fixed_point(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                               const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
+                               const void* x, void* x_ref, double* abs_res, double* rel_res, qtx_stream stream) {
+  return guarded(ctx, [&] {
+    if (n < 1 || batch < 1 || !a_ii || !a_ij || !a_ji || !x || !x_ref) throw QtxError(QTX_E_INVAL, "qtx_obc_fixed_point");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int64_t bb = (int64_t)n * n;
+    DevBuf t(sizeof(cplx) * 2 * bb * batch, s);
+    MutView t0{t.as<cplx>(), n, bb}, t1{t.as<cplx>() + bb * batch, n, bb};
+    MatView aii{reinterpret_cast<const cplx*>(a_ii), n, stride_ii};
+    MatView aij{reinterpret_cast<const cplx*>(a_ij), n, stride_ij};
+    MatView aji{reinterpret_cast<const cplx*>(a_ji), n, stride_ji};
+    MatView xv{reinterpret_cast<const cplx*>(x), n, bb};
+    // x_ref = inv(a_ii - a_ji x a_ij)
+    gemm(n, n, n, batch, ONE, aji, OP_N, xv, OP_N, t0, s);
+    gemm(n, n, n, batch, MONE, t0, OP_N, aij, OP_N, t1, s, aii, ONE);
+    DevBuf info(sizeof(int) * batch, s);
+    QTX_CUDA_TRY(cudaMemsetAsync(info.as<int>(), 0, sizeof(int) * batch, s));
+    zinv(n, batch, t1, MutView{reinterpret_cast<cplx*>(x_ref), n, bb}, info.as<int>(), nullptr, s);
+    if (abs_res && rel_res)
+      launch_residual_norm(n, batch, MatView{reinterpret_cast<cplx*>(x_ref), n, bb}, xv, abs_res, rel_res, s);
+    read_info_or_throw(ctx, info.as<int>(), batch, s, "qtx_obc_fixed_point");
+  });
+}
+
 qtx_status qtx_obc_assemble(qtx_ctx* ctx, int32_t n, int64_t batch, const void* g, const void* m_ji,
                             int64_t stride_ji, const void* m_ij, int64_t stride_ij, const double* occupancy,
                             void* sigma_r, void* sigma_l, void* sigma_g, qtx_stream stream) {
