@@ -36,9 +36,14 @@ struct GemmCall {
 };
 void launch_zgemm(const GemmCall& g, cudaStream_t stream);
 
-// Mixed-precision (3xTF32 on tcgen05) variant of the same contract.
-void launch_zgemm_tf32x3(const GemmCall& g, cudaStream_t stream);
-bool tf32x3_supported(const GemmCall& g);
+// Mixed-precision variant of the same contract: FP64 operands split into
+// 7-bit integer slices whose products run on tcgen05 kind::i8 with exact
+// INT32 accumulation (Ozaki scheme); see zgemm_ozaki.cu.
+void launch_zgemm_mixed(const GemmCall& g, cudaStream_t stream);
+bool mixed_supported(const GemmCall& g);
+// Throws QTX_E_TIMEOUT (and clears the flag) if a mixed GEMM since the last
+// check gave up a pipeline wait.  Synchronises the stream.
+void mixed_check_error(cudaStream_t stream);
 
 // Batched in-place-capable Gauss-Jordan inverse with partial pivoting:
 // X = A^-1 for n x n matrices.  info[e] (device, optional) receives 0 or the

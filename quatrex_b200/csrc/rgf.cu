@@ -243,7 +243,7 @@ void gemm(int m, int n, int k, int64_t batch, cplx alpha, MatView a, int op_a, M
   g.c = c; g.beta = beta; g.c2 = c2; g.gamma = gamma;
   g.d = d; g.alpha = alpha; g.active = active; g.diag_shift = diag_shift;
   TimedScope ts(0, 8.0 * m * n * (double)k * batch, s);
-  if (precision == QTX_PREC_MIXED && tf32x3_supported(g)) launch_zgemm_tf32x3(g, s);
+  if (precision == QTX_PREC_MIXED && mixed_supported(g)) launch_zgemm_mixed(g, s);
   else launch_zgemm(g, s);
 }
 
@@ -384,6 +384,7 @@ void selected_inv_impl(qtx_ctx* ctx, const Btd& a, const void* const* obc_r, con
     }
   }
   read_info_or_throw(ctx, info, ne_max * nb, s, "selected_inv");
+  if (precision == QTX_PREC_MIXED) mixed_check_error(s);
 }
 
 // ---------------------------------------------------------------------------
@@ -596,6 +597,7 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
     }
   }
   read_info_or_throw(ctx, info, ne_max * nb, s, "selected_solve");
+  if (prec == QTX_PREC_MIXED) mixed_check_error(s);
 }
 
 // ---------------------------------------------------------------------------
@@ -841,6 +843,7 @@ void transport_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qtx_tran
     }
   }
   read_info_or_throw(ctx, info, (int64_t)nb * ne_max, s, "transport_solve");
+  if (prec == QTX_PREC_MIXED) mixed_check_error(s);
 }
 
 // ---------------------------------------------------------------------------
@@ -979,6 +982,7 @@ qtx_status qtx_zgemm(qtx_ctx* ctx, int32_t m, int32_t n, int32_t k, int64_t batc
          MutView{reinterpret_cast<cplx*>(d), ldd, stride_d}, s,
          MatView{reinterpret_cast<const cplx*>(c), ldc, stride_c}, cmk(beta_re, beta_im), MatView{}, ZERO, nullptr,
          nullptr, precision);
+    if (precision == QTX_PREC_MIXED) mixed_check_error(s);
   });
 }
 
