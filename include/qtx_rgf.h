@@ -72,6 +72,8 @@ typedef int qtx_status;
 #define QTX_FLAG_SYMMETRIC_OUT 0x4u    /* outputs store the upper triangle only (rgf.py:351, 373) */
 #define QTX_FLAG_HOST_BUFFERS 0x8u     /* every data pointer is host memory */
 #define QTX_FLAG_RETARDED_OFFDIAG 0x10u /* also write X^R off-diagonal blocks into xr */
+#define QTX_FLAG_GRAPH 0x20u           /* qtx_transport_solve: capture the sweep of a single-batch call as a
+                                          CUDA graph, cache it per (shapes, buffers, precision) and replay it */
 
 typedef struct qtx_ctx qtx_ctx;
 typedef struct CUstream_st* qtx_stream; /* == cudaStream_t; NULL = legacy default stream */
@@ -222,6 +224,9 @@ typedef struct qtx_transport_outputs {
 
 qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,
                                int32_t precision, uint32_t flags, qtx_stream stream);
+
+/* Number of captured-sweep replays issued by this context (QTX_FLAG_GRAPH). */
+int64_t qtx_graph_replays(const qtx_ctx* ctx);
 
 /* FP64 roofline probe -- no counterpart in the upstream code.  Measures the
  * issue-rate ceiling of the FP64 tensor path (kind 0: DMMA mma.sync m8n8k4)

@@ -34,6 +34,7 @@ QTX_FLAG_RETURN_CURRENT = 0x2
 QTX_FLAG_SYMMETRIC_OUT = 0x4
 QTX_FLAG_HOST_BUFFERS = 0x8
 QTX_FLAG_RETARDED_OFFDIAG = 0x10
+QTX_FLAG_GRAPH = 0x20
 
 c_void_p = ctypes.c_void_p
 c_int32 = ctypes.c_int32
@@ -107,6 +108,7 @@ SIGNATURES = {
     "qtx_ctx_set_memory_limit": (c_int32, [c_void_p, ctypes.c_size_t]),
     "qtx_ctx_trim": (c_int32, [c_void_p]),
     "qtx_launch_count": (c_int64, [c_void_p]),
+    "qtx_graph_replays": (c_int64, [c_void_p]),
     "qtx_ctx_set_timing": (c_int32, [c_void_p, ctypes.c_int]),
     "qtx_ctx_timing_report": (
         c_int32, [c_void_p, c_int32, ctypes.POINTER(c_double), ctypes.POINTER(c_double), ctypes.POINTER(c_int64)]),
@@ -204,6 +206,20 @@ def context(device: int) -> int:
             h = p.value
             _ctx[device] = h
         return h
+
+
+def new_context(device: int) -> int:
+    """A fresh qtx_ctx handle (one per host thread that drives its own stream)."""
+    lib = load()
+    p = c_void_p()
+    st = lib.qtx_ctx_create(device, ctypes.byref(p))
+    if st != QTX_OK:
+        raise QtxError(st, f"qtx_ctx_create(device={device}) failed")
+    return p.value
+
+
+def destroy_context(ctx: int) -> None:
+    load().qtx_ctx_destroy(ctx)
 
 
 def check(status: int, ctx: int, what: str) -> None:

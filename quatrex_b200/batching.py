@@ -1,0 +1,161 @@
+"""Uneven batches of transport instances on one GPU.
+
+Instances differ in block size, number of blocks and energy grid.  Each is
+solved by a worker that owns a CUDA stream and its own library context, so
+several instances run on the device at the same time (small instances alone
+cannot fill 148 SMs); instances are handed out longest first.  Per instance
+the energy grid is cut into device calls of the size the autotuner picked for
+(block size, number of energies, precision), and the sweep of every full-size
+call is a replayed CUDA graph when the tuner found that faster.
+
+Only observables travel back to the host (per-block density and hole
+density, transmission, contact currents, Sancho-Rubio iteration counts); the
+Green's-function blocks stay on the device inside each call.
+"""
+
+from __future__ import annotations
+
+import math
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from quatrex_b200 import _lib
+from quatrex_b200.autotune import Autotuner
+from quatrex_b200.transport import TransportSolver
+from quatrex_b200.workloads import TransportDevice
+
+OBSERVABLE_KEYS = ("density", "hole_density", "transmission", "current_left", "current_right", "sr_iterations")
+
+
+def instance_flops(dev: TransportDevice, num_energies: int) -> float:
+    """Algorithmic flops of one instance (8 b^3 per block product, ~26 per
+    block step, Sancho-Rubio at ~22 iterations per contact)."""
+    b, nb = dev.block_size, dev.num_blocks
+    return 8.0 * b ** 3 * (26 * (nb - 1) + 11 + 2 * (7 * 22 + 1)) * num_energies
+
+
+class Worker:
+    """A CUDA stream plus its own library context, driven by one host thread."""
+
+    def __init__(self, cuda_device: int):
+        self.cuda = cuda_device
+        self.stream = torch.cuda.Stream(device=cuda_device)
+        self.ctx = _lib.new_context(cuda_device)
+        self.busy_s = 0.0
+
+    def close(self):
+        if self.ctx:
+            torch.cuda.synchronize(self.cuda)
+            _lib.destroy_context(self.ctx)
+            self.ctx = None
+
+    def solve(self, dev: TransportDevice, energies: np.ndarray, precision: str, choice: dict,
+              keys=OBSERVABLE_KEYS) -> dict:
+        """Solve one instance on this worker's stream; returns host arrays."""
+        t0 = time.perf_counter()
+        ne_call = int(choice["energies_per_call"])
+        path = choice.get("gemm_path", precision)
+        graph = bool(choice.get("graph", False))
+        energies = np.asarray(energies, dtype=np.float64)
+        results = {k: [] for k in keys}
+        with torch.cuda.stream(self.stream):
+            h_diag = torch.from_numpy(dev.h_diag).to(f"cuda:{self.cuda}", non_blocking=False)
+            h_upper = torch.from_numpy(dev.h_upper).to(f"cuda:{self.cuda}", non_blocking=False)
+            solver = TransportSolver(dev, max_batch_size=ne_call, precision=path, cuda_device=self.cuda,
+                                     h_diag=h_diag, h_upper=h_upper, ctx=self.ctx, stream=self.stream,
+                                     use_graph=graph)
+            outs = {}
+            for c0 in range(0, len(energies), ne_call):
+                chunk = energies[c0:c0 + ne_call]
+                n = len(chunk)
+                if n not in outs:
+                    outs[n] = solver.allocate_outputs(n, keys)
+                out = solver.solve(chunk, outs[n])
+                for k in keys:
+                    results[k].append(out[k].cpu())
+            self.stream.synchronize()
+        self.busy_s += time.perf_counter() - t0
+        return {k: torch.cat(v).numpy() for k, v in results.items()}
+
+
+@dataclass
+class Instance:
+    device: TransportDevice
+    energies: np.ndarray
+
+
+class BatchedTransport:
+    """Solve a list of uneven instances with ``streams`` concurrent workers."""
+
+    def __init__(self, precision: str = "fp64", streams: int = 4, tuner: Autotuner | None = None,
+                 cuda_device: int | None = None, keys=OBSERVABLE_KEYS):
+        self.precision = precision
+        self.cuda = torch.cuda.current_device() if cuda_device is None else cuda_device
+        self.tuner = tuner if tuner is not None else Autotuner()
+        self.keys = keys
+        self.workers = [Worker(self.cuda) for _ in range(max(1, streams))]
+        self._free = list(self.workers)
+        self._cv = threading.Condition()
+
+    def close(self):
+        for w in self.workers:
+            w.close()
+
+    def _take(self) -> Worker:
+        with self._cv:
+            while not self._free:
+                self._cv.wait()
+            return self._free.pop()
+
+    def _give(self, w: Worker):
+        with self._cv:
+            self._free.append(w)
+            self._cv.notify()
+
+    def choice_for(self, inst: Instance) -> dict:
+        return self.tuner.best(inst.device.block_size, len(inst.energies), self.precision)
+
+    def run(self, instances: list[Instance]) -> list[dict]:
+        """Results in input order; each dict also holds 'seconds' (wall time on its worker)."""
+        order = sorted(range(len(instances)),
+                       key=lambda i: -instance_flops(instances[i].device, len(instances[i].energies)))
+        # tune every key up front (serially), so workers only read the table
+        for i in order:
+            self.choice_for(instances[i])
+        results: list[dict | None] = [None] * len(instances)
+
+        def job(i):
+            w = self._take()
+            try:
+                t0 = time.perf_counter()
+                r = w.solve(instances[i].device, instances[i].energies, self.precision,
+                            self.choice_for(instances[i]), self.keys)
+                r["seconds"] = time.perf_counter() - t0
+                results[i] = r
+            finally:
+                self._give(w)
+
+        with ThreadPoolExecutor(max_workers=len(self.workers)) as ex:
+            list(ex.map(job, order))
+        return results
+
+
+def total_solves(instances: list[Instance]) -> int:
+    return int(sum(len(x.energies) for x in instances))
+
+
+def total_flops(instances: list[Instance]) -> float:
+    return float(sum(instance_flops(x.device, len(x.energies)) for x in instances))
+
+
+def geometric_energies(n: int, e_min: float = -2.0, e_max: float = 2.0) -> np.ndarray:
+    return np.linspace(e_min, e_max, int(n))
+
+
+def ceil_div(a: int, b: int) -> int:
+    return int(math.ceil(a / b))

@@ -27,8 +27,73 @@ struct TimedLaunch {
   double flops;
 };
 
+struct GraphKey {
+  std::vector<uintptr_t> v;
+  bool operator==(const GraphKey& o) const { return v == o.v; }
+};
+
+struct GraphEntry {
+  GraphKey key;
+  void* mem = nullptr;
+  size_t bytes = 0;
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;
+  uint64_t last_use = 0;
+};
+
+// Small LRU cache of captured sweeps (each holds its work space).
+struct GraphCache {
+  std::vector<GraphEntry> entries;
+  uint64_t clock = 0;
+  size_t capacity = 8;
+  GraphEntry* find(const GraphKey& k) {
+    for (auto& e : entries)
+      if (e.key == k) {
+        e.last_use = ++clock;
+        return &e;
+      }
+    return nullptr;
+  }
+  static void release(GraphEntry& e) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (e.mem) cudaFree(e.mem);
+    e.exec = nullptr;
+    e.mem = nullptr;
+  }
+  GraphEntry* insert(const GraphKey& k) {
+    if (entries.size() >= capacity) {
+      size_t victim = 0;
+      for (size_t i = 1; i < entries.size(); ++i)
+        if (entries[i].last_use < entries[victim].last_use) victim = i;
+      cudaDeviceSynchronize();
+      release(entries[victim]);
+      entries.erase(entries.begin() + victim);
+    }
+    entries.push_back(GraphEntry{});
+    entries.back().key = k;
+    entries.back().last_use = ++clock;
+    return &entries.back();
+  }
+  void erase(const GraphKey& k) {
+    for (size_t i = 0; i < entries.size(); ++i)
+      if (entries[i].key == k) {
+        release(entries[i]);
+        entries.erase(entries.begin() + i);
+        return;
+      }
+  }
+  void clear() {
+    for (auto& e : entries) release(e);
+    entries.clear();
+  }
+};
+
 struct qtx_ctx {
   int device = 0;
+  GraphCache graphs;
+  cudaStream_t capture_stream = nullptr;  // graphs are captured here (the legacy stream cannot be)
+  bool capturing = false;
+  int64_t graph_replays = 0;
   std::string last_error;
   int64_t launches = 0;
   size_t mem_limit = 0;
@@ -61,7 +126,7 @@ struct TimedScope {
   cudaStream_t s;
   TimedLaunch t;
   TimedScope(int kind, double flops, cudaStream_t stream) : c(g_timing_ctx), s(stream) {
-    if (!c || !c->timing) { c = nullptr; return; }
+    if (!c || !c->timing || c->capturing) { c = nullptr; return; }
     t.kind = kind;
     t.flops = flops;
     t.start = pool_event(c);
@@ -652,197 +717,326 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
 // Generator-form transport solve (ElectronSolver.solve for a device whose leads
 // repeat its end cells; interior scattering self-energies are zero)
 // ---------------------------------------------------------------------------
+// Work space of one energy batch: couplings, the three block stacks, temporaries,
+// contact buffers and small per-energy arrays, carved from one allocation.
+struct TransportWS {
+  int nb = 0, b = 0;
+  int64_t ne_max = 0;
+  cplx* a_up = nullptr;  // A_i,i+1 = -H_i,i+1
+  cplx* a_lo = nullptr;  // A_i+1,i = -H_i,i+1^H
+  BlockStack xr, xl, xg;
+  cplx* T[10];
+  cplx* C[10];  // g_L, g_R, SigR_L, SigR_R, SigL_L, SigL_R, SigG_L, SigG_R, Gam_L, Gam_R
+  cplx *shift = nullptr, *tr = nullptr, *cl = nullptr, *cr = nullptr;
+  double *occ_l = nullptr, *occ_r = nullptr;
+  int *info = nullptr, *its = nullptr;
+};
+
+size_t transport_ws_bytes(int nb, int b, int64_t ne_max) {
+  const size_t bb = (size_t)b * b, tmp = bb * ne_max;
+  const size_t cplx_elems = 2 * bb * std::max(nb - 1, 1) + 3 * (size_t)nb * tmp + 20 * tmp + 4 * ne_max;
+  return sizeof(cplx) * cplx_elems + sizeof(double) * 2 * ne_max + sizeof(int) * (nb + 2) * ne_max + 256;
+}
+
+TransportWS carve_transport_ws(void* mem, int nb, int b, int64_t ne_max) {
+  TransportWS w;
+  w.nb = nb;
+  w.b = b;
+  w.ne_max = ne_max;
+  const int64_t bb = (int64_t)b * b;
+  const size_t tmp = (size_t)bb * ne_max;
+  cplx* cur = reinterpret_cast<cplx*>(mem);
+  w.a_up = cur;
+  cur += bb * std::max(nb - 1, 1);
+  w.a_lo = cur;
+  cur += bb * std::max(nb - 1, 1);
+  std::vector<int> sizes(nb, b);
+  w.xr = carve(cur, sizes, ne_max, b);
+  w.xl = carve(cur, sizes, ne_max, b);
+  w.xg = carve(cur, sizes, ne_max, b);
+  for (int q = 0; q < 10; ++q) { w.T[q] = cur; cur += tmp; }
+  for (int q = 0; q < 10; ++q) { w.C[q] = cur; cur += tmp; }
+  w.shift = cur; cur += ne_max;
+  w.tr = cur; cur += ne_max;
+  w.cl = cur; cur += ne_max;
+  w.cr = cur; cur += ne_max;
+  w.occ_l = reinterpret_cast<double*>(cur);
+  w.occ_r = w.occ_l + ne_max;
+  w.info = reinterpret_cast<int*>(w.occ_r + ne_max);
+  w.its = w.info + nb * ne_max;
+  return w;
+}
+
+// A_i,i+1 = -H_i,i+1 ; A_i+1,i = -H_i,i+1^H (energy independent)
+void transport_couplings(const TransportWS& w, const cplx* h_upper, cudaStream_t s) {
+  const int b = w.b;
+  const int64_t bb = (int64_t)b * b;
+  for (int i = 0; i + 1 < w.nb; ++i) {
+    launch_axpby(b, b, 1, MONE, MatView{h_upper + i * bb, b, bb}, ZERO, {}, MutView{w.a_up + i * bb, b, bb}, s);
+    launch_neg_herm(b, h_upper + i * bb, w.a_lo + i * bb, s);
+  }
+}
+
+// Contacts of energies [e0, e0 + ne) (src/quatrex/electron/solver.py:305-386):
+// Sancho-Rubio on both leads (host-synchronising convergence checks), then
+// Sigma^R, Gamma, Sigma^<, Sigma^> and the (E + i eta) shifts, all into `w`.
+bool transport_contacts(qtx_ctx* ctx, const TransportWS& w, const qtx_transport_problem& P,
+                        const qtx_transport_outputs& O, int64_t e0, int64_t ne, cudaStream_t s) {
+  const int nb = w.nb, b = w.b;
+  const int64_t bb = (int64_t)b * b;
+  const cplx* h_diag = reinterpret_cast<const cplx*>(P.h_diag);
+  auto up = [&](int i) { return MatView{w.a_up + i * bb, b, 0}; };
+  auto lo = [&](int i) { return MatView{w.a_lo + i * bb, b, 0}; };
+  auto V = [&](cplx* p) { return MutView{p, b, bb}; };
+  const double* en = P.energies + e0;
+  launch_energy_shift(ne, en, P.eta, w.shift, s);
+  // left: g_L = SR(A_00, A_01, A_10)
+  launch_assemble_diag(b, ne, h_diag, en, P.eta, V(w.T[0]), s);
+  bool okl = sancho_rubio_impl(ctx, b, ne, V(w.T[0]), up(0), lo(0), P.sr_tol, P.sr_max_iterations, V(w.C[0]), w.its,
+                               s);
+  if (O.sr_iterations)
+    QTX_CUDA_TRY(cudaMemcpy2DAsync(O.sr_iterations + 2 * e0, 2 * sizeof(int), w.its, sizeof(int), sizeof(int), ne,
+                                   cudaMemcpyDeviceToDevice, s));
+  // right: g_R = SR(A_nn, A_nm, A_mn)
+  launch_assemble_diag(b, ne, h_diag + (int64_t)(nb - 1) * bb, en, P.eta, V(w.T[0]), s);
+  bool okr = sancho_rubio_impl(ctx, b, ne, V(w.T[0]), lo(nb - 2), up(nb - 2), P.sr_tol, P.sr_max_iterations,
+                               V(w.C[1]), w.its, s);
+  if (O.sr_iterations)
+    QTX_CUDA_TRY(cudaMemcpy2DAsync(O.sr_iterations + 2 * e0 + 1, 2 * sizeof(int), w.its, sizeof(int), sizeof(int),
+                                   ne, cudaMemcpyDeviceToDevice, s));
+  // Sigma^R_L = A_10 g_L A_01 ; Sigma^R_R = A_mn g_R A_nm
+  gemm(b, b, b, ne, ONE, lo(0), OP_N, V(w.C[0]), OP_N, V(w.T[1]), s);
+  gemm(b, b, b, ne, ONE, V(w.T[1]), OP_N, up(0), OP_N, V(w.C[2]), s);
+  gemm(b, b, b, ne, ONE, up(nb - 2), OP_N, V(w.C[1]), OP_N, V(w.T[1]), s);
+  gemm(b, b, b, ne, ONE, V(w.T[1]), OP_N, lo(nb - 2), OP_N, V(w.C[3]), s);
+  launch_fermi(ne, en, P.mu_left, P.kt, w.occ_l, s);
+  launch_fermi(ne, en, P.mu_right, P.kt, w.occ_r, s);
+  launch_obc_lesser_greater(b, ne, V(w.C[2]), w.occ_l, V(w.C[4]), V(w.C[6]), V(w.C[8]), s);
+  launch_obc_lesser_greater(b, ne, V(w.C[3]), w.occ_r, V(w.C[5]), V(w.C[7]), V(w.C[9]), s);
+  return okl && okr;
+}
+
+// Selected solve and observables of energies [e0, e0 + ne) once the contacts
+// are in `w`.  Only kernel launches and device-to-device copies: it can be
+// captured into a CUDA graph.  `w` is taken by value: the buffer swaps of the
+// recursion permute this copy only, so every call starts from the same layout.
+void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_transport_outputs& O, int64_t e0,
+                     int64_t ne, int prec, cudaStream_t s) {
+  const int nb = w.nb, b = w.b;
+  const int64_t bb = (int64_t)b * b;
+  const int64_t ne_max = w.ne_max;
+  const cplx* h_diag = reinterpret_cast<const cplx*>(P.h_diag);
+  auto up = [&](int i) { return MatView{w.a_up + i * bb, b, 0}; };
+  auto lo = [&](int i) { return MatView{w.a_lo + i * bb, b, 0}; };
+  auto hd = [&](int i) { return MatView{h_diag + i * bb, b, 0}; };
+  auto V = [&](cplx* p) { return MutView{p, b, bb}; };
+  cplx** T = w.T;
+  cplx** C = w.C;
+  BlockStack& xr = w.xr;
+  BlockStack& xl = w.xl;
+  BlockStack& xg = w.xg;
+  cplx* shift = w.shift;
+  cplx* tr = w.tr;
+  cplx* cl = w.cl;
+  cplx* cr = w.cr;
+  int* info = w.info;
+  auto obc_r = [&](int i) { return i == 0 ? MatView(V(C[2])) : (i == nb - 1 ? MatView(V(C[3])) : MatView{}); };
+  auto obc_x = [&](int comp, int i) {
+    int base = comp == 0 ? 4 : 6;
+    return i == 0 ? MatView(V(C[base])) : (i == nb - 1 ? MatView(V(C[base + 1])) : MatView{});
+  };
+  auto tv = [&](int idx) { return V(T[idx]); };
+  auto out_at = [&](void* base, int64_t blocks_per_e, int blk) {
+    return MutView{reinterpret_cast<cplx*>(base) + (e0 * blocks_per_e + blk) * bb, b, blocks_per_e * bb};
+  };
+
+  // ---- first block: x_0 = inv(A_00 - Sigma^R_L), X_0 = x_0 Sigma_0 x_0^H
+  // M_0 = (E + i eta) I - H_00 - Sigma^R_L
+  // (a K = 0 product: the epilogue alone forms -H_00 - Sigma^R_L + shift on the diagonal)
+  gemm(b, b, 0, ne, ONE, tv(0), OP_N, tv(0), OP_N, tv(1), s, hd(0), MONE, obc_r(0), MONE, nullptr, shift);
+  zinv(b, ne, tv(1), xr.view(0), info, nullptr, s);
+  for (int comp = 0; comp < 2; ++comp) {
+    BlockStack& X = comp == 0 ? xl : xg;
+    gemm(b, b, b, ne, ONE, xr.view(0), OP_N, obc_x(comp, 0), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+         prec);
+    gemm(b, b, b, ne, ONE, tv(2), OP_N, xr.view(0), OP_C, X.view(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+  }
+  // ---- forward sweep
+  for (int i = 0; i + 1 < nb; ++i) {
+    const int j = i + 1;
+    gemm(b, b, b, ne, ONE, lo(i), OP_N, xr.view(i), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    // M = (E + i eta) I - H_jj - Sigma^R_j - U A_ij
+    gemm(b, b, b, ne, MONE, tv(0), OP_N, up(i), OP_N, tv(1), s, hd(j), MONE, obc_r(j), MONE, nullptr, shift, prec);
+    zinv(b, ne, tv(1), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
+    for (int comp = 0; comp < 2; ++comp) {
+      BlockStack& X = comp == 0 ? xl : xg;
+      // V = X_i A_ji^H ; Q = A_ji V + Sigma_obc,j ; X_j = x_j Q x_j^H   (interior Sigma = 0)
+      gemm(b, b, b, ne, ONE, X.view(i), OP_N, lo(i), OP_C, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      gemm(b, b, b, ne, ONE, lo(i), OP_N, tv(3), OP_N, tv(4), s, obc_x(comp, j), ONE, {}, ZERO, nullptr, nullptr,
+           prec);
+      gemm(b, b, b, ne, ONE, xr.view(j), OP_N, tv(4), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      gemm(b, b, b, ne, ONE, tv(5), OP_N, xr.view(j), OP_C, X.view(j), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    }
+  }
+  // ---- last blocks, corner chain start
+  const int n = nb - 1;
+  if (O.gl_diag) launch_block_scatter(b, b, ne, xl.view(n), 1, out_at(O.gl_diag, nb, n).ptr, nb * bb, bb, nullptr, s);
+  if (O.gg_diag) launch_block_scatter(b, b, ne, xg.view(n), 1, out_at(O.gg_diag, nb, n).ptr, nb * bb, bb, nullptr, s);
+  if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, out_at(O.gr_diag, nb, n), s);
+  if (O.density) launch_diag_imag_sum(b, ne, xl.view(n), 1.0, O.density + e0 * nb, nb, n, s);
+  if (O.hole_density) launch_diag_imag_sum(b, ne, xg.view(n), -1.0, O.hole_density + e0 * nb, nb, n, s);
+  // contact current at the right contact uses the symmetrised G^<_nn, G^>_nn
+  if (O.current_right) {
+    launch_block_scatter(b, b, ne, xl.view(n), 1, T[6], bb, bb, nullptr, s);
+    launch_block_scatter(b, b, ne, xg.view(n), 1, T[7], bb, bb, nullptr, s);
+    launch_trace_product(b, b, ne, V(C[7]), tv(6), ONE, cr, false, s);
+    launch_trace_product(b, b, ne, tv(7), V(C[5]), MONE, cr, true, s);
+    QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_right) + e0, cr, sizeof(cplx) * ne,
+                                 cudaMemcpyDeviceToDevice, s));
+  }
+  cplx* corner = T[8];
+  cplx* corner2 = T[9];
+  if (O.transmission) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, V(corner), s);
+  // ---- backward sweep
+  for (int i = nb - 2; i >= 0; --i) {
+    const int j = i + 1;
+    gemm(b, b, b, ne, ONE, xr.view(i), OP_N, up(i), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, xr.view(j), OP_N, lo(i), OP_N, tv(1), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, tv(0), OP_N, xr.view(j), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, tv(0), OP_N, tv(1), OP_N, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    if (O.gr_upper) launch_axpby(b, b, ne, MONE, tv(2), ZERO, {}, out_at(O.gr_upper, nb - 1, i), s);
+    if (O.gr_lower)
+      gemm(b, b, b, ne, MONE, tv(1), OP_N, xr.view(i), OP_N, out_at(O.gr_lower, nb - 1, i), s, {}, ZERO, {}, ZERO,
+           nullptr, nullptr, prec);
+    if (O.transmission) {
+      // G_{i,N-1} = -(x_i A_ij) G_{j,N-1}
+      gemm(b, b, b, ne, MONE, tv(0), OP_N, V(corner), OP_N, V(corner2), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+           prec);
+      std::swap(corner, corner2);
+    }
+    for (int comp = 0; comp < 2; ++comp) {
+      BlockStack& X = comp == 0 ? xl : xg;
+      void* od = comp == 0 ? O.gl_diag : O.gg_diag;
+      void* ou = comp == 0 ? O.gl_upper : O.gg_upper;
+      // t1 = P4 X_i - (P4 X_i)^H ; t2 = P1 X_j
+      gemm(b, b, b, ne, ONE, tv(3), OP_N, X.view(i), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      launch_sub_herm_inplace(b, ne, tv(5), s);
+      gemm(b, b, b, ne, ONE, tv(0), OP_N, X.view(j), OP_N, tv(6), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+      // X_ij = -t2 - X_i P2^H
+      if (ou)
+        gemm(b, b, b, ne, MONE, X.view(i), OP_N, tv(1), OP_C, out_at(ou, nb - 1, i), s, tv(6), MONE, {}, ZERO,
+             nullptr, nullptr, prec);
+      // X_i += t2 P1^H + t1
+      gemm(b, b, b, ne, ONE, tv(6), OP_N, tv(0), OP_C, X.view(i), s, X.view(i), ONE, tv(5), ONE, nullptr, nullptr,
+           prec);
+      if (od) launch_block_scatter(b, b, ne, X.view(i), 1, out_at(od, nb, i).ptr, nb * bb, bb, nullptr, s);
+    }
+    if (O.density) launch_diag_imag_sum(b, ne, xl.view(i), 1.0, O.density + e0 * nb, nb, i, s);
+    if (O.hole_density) launch_diag_imag_sum(b, ne, xg.view(i), -1.0, O.hole_density + e0 * nb, nb, i, s);
+    gemm(b, b, b, ne, ONE, tv(3), OP_N, xr.view(i), OP_N, tv(4), s, xr.view(i), ONE, {}, ZERO, nullptr, nullptr,
+         prec);
+    std::swap(xr.ptr[i], T[4]);
+    if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(i), ZERO, {}, out_at(O.gr_diag, nb, i), s);
+  }
+  if (O.current_left) {
+    launch_block_scatter(b, b, ne, xl.view(0), 1, T[6], bb, bb, nullptr, s);
+    launch_block_scatter(b, b, ne, xg.view(0), 1, T[7], bb, bb, nullptr, s);
+    launch_trace_product(b, b, ne, V(C[6]), tv(6), ONE, cl, false, s);
+    launch_trace_product(b, b, ne, tv(7), V(C[4]), MONE, cl, true, s);
+    QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_left) + e0, cl, sizeof(cplx) * ne,
+                                 cudaMemcpyDeviceToDevice, s));
+  }
+  if (O.transmission) {
+    // T = Tr[Gamma_L G_0N Gamma_R G_0N^H]
+    gemm(b, b, b, ne, ONE, V(C[8]), OP_N, V(corner), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, tv(0), OP_N, V(C[9]), OP_N, tv(1), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    launch_trace_product_h(b, b, ne, tv(1), V(corner), tr, s);
+    launch_real_part(ne, tr, O.transmission + e0, s);
+  }
+
+}
+
 void transport_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qtx_transport_outputs& O, int prec,
                     cudaStream_t s, bool& all_converged) {
   const int nb = P.num_blocks, b = P.block_size;
   const int64_t NE = P.num_energies;
-  const int64_t bb = (int64_t)b * b;
-  const cplx* h_diag = reinterpret_cast<const cplx*>(P.h_diag);
-  const cplx* h_upper = reinterpret_cast<const cplx*>(P.h_upper);
   auto offs = batch_offsets(NE, P.max_batch_size > 0 ? P.max_batch_size : NE);
   int64_t ne_max = 0;
   for (size_t q = 0; q + 1 < offs.size(); ++q) ne_max = std::max(ne_max, offs[q + 1] - offs[q]);
   if (ne_max == 0) return;
-
-  // energy-independent couplings: A_i,i+1 = -H_i,i+1 ; A_i+1,i = -H_i,i+1^H
-  DevBuf cpl(sizeof(cplx) * 2 * bb * std::max(nb - 1, 1), s);
-  cplx* a_up = cpl.as<cplx>();
-  cplx* a_lo = a_up + bb * std::max(nb - 1, 1);
-  for (int i = 0; i + 1 < nb; ++i) {
-    launch_axpby(b, b, 1, MONE, MatView{h_upper + i * bb, b, bb}, ZERO, {}, MutView{a_up + i * bb, b, bb}, s);
-    launch_neg_herm(b, h_upper + i * bb, a_lo + i * bb, s);
-  }
-  auto up = [&](int i) { return MatView{a_up + i * bb, b, 0}; };
-  auto lo = [&](int i) { return MatView{a_lo + i * bb, b, 0}; };
-  auto hd = [&](int i) { return MatView{h_diag + i * bb, b, 0}; };
-
-  const size_t tmp = (size_t)bb * ne_max;
-  const int NT = 10;
-  const size_t total = 3 * (size_t)nb * tmp + NT * tmp + 10 * tmp;
-  DevBuf buf(sizeof(cplx) * total + sizeof(cplx) * 4 * ne_max + sizeof(double) * 2 * ne_max +
-                 sizeof(int) * (nb + 2) * ne_max,
-             s);
-  cplx* cur = buf.as<cplx>();
-  std::vector<int> sizes(nb, b);
-  BlockStack xr = carve(cur, sizes, ne_max, b), xl = carve(cur, sizes, ne_max, b), xg = carve(cur, sizes, ne_max, b);
-  cplx* T[NT];
-  for (int q = 0; q < NT; ++q) { T[q] = cur; cur += tmp; }
-  // contact buffers: g_L, g_R, SigR_L, SigR_R, SigL_L, SigL_R, SigG_L, SigG_R, Gam_L, Gam_R
-  cplx* C[10];
-  for (int q = 0; q < 10; ++q) { C[q] = cur; cur += tmp; }
-  cplx* shift = cur; cur += ne_max;
-  cplx* tr = cur; cur += ne_max;
-  cplx* cl = cur; cur += ne_max;
-  cplx* cr = cur; cur += ne_max;
-  double* occ_l = reinterpret_cast<double*>(cur);
-  double* occ_r = occ_l + ne_max;
-  int* info = reinterpret_cast<int*>(occ_r + ne_max);
-  int* its = info + nb * ne_max;
-  QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * nb * ne_max, s));
-
-  auto V = [&](cplx* p) { return MutView{p, b, bb}; };
+  DevBuf mem(transport_ws_bytes(nb, b, ne_max), s);
+  TransportWS w = carve_transport_ws(mem.as<void>(), nb, b, ne_max);
+  transport_couplings(w, reinterpret_cast<const cplx*>(P.h_upper), s);
+  QTX_CUDA_TRY(cudaMemsetAsync(w.info, 0, sizeof(int) * nb * ne_max, s));
   for (size_t q = 0; q + 1 < offs.size(); ++q) {
     const int64_t e0 = offs[q], ne = offs[q + 1] - offs[q];
-    const double* en = P.energies + e0;
-    launch_energy_shift(ne, en, P.eta, shift, s);
-    // ---- contacts (src/quatrex/electron/solver.py:305-386)
-    // left: A_00(E) into T0 ; g_L = SR(A_00, A_01, A_10)
-    launch_assemble_diag(b, ne, h_diag, en, P.eta, V(T[0]), s);
-    bool okl = sancho_rubio_impl(ctx, b, ne, V(T[0]), up(0), lo(0), P.sr_tol, P.sr_max_iterations, V(C[0]), its, s);
-    if (O.sr_iterations)
-      QTX_CUDA_TRY(cudaMemcpy2DAsync(O.sr_iterations + 2 * e0, 2 * sizeof(int), its, sizeof(int), sizeof(int), ne,
-                                     cudaMemcpyDeviceToDevice, s));
-    launch_assemble_diag(b, ne, h_diag + (int64_t)(nb - 1) * bb, en, P.eta, V(T[0]), s);
-    bool okr = sancho_rubio_impl(ctx, b, ne, V(T[0]), lo(nb - 2), up(nb - 2), P.sr_tol, P.sr_max_iterations,
-                                 V(C[1]), its, s);
-    if (O.sr_iterations)
-      QTX_CUDA_TRY(cudaMemcpy2DAsync(O.sr_iterations + 2 * e0 + 1, 2 * sizeof(int), its, sizeof(int), sizeof(int),
-                                     ne, cudaMemcpyDeviceToDevice, s));
-    all_converged = all_converged && okl && okr;
-    // Sigma^R_L = A_10 g_L A_01 ; Sigma^R_R = A_mn g_R A_nm
-    gemm(b, b, b, ne, ONE, lo(0), OP_N, V(C[0]), OP_N, V(T[1]), s);
-    gemm(b, b, b, ne, ONE, V(T[1]), OP_N, up(0), OP_N, V(C[2]), s);
-    gemm(b, b, b, ne, ONE, up(nb - 2), OP_N, V(C[1]), OP_N, V(T[1]), s);
-    gemm(b, b, b, ne, ONE, V(T[1]), OP_N, lo(nb - 2), OP_N, V(C[3]), s);
-    launch_fermi(ne, en, P.mu_left, P.kt, occ_l, s);
-    launch_fermi(ne, en, P.mu_right, P.kt, occ_r, s);
-    launch_obc_lesser_greater(b, ne, V(C[2]), occ_l, V(C[4]), V(C[6]), V(C[8]), s);
-    launch_obc_lesser_greater(b, ne, V(C[3]), occ_r, V(C[5]), V(C[7]), V(C[9]), s);
-    auto obc_r = [&](int i) { return i == 0 ? MatView(V(C[2])) : (i == nb - 1 ? MatView(V(C[3])) : MatView{}); };
-    auto obc_x = [&](int comp, int i) {
-      int base = comp == 0 ? 4 : 6;
-      return i == 0 ? MatView(V(C[base])) : (i == nb - 1 ? MatView(V(C[base + 1])) : MatView{});
-    };
-    auto tv = [&](int idx) { return V(T[idx]); };
-    auto out_at = [&](void* base, int64_t blocks_per_e, int blk) {
-      return MutView{reinterpret_cast<cplx*>(base) + (e0 * blocks_per_e + blk) * bb, b, blocks_per_e * bb};
-    };
+    all_converged = transport_contacts(ctx, w, P, O, e0, ne, s) && all_converged;
+    transport_sweep(w, P, O, e0, ne, prec, s);
+  }
+  read_info_or_throw(ctx, w.info, (int64_t)nb * ne_max, s, "transport_solve");
+  if (prec == QTX_PREC_MIXED) mixed_check_error(s);
+}
 
-    // ---- first block: x_0 = inv(A_00 - Sigma^R_L), X_0 = x_0 Sigma_0 x_0^H
-    // M_0 = (E + i eta) I - H_00 - Sigma^R_L
-    // (a K = 0 product: the epilogue alone forms -H_00 - Sigma^R_L + shift on the diagonal)
-    gemm(b, b, 0, ne, ONE, tv(0), OP_N, tv(0), OP_N, tv(1), s, hd(0), MONE, obc_r(0), MONE, nullptr, shift);
-    zinv(b, ne, tv(1), xr.view(0), info, nullptr, s);
-    for (int comp = 0; comp < 2; ++comp) {
-      BlockStack& X = comp == 0 ? xl : xg;
-      gemm(b, b, b, ne, ONE, xr.view(0), OP_N, obc_x(comp, 0), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
-           prec);
-      gemm(b, b, b, ne, ONE, tv(2), OP_N, xr.view(0), OP_C, X.view(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    }
-    // ---- forward sweep
-    for (int i = 0; i + 1 < nb; ++i) {
-      const int j = i + 1;
-      gemm(b, b, b, ne, ONE, lo(i), OP_N, xr.view(i), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      // M = (E + i eta) I - H_jj - Sigma^R_j - U A_ij
-      gemm(b, b, b, ne, MONE, tv(0), OP_N, up(i), OP_N, tv(1), s, hd(j), MONE, obc_r(j), MONE, nullptr, shift, prec);
-      zinv(b, ne, tv(1), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
-      for (int comp = 0; comp < 2; ++comp) {
-        BlockStack& X = comp == 0 ? xl : xg;
-        // V = X_i A_ji^H ; Q = A_ji V + Sigma_obc,j ; X_j = x_j Q x_j^H   (interior Sigma = 0)
-        gemm(b, b, b, ne, ONE, X.view(i), OP_N, lo(i), OP_C, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-        gemm(b, b, b, ne, ONE, lo(i), OP_N, tv(3), OP_N, tv(4), s, obc_x(comp, j), ONE, {}, ZERO, nullptr, nullptr,
-             prec);
-        gemm(b, b, b, ne, ONE, xr.view(j), OP_N, tv(4), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-        gemm(b, b, b, ne, ONE, tv(5), OP_N, xr.view(j), OP_C, X.view(j), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      }
-    }
-    // ---- last blocks, corner chain start
-    const int n = nb - 1;
-    if (O.gl_diag) launch_block_scatter(b, b, ne, xl.view(n), 1, out_at(O.gl_diag, nb, n).ptr, nb * bb, bb, nullptr, s);
-    if (O.gg_diag) launch_block_scatter(b, b, ne, xg.view(n), 1, out_at(O.gg_diag, nb, n).ptr, nb * bb, bb, nullptr, s);
-    if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, out_at(O.gr_diag, nb, n), s);
-    if (O.density) launch_diag_imag_sum(b, ne, xl.view(n), 1.0, O.density + e0 * nb, nb, n, s);
-    if (O.hole_density) launch_diag_imag_sum(b, ne, xg.view(n), -1.0, O.hole_density + e0 * nb, nb, n, s);
-    // contact current at the right contact uses the symmetrised G^<_nn, G^>_nn
-    if (O.current_right) {
-      launch_block_scatter(b, b, ne, xl.view(n), 1, T[6], bb, bb, nullptr, s);
-      launch_block_scatter(b, b, ne, xg.view(n), 1, T[7], bb, bb, nullptr, s);
-      launch_trace_product(b, b, ne, V(C[7]), tv(6), ONE, cr, false, s);
-      launch_trace_product(b, b, ne, tv(7), V(C[5]), MONE, cr, true, s);
-      QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_right) + e0, cr, sizeof(cplx) * ne,
-                                   cudaMemcpyDeviceToDevice, s));
-    }
-    cplx* corner = T[8];
-    cplx* corner2 = T[9];
-    if (O.transmission) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, V(corner), s);
-    // ---- backward sweep
-    for (int i = nb - 2; i >= 0; --i) {
-      const int j = i + 1;
-      gemm(b, b, b, ne, ONE, xr.view(i), OP_N, up(i), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      gemm(b, b, b, ne, ONE, xr.view(j), OP_N, lo(i), OP_N, tv(1), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      gemm(b, b, b, ne, ONE, tv(0), OP_N, xr.view(j), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      gemm(b, b, b, ne, ONE, tv(0), OP_N, tv(1), OP_N, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      if (O.gr_upper) launch_axpby(b, b, ne, MONE, tv(2), ZERO, {}, out_at(O.gr_upper, nb - 1, i), s);
-      if (O.gr_lower)
-        gemm(b, b, b, ne, MONE, tv(1), OP_N, xr.view(i), OP_N, out_at(O.gr_lower, nb - 1, i), s, {}, ZERO, {}, ZERO,
-             nullptr, nullptr, prec);
-      if (O.transmission) {
-        // G_{i,N-1} = -(x_i A_ij) G_{j,N-1}
-        gemm(b, b, b, ne, MONE, tv(0), OP_N, V(corner), OP_N, V(corner2), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
-             prec);
-        std::swap(corner, corner2);
-      }
-      for (int comp = 0; comp < 2; ++comp) {
-        BlockStack& X = comp == 0 ? xl : xg;
-        void* od = comp == 0 ? O.gl_diag : O.gg_diag;
-        void* ou = comp == 0 ? O.gl_upper : O.gg_upper;
-        // t1 = P4 X_i - (P4 X_i)^H ; t2 = P1 X_j
-        gemm(b, b, b, ne, ONE, tv(3), OP_N, X.view(i), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-        launch_sub_herm_inplace(b, ne, tv(5), s);
-        gemm(b, b, b, ne, ONE, tv(0), OP_N, X.view(j), OP_N, tv(6), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-        // X_ij = -t2 - X_i P2^H
-        if (ou)
-          gemm(b, b, b, ne, MONE, X.view(i), OP_N, tv(1), OP_C, out_at(ou, nb - 1, i), s, tv(6), MONE, {}, ZERO,
-               nullptr, nullptr, prec);
-        // X_i += t2 P1^H + t1
-        gemm(b, b, b, ne, ONE, tv(6), OP_N, tv(0), OP_C, X.view(i), s, X.view(i), ONE, tv(5), ONE, nullptr, nullptr,
-             prec);
-        if (od) launch_block_scatter(b, b, ne, X.view(i), 1, out_at(od, nb, i).ptr, nb * bb, bb, nullptr, s);
-      }
-      if (O.density) launch_diag_imag_sum(b, ne, xl.view(i), 1.0, O.density + e0 * nb, nb, i, s);
-      if (O.hole_density) launch_diag_imag_sum(b, ne, xg.view(i), -1.0, O.hole_density + e0 * nb, nb, i, s);
-      gemm(b, b, b, ne, ONE, tv(3), OP_N, xr.view(i), OP_N, tv(4), s, xr.view(i), ONE, {}, ZERO, nullptr, nullptr,
-           prec);
-      std::swap(xr.ptr[i], T[4]);
-      if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(i), ZERO, {}, out_at(O.gr_diag, nb, i), s);
-    }
-    if (O.current_left) {
-      launch_block_scatter(b, b, ne, xl.view(0), 1, T[6], bb, bb, nullptr, s);
-      launch_block_scatter(b, b, ne, xg.view(0), 1, T[7], bb, bb, nullptr, s);
-      launch_trace_product(b, b, ne, V(C[6]), tv(6), ONE, cl, false, s);
-      launch_trace_product(b, b, ne, tv(7), V(C[4]), MONE, cl, true, s);
-      QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_left) + e0, cl, sizeof(cplx) * ne,
-                                   cudaMemcpyDeviceToDevice, s));
-    }
-    if (O.transmission) {
-      // T = Tr[Gamma_L G_0N Gamma_R G_0N^H]
-      gemm(b, b, b, ne, ONE, V(C[8]), OP_N, V(corner), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      gemm(b, b, b, ne, ONE, tv(0), OP_N, V(C[9]), OP_N, tv(1), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      launch_trace_product_h(b, b, ne, tv(1), V(corner), tr, s);
-      launch_real_part(ne, tr, O.transmission + e0, s);
+// CUDA-graph form: the sweep of a single-batch call is captured once per
+// (shapes, buffers, precision) and replayed; the contacts run eagerly each call
+// (their convergence checks synchronise with the host).
+void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qtx_transport_outputs& O, int prec,
+                          cudaStream_t s, bool& all_converged) {
+  const int nb = P.num_blocks, b = P.block_size;
+  const int64_t ne = P.num_energies;
+  if (ne == 0) return;
+  GraphKey key;
+  key.v = {(uintptr_t)P.h_diag, (uintptr_t)P.h_upper, (uintptr_t)P.energies, (uintptr_t)nb, (uintptr_t)b,
+           (uintptr_t)ne, (uintptr_t)prec, (uintptr_t)O.gr_diag, (uintptr_t)O.gr_upper, (uintptr_t)O.gr_lower,
+           (uintptr_t)O.gl_diag, (uintptr_t)O.gl_upper, (uintptr_t)O.gg_diag, (uintptr_t)O.gg_upper,
+           (uintptr_t)O.density, (uintptr_t)O.hole_density, (uintptr_t)O.transmission, (uintptr_t)O.current_left,
+           (uintptr_t)O.current_right};
+  GraphEntry* g = ctx->graphs.find(key);
+  if (!g) {
+    g = ctx->graphs.insert(key);
+    g->bytes = transport_ws_bytes(nb, b, ne);
+    cudaError_t e = cudaMalloc(&g->mem, g->bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      ctx->graphs.erase(key);
+      throw QtxError(QTX_E_NOMEM, "transport graph: work space allocation failed");
     }
   }
-  read_info_or_throw(ctx, info, (int64_t)nb * ne_max, s, "transport_solve");
+  TransportWS w = carve_transport_ws(g->mem, nb, b, ne);
+  transport_couplings(w, reinterpret_cast<const cplx*>(P.h_upper), s);
+  QTX_CUDA_TRY(cudaMemsetAsync(w.info, 0, sizeof(int) * nb * ne, s));
+  all_converged = transport_contacts(ctx, w, P, O, 0, ne, s) && all_converged;
+  if (!g->exec) {
+    const int64_t before = ctx->launches;
+    ctx->capturing = true;
+    if (!ctx->capture_stream) QTX_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
+    cudaStream_t cs = ctx->capture_stream;
+    QTX_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    try {
+      transport_sweep(w, P, O, 0, ne, prec, cs);
+    } catch (...) {
+      cudaGraph_t dummy = nullptr;
+      cudaStreamEndCapture(cs, &dummy);
+      if (dummy) cudaGraphDestroy(dummy);
+      ctx->capturing = false;
+      throw;
+    }
+    cudaGraph_t graph = nullptr;
+    QTX_CUDA_TRY(cudaStreamEndCapture(cs, &graph));
+    ctx->capturing = false;
+    cudaError_t e = cudaGraphInstantiate(&g->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      g->exec = nullptr;
+      throw QtxError(QTX_E_CUDA, std::string("transport graph instantiation: ") + cudaGetErrorString(e));
+    }
+    g->launches = ctx->launches - before;
+    ctx->launches = before;
+  }
+  QTX_CUDA_TRY(cudaGraphLaunch(g->exec, s));
+  ctx->launches += g->launches;
+  ctx->graph_replays += 1;
+  read_info_or_throw(ctx, w.info, (int64_t)nb * ne, s, "transport_solve");
   if (prec == QTX_PREC_MIXED) mixed_check_error(s);
 }
 
@@ -906,6 +1100,9 @@ qtx_status qtx_ctx_create(int device, qtx_ctx** out) {
 qtx_status qtx_ctx_destroy(qtx_ctx* ctx) {
   if (!ctx) return QTX_E_INVAL;
   cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  ctx->graphs.clear();
+  if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
   cudaFree(ctx->d_scratch);
   cudaFreeHost(ctx->h_pinned);
   delete ctx;
@@ -925,11 +1122,14 @@ qtx_status qtx_ctx_trim(qtx_ctx* ctx) {
     cudaMemPool_t pool;
     QTX_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
     QTX_CUDA_TRY(cudaDeviceSynchronize());
+    ctx->graphs.clear();
     QTX_CUDA_TRY(cudaMemPoolTrimTo(pool, 0));
   });
 }
 
 int64_t qtx_launch_count(const qtx_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int64_t qtx_graph_replays(const qtx_ctx* ctx) { return ctx ? ctx->graph_replays : -1; }
 
 qtx_status qtx_ctx_set_timing(qtx_ctx* ctx, int enable) {
   if (!ctx) return QTX_E_INVAL;
@@ -1122,8 +1322,10 @@ qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, con
     if (p->num_blocks < 2 || p->block_size < 1 || p->num_energies < 0 || !p->h_diag || !p->h_upper ||
         !p->energies || p->kt <= 0 || p->sr_max_iterations < 1)
       throw QtxError(QTX_E_INVAL, "qtx_transport_solve: bad problem");
-    (void)flags;
-    transport_impl(ctx, *p, *o, precision, reinterpret_cast<cudaStream_t>(stream), ok);
+    const bool use_graph = (flags & QTX_FLAG_GRAPH) != 0 &&
+                           (p->max_batch_size <= 0 || p->max_batch_size >= p->num_energies);
+    if (use_graph) transport_graph_impl(ctx, *p, *o, precision, reinterpret_cast<cudaStream_t>(stream), ok);
+    else transport_impl(ctx, *p, *o, precision, reinterpret_cast<cudaStream_t>(stream), ok);
   });
   if (st == QTX_OK && !ok) {
     ctx->last_error = "Surface Green's function did not converge.";

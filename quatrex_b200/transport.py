@@ -30,7 +30,8 @@ class TransportSolver:
     """Device-resident transport solver for one ``TransportDevice``."""
 
     def __init__(self, device: TransportDevice, max_batch_size: int = 128, precision: str = "fp64",
-                 cuda_device: int | None = None, h_diag=None, h_upper=None):
+                 cuda_device: int | None = None, h_diag=None, h_upper=None, ctx: int | None = None,
+                 stream=None, use_graph: bool = False):
         if not torch.cuda.is_available():
             raise RuntimeError("quatrex_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
         self.dev = device
@@ -42,6 +43,25 @@ class TransportSolver:
         # H may be handed in already on the device (e.g. shared by several solvers)
         self.h_diag = h_diag if h_diag is not None else torch.from_numpy(device.h_diag).to(f"cuda:{self.cuda}")
         self.h_upper = h_upper if h_upper is not None else torch.from_numpy(device.h_upper).to(f"cuda:{self.cuda}")
+        self.ctx = ctx
+        self.stream = stream
+        # CUDA-graph replay needs the same buffers every call: a fixed energy buffer
+        self.use_graph = use_graph
+        self._e_buf = None
+
+    @staticmethod
+    def footprint_bytes(num_blocks: int, block_size: int, energies_per_call: int, keys=OUTPUT_KEYS) -> int:
+        """Device bytes one call holds: H and couplings, the work space of one
+        energy batch and the requested outputs (used for admission control)."""
+        nb, b, ne = int(num_blocks), int(block_size), int(energies_per_call)
+        bb = 16 * b * b
+        h = bb * (nb + 3 * max(nb - 1, 1))
+        ws = bb * ne * (3 * nb + 20) + 64 * ne + 4 * (nb + 2) * ne
+        sr = bb * ne * 9
+        blocks = {"gr_diag": nb, "gr_upper": nb - 1, "gr_lower": nb - 1, "gl_diag": nb, "gl_upper": nb - 1,
+                  "gg_diag": nb, "gg_upper": nb - 1}
+        out = sum(bb * ne * blocks[k] for k in keys if k in blocks) + 64 * ne * nb
+        return int(h + ws + sr + out)
 
     def allocate_outputs(self, num_energies: int, keys=OUTPUT_KEYS) -> dict:
         nb, b, ne = self.nb, self.b, int(num_energies)
@@ -70,17 +90,29 @@ class TransportSolver:
         e = energies if isinstance(energies, torch.Tensor) else torch.as_tensor(np.asarray(energies, dtype=np.float64))
         e = e.to(device=f"cuda:{self.cuda}", dtype=torch.float64).contiguous()
         ne = int(e.shape[0])
+        flags = 0
+        if self.use_graph and ne <= self.max_batch_size:
+            if self._e_buf is None or self._e_buf.shape[0] != ne:
+                self._e_buf = torch.empty(ne, dtype=torch.float64, device=f"cuda:{self.cuda}")
+            self._e_buf.copy_(e, non_blocking=True)
+            e = self._e_buf
+            flags |= _lib.QTX_FLAG_GRAPH
         if outputs is None:
             outputs = self.allocate_outputs(ne, keys)
         lib = _lib.load()
-        ctx = _lib.context(self.cuda)
+        ctx = self.ctx if self.ctx is not None else _lib.context(self.cuda)
         p = _lib.TransportProblem(
             num_blocks=self.nb, block_size=self.b, num_energies=ne, h_diag=self.h_diag.data_ptr(),
             h_upper=self.h_upper.data_ptr(), energies=e.data_ptr(), eta=self.dev.eta, mu_left=self.dev.mu_left,
             mu_right=self.dev.mu_right, kt=self.dev.kt, sr_tol=self.dev.sr_tol,
             sr_max_iterations=self.dev.sr_max_iter, max_batch_size=self.max_batch_size)
         o = _lib.TransportOutputs(**{k: (outputs[k].data_ptr() if k in outputs else None) for k in OUTPUT_KEYS})
-        s = stream if stream is not None else torch.cuda.current_stream(self.cuda).cuda_stream
-        st = lib.qtx_transport_solve(ctx, ctypes.byref(p), ctypes.byref(o), _PRECISIONS[self.precision], 0, s)
+        if stream is None:
+            stream = self.stream
+        if stream is None:
+            s = torch.cuda.current_stream(self.cuda).cuda_stream
+        else:
+            s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        st = lib.qtx_transport_solve(ctx, ctypes.byref(p), ctypes.byref(o), _PRECISIONS[self.precision], flags, s)
         _lib.check(st, ctx, "transport_solve")
         return outputs
