@@ -305,6 +305,32 @@ def run_ours(args):
     alg = _flops_per_energy(nb, b, [float(np.mean(sr_its[:, 0])), float(np.mean(sr_its[:, 1]))])
     whole_tflops = alg * args.steps * E / (elapsed_ms / 1000.0) / 1e12
 
+    if args.precision == "mixed":
+        roofline["kernel"] = ("complex GEMM class: ozaki_split + ozaki_gemm_kernel (INT8 tcgen05) in the sweep, "
+                              "zgemm_dmma_kernel in Sancho-Rubio; FP64-equivalent flops")
+
+    # ---- accuracy of the mixed form against the FP64 form (itself within 1e-10
+    # of the oracle) on the first energies of the first step
+    accuracy = None
+    if args.precision == "mixed" and rank == 0:
+        n_chk = min(32, E)
+        e_chk = step_e[0][:n_chk].contiguous()
+        keys = ("gr_diag", "gl_diag", "density", "transmission")
+        mix = TransportSolver(dev, max_batch_size=n_chk, precision="mixed", cuda_device=local).solve(e_chk, keys=keys)
+        ref = TransportSolver(dev, max_batch_size=n_chk, precision="fp64", cuda_device=local).solve(e_chk, keys=keys)
+
+        def block_rel(a, r):
+            return float((torch.linalg.norm(a - r, dim=(-2, -1)) / torch.linalg.norm(r, dim=(-2, -1))).max())
+
+        dens = (torch.abs(mix["density"] - ref["density"]) / torch.abs(ref["density"]).amax(dim=1, keepdim=True))
+        tr = torch.abs(mix["transmission"] - ref["transmission"]) / torch.clamp(torch.abs(ref["transmission"]),
+                                                                                   min=1e-12)
+        accuracy = {"against": "fp64 form, same energies", "energies": n_chk,
+                    "gr_diag_block_rel_max": block_rel(mix["gr_diag"], ref["gr_diag"]),
+                    "gl_diag_block_rel_max": block_rel(mix["gl_diag"], ref["gl_diag"]),
+                    "density_rel_max": float(dens.max()), "transmission_rel_max": float(tr.max())}
+        del mix, ref
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         bt = blas_threads()
@@ -328,9 +354,117 @@ def run_ours(args):
             "whole_step_tflops_fp64_equiv": round(whole_tflops, 3),
             "sr_iterations_mean": [float(np.mean(sr_its[:, 0])), float(np.mean(sr_its[:, 1]))],
         }
+        if accuracy is not None:
+            line["accuracy"] = accuracy
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+def run_uneven(args):
+    """Uneven batch: a seeded prefix of instances drawn with the uneven-batch size
+    distribution (b log-uniform over 32..512, nb uniform in [8, 128], 64-512
+    energies), solved with concurrent streams, both precisions."""
+    import torch
+
+    from quatrex_b200.autotune import Autotuner
+    from quatrex_b200.batching import BatchedTransport, Instance, total_flops, total_solves
+    from quatrex_b200.workloads import make_device, uneven_instances
+
+    draws = uneven_instances(args.instances, seed=4321)
+    insts = [Instance(make_device(**d), None) for d in draws]
+    for x in insts:
+        x.energies = x.device.energies
+    lines = []
+    if args.uneven_precision == "both":
+        # each precision in a fresh process: the device memory pools, graph
+        # memory and autotuner probes of one run do not weigh on the other
+        rc = 0
+        for prec in ("fp64", "mixed"):
+            cmd = [sys.executable, os.path.abspath(__file__), "--workload", "uneven", "--instances",
+                   str(args.instances), "--streams", str(args.streams), "--uneven-precision", prec]
+            rc = rc or subprocess.call(cmd)
+        return rc
+    for prec in (args.uneven_precision,):
+        tuner = Autotuner(cache_path=os.path.join(ROOT, "_build", "autotune.json"))
+        bt = BatchedTransport(precision=prec, streams=args.streams, tuner=tuner)
+        try:
+            # warm-up outside the timed region: tune every (b, batch, precision)
+            # key the instances use, then run the smallest instance once
+            for x in insts:
+                bt.choice_for(x)
+            bt.run([min(insts, key=lambda x: x.device.block_size * x.device.num_blocks)])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = bt.run(insts)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            per_instance = [{"b": x.device.block_size, "nb": x.device.num_blocks, "ne": len(x.energies),
+                             "seconds": round(r["seconds"], 3),
+                             "choice": {k: v for k, v in bt.choice_for(x).items() if k != "probe_solves_per_s"}}
+                            for x, r in zip(insts, res)]
+        finally:
+            bt.close()
+        lines.append({"metric": "rgf_energy_solves_per_s", "impl": "ours", "workload": "uneven",
+                      "precision": prec, "value": total_solves(insts) / dt, "unit": "solves/s",
+                      "seconds": dt, "instances": len(insts), "solves": total_solves(insts),
+                      "alg_tflops": total_flops(insts) / dt / 1e12, "streams": args.streams,
+                      "per_instance": per_instance})
+        print(json.dumps(lines[-1]), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """Serving: a seeded Poisson stream of requests (b in 32..256, nb 8..32,
+    16-64 energies each), continuous batching, both precisions; p50/p99."""
+    import torch
+
+    from quatrex_b200.autotune import Autotuner
+    from quatrex_b200.serving import TransportServer, poisson_arrivals
+    from quatrex_b200.workloads import make_device
+
+    rng = np.random.default_rng(99)
+    reqs = []
+    for k in range(args.requests):
+        b = int(2 ** rng.integers(5, 9))
+        nb = int(rng.integers(8, 33))
+        ne = int(rng.integers(16, 65))
+        reqs.append(make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=5000 + k))
+    arrivals = poisson_arrivals(len(reqs), rate_hz=args.rate, seed=7)
+    for prec in ("fp64", "mixed"):
+        tuner = Autotuner(cache_path=os.path.join(ROOT, "_build", "autotune.json"))
+        server = TransportServer(slots=args.streams, precision=prec, tuner=tuner)
+        try:
+            # warm-up outside the timed region: tune every (b, batch, precision)
+            # key the requests use, and run one request of each block size alone
+            for d in reqs:
+                tuner.best(d.block_size, len(d.energies), prec)
+            seen = set()
+            for d in reqs:
+                if d.block_size not in seen:
+                    seen.add(d.block_size)
+                    server.submit(d, d.energies[:8]).result()
+            server.latencies.clear()
+            server.completed = server.solves = 0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            futs = []
+            for d, t in zip(reqs, arrivals):
+                while time.perf_counter() - t0 < t:
+                    time.sleep(0.0002)
+                futs.append(server.submit(d, d.energies))
+            for f in futs:
+                f.result()
+            dt = time.perf_counter() - t0
+            st = server.stats()
+        finally:
+            server.close()
+        print(json.dumps({"metric": "rgf_energy_solves_per_s", "impl": "ours", "workload": "serve",
+                          "precision": prec, "value": st["solves"] / dt, "unit": "solves/s", "seconds": dt,
+                          "requests": st["completed"], "p50_latency_s": st["p50_s"], "p99_latency_s": st["p99_s"],
+                          "mean_latency_s": st["mean_s"], "peak_concurrency": st["peak_concurrency"],
+                          "arrival_rate_hz": args.rate, "slots": args.streams}), flush=True)
     return 0
 
 
@@ -340,7 +474,12 @@ def main():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["large", "small"], default="large")
+    ap.add_argument("--workload", choices=["large", "small", "uneven", "serve"], default="large")
+    ap.add_argument("--instances", type=int, default=8, help="uneven workload: number of instances")
+    ap.add_argument("--streams", type=int, default=4, help="uneven/serve: concurrent streams (slots)")
+    ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve workload: Poisson arrival rate (1/s)")
+    ap.add_argument("--uneven-precision", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--energies-per-step", type=int, default=128)
     ap.add_argument("--cpu-energies", type=int, default=3)
@@ -350,6 +489,10 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "uneven":
+        return run_uneven(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -227,6 +227,11 @@ qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, con
 
 /* Number of captured-sweep replays issued by this context (QTX_FLAG_GRAPH). */
 int64_t qtx_graph_replays(const qtx_ctx* ctx);
+/* Drop every captured sweep the context holds; their work spaces are freed in
+ * stream order on `stream` after their last use, without a device-wide
+ * synchronisation (safe while other threads capture or run).  No reference
+ * counterpart: the reference captures no graphs. */
+qtx_status qtx_ctx_release_graphs(qtx_ctx* ctx, qtx_stream stream);
 
 /* FP64 roofline probe -- no counterpart in the upstream code.  Measures the
  * issue-rate ceiling of the FP64 tensor path (kind 0: DMMA mma.sync m8n8k4)

@@ -109,6 +109,7 @@ SIGNATURES = {
     "qtx_ctx_trim": (c_int32, [c_void_p]),
     "qtx_launch_count": (c_int64, [c_void_p]),
     "qtx_graph_replays": (c_int64, [c_void_p]),
+    "qtx_ctx_release_graphs": (c_int32, [c_void_p, c_void_p]),
     "qtx_ctx_set_timing": (c_int32, [c_void_p, ctypes.c_int]),
     "qtx_ctx_timing_report": (
         c_int32, [c_void_p, c_int32, ctypes.POINTER(c_double), ctypes.POINTER(c_double), ctypes.POINTER(c_int64)]),

@@ -69,14 +69,20 @@ class Autotuner:
         s = TransportSolver(dev, max_batch_size=ne, precision=precision, use_graph=graph)
         keys = ("density", "transmission")
         out = s.allocate_outputs(ne, keys)
-        s.solve(energies, out)  # warm-up (and graph capture)
-        torch.cuda.synchronize()
-        best = float("inf")
-        for _ in range(self.repeats):
-            t0 = time.perf_counter()
-            s.solve(energies, out)
+        try:
+            s.solve(energies, out)  # warm-up (and graph capture)
             torch.cuda.synchronize()
-            best = min(best, time.perf_counter() - t0)
+            best = float("inf")
+            for _ in range(self.repeats):
+                t0 = time.perf_counter()
+                s.solve(energies, out)
+                torch.cuda.synchronize()
+                best = min(best, time.perf_counter() - t0)
+        finally:
+            if graph:
+                # the probe's captured sweep (and its work space) is of no further use
+                s.release_graphs()
+                torch.cuda.synchronize()
         return ne / best
 
     def tune(self, block_size: int, batch: int, precision: str) -> dict:

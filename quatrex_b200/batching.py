@@ -60,7 +60,9 @@ class Worker:
         t0 = time.perf_counter()
         ne_call = int(choice["energies_per_call"])
         path = choice.get("gemm_path", precision)
-        graph = bool(choice.get("graph", False))
+        # a captured sweep pays off only when it is replayed: use it when the
+        # instance has at least three full-size calls (same buffers each time)
+        graph = bool(choice.get("graph", False)) and len(energies) // max(ne_call, 1) >= 3
         energies = np.asarray(energies, dtype=np.float64)
         results = {k: [] for k in keys}
         with torch.cuda.stream(self.stream):
@@ -78,6 +80,9 @@ class Worker:
                 out = solver.solve(chunk, outs[n])
                 for k in keys:
                     results[k].append(out[k].cpu())
+            if graph:
+                # the captured sweeps reference this instance's buffers: drop them
+                solver.release_graphs()
             self.stream.synchronize()
         self.busy_s += time.perf_counter() - t0
         return {k: torch.cat(v).numpy() for k, v in results.items()}
@@ -93,9 +98,14 @@ class BatchedTransport:
     """Solve a list of uneven instances with ``streams`` concurrent workers."""
 
     def __init__(self, precision: str = "fp64", streams: int = 4, tuner: Autotuner | None = None,
-                 cuda_device: int | None = None, keys=OBSERVABLE_KEYS):
+                 cuda_device: int | None = None, keys=OBSERVABLE_KEYS, memory_budget: int | None = None):
         self.precision = precision
         self.cuda = torch.cuda.current_device() if cuda_device is None else cuda_device
+        if memory_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.cuda)
+            memory_budget = int(free * 0.6)
+        self.budget = int(memory_budget)
+        self._used = 0
         self.tuner = tuner if tuner is not None else Autotuner()
         self.keys = keys
         self.workers = [Worker(self.cuda) for _ in range(max(1, streams))]
@@ -118,7 +128,18 @@ class BatchedTransport:
             self._cv.notify()
 
     def choice_for(self, inst: Instance) -> dict:
-        return self.tuner.best(inst.device.block_size, len(inst.energies), self.precision)
+        """Tuned setting, with the energies per call capped so that one call of
+        this instance (its actual number of blocks) fits in the budget."""
+        c = dict(self.tuner.best(inst.device.block_size, len(inst.energies), self.precision))
+        ne = int(c["energies_per_call"])
+        while ne > 1 and self.footprint(inst, ne) > self.budget:
+            ne //= 2
+        c["energies_per_call"] = max(1, ne)
+        return c
+
+    def footprint(self, inst: Instance, ne_call: int) -> int:
+        return TransportSolver.footprint_bytes(inst.device.num_blocks, inst.device.block_size,
+                                               min(ne_call, len(inst.energies)), ("density", "transmission"))
 
     def run(self, instances: list[Instance]) -> list[dict]:
         """Results in input order; each dict also holds 'seconds' (wall time on its worker)."""
@@ -130,15 +151,24 @@ class BatchedTransport:
         results: list[dict | None] = [None] * len(instances)
 
         def job(i):
+            choice = self.choice_for(instances[i])
+            fp = self.footprint(instances[i], int(choice["energies_per_call"]))
+            with self._cv:
+                # admission by device-memory footprint next to the instances already running
+                while self._used + fp > self.budget and self._used > 0:
+                    self._cv.wait()
+                self._used += fp
             w = self._take()
             try:
                 t0 = time.perf_counter()
-                r = w.solve(instances[i].device, instances[i].energies, self.precision,
-                            self.choice_for(instances[i]), self.keys)
+                r = w.solve(instances[i].device, instances[i].energies, self.precision, choice, self.keys)
                 r["seconds"] = time.perf_counter() - t0
                 results[i] = r
             finally:
                 self._give(w)
+                with self._cv:
+                    self._used -= fp
+                    self._cv.notify_all()
 
         with ThreadPoolExecutor(max_workers=len(self.workers)) as ex:
             list(ex.map(job, order))

@@ -69,3 +69,31 @@ inline void qtx_check_launch(const char* what) {
 }
 
 inline unsigned ceil_div_u(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+// Stream-ordered allocation from the device's default pool.  The pool keeps
+// freed memory for reuse (release threshold unlimited); when a request does
+// not fit, the memory the pool holds unused is returned to the driver and the
+// request is tried once more (no device-wide synchronisation: only blocks
+// whose stream-ordered free has completed are released).  Returns nullptr on
+// failure, with the CUDA error cleared.
+inline void* qtx_malloc_async(size_t bytes, cudaStream_t s) {
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, bytes, s) == cudaSuccess) return p;
+  cudaGetLastError();
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  int dev = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess ||
+      cudaMemPoolTrimTo(pool, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  p = nullptr;
+  if (cudaMallocAsync(&p, bytes, s) == cudaSuccess) return p;
+  cudaGetLastError();
+  return nullptr;
+}

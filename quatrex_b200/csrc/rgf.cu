@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -34,14 +35,23 @@ struct GraphKey {
 
 struct GraphEntry {
   GraphKey key;
-  void* mem = nullptr;
+  void* mem = nullptr;  // work space, stream-ordered allocation
   size_t bytes = 0;
   cudaGraphExec_t exec = nullptr;
+  cudaEvent_t done = nullptr;  // recorded after every use of `mem`
   int64_t launches = 0;
   uint64_t last_use = 0;
 };
 
-// Small LRU cache of captured sweeps (each holds its work space).
+// Graph captures and the library's own device-wide synchronisation never
+// overlap: a device-wide synchronisation (or cudaFree) issued by one thread
+// while another thread's stream is capturing invalidates that capture.
+std::mutex g_capture_mutex;
+
+// Small LRU cache of captured sweeps (each holds its work space).  Nothing here
+// synchronises the device: an evicted entry's memory is freed in stream order
+// after its last use (its `done` event), and an executable graph still in
+// flight is released by the driver when it completes.
 struct GraphCache {
   std::vector<GraphEntry> entries;
   uint64_t clock = 0;
@@ -54,19 +64,23 @@ struct GraphCache {
       }
     return nullptr;
   }
-  static void release(GraphEntry& e) {
+  static void release(GraphEntry& e, cudaStream_t s) {
     if (e.exec) cudaGraphExecDestroy(e.exec);
-    if (e.mem) cudaFree(e.mem);
+    if (e.mem) {
+      if (e.done) cudaStreamWaitEvent(s, e.done, 0);
+      cudaFreeAsync(e.mem, s);
+    }
+    if (e.done) cudaEventDestroy(e.done);
     e.exec = nullptr;
     e.mem = nullptr;
+    e.done = nullptr;
   }
-  GraphEntry* insert(const GraphKey& k) {
+  GraphEntry* insert(const GraphKey& k, cudaStream_t s) {
     if (entries.size() >= capacity) {
       size_t victim = 0;
       for (size_t i = 1; i < entries.size(); ++i)
         if (entries[i].last_use < entries[victim].last_use) victim = i;
-      cudaDeviceSynchronize();
-      release(entries[victim]);
+      release(entries[victim], s);
       entries.erase(entries.begin() + victim);
     }
     entries.push_back(GraphEntry{});
@@ -74,19 +88,43 @@ struct GraphCache {
     entries.back().last_use = ++clock;
     return &entries.back();
   }
-  void erase(const GraphKey& k) {
+  void erase(const GraphKey& k, cudaStream_t s) {
     for (size_t i = 0; i < entries.size(); ++i)
       if (entries[i].key == k) {
-        release(entries[i]);
+        release(entries[i], s);
         entries.erase(entries.begin() + i);
         return;
       }
   }
-  void clear() {
-    for (auto& e : entries) release(e);
+  void clear(cudaStream_t s) {
+    for (auto& e : entries) release(e, s);
     entries.clear();
   }
 };
+
+// Pinned host words for small device-to-host reads (convergence counters).
+// Process-wide and never freed: cudaFreeHost may synchronise the device.
+std::mutex g_pinned_mutex;
+std::vector<int*> g_pinned_free;
+int* pinned_take() {
+  std::lock_guard<std::mutex> lk(g_pinned_mutex);
+  if (!g_pinned_free.empty()) {
+    int* p = g_pinned_free.back();
+    g_pinned_free.pop_back();
+    return p;
+  }
+  int* p = nullptr;
+  if (cudaMallocHost(&p, 4096) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+void pinned_give(int* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_pinned_mutex);
+  g_pinned_free.push_back(p);
+}
 
 struct qtx_ctx {
   int device = 0;
@@ -97,8 +135,7 @@ struct qtx_ctx {
   std::string last_error;
   int64_t launches = 0;
   size_t mem_limit = 0;
-  int* d_scratch = nullptr;    // small device scratch (flags, counters)
-  int* h_pinned = nullptr;     // pinned host mirror
+  int* h_pinned = nullptr;     // pinned host word (process-wide pool)
   bool timing = false;
   std::vector<TimedLaunch> timed;
   std::vector<cudaEvent_t> event_pool;
@@ -179,13 +216,8 @@ class DevBuf {
   DevBuf() = default;
   DevBuf(size_t bytes, cudaStream_t s) : stream_(s), bytes_(bytes) {
     if (bytes == 0) return;
-    cudaError_t e = cudaMallocAsync(&ptr_, bytes, s);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      ptr_ = nullptr;
-      throw QtxError(QTX_E_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed: " +
-                                      cudaGetErrorString(e));
-    }
+    ptr_ = qtx_malloc_async(bytes, s);
+    if (!ptr_) throw QtxError(QTX_E_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
   }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
@@ -991,22 +1023,32 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
            (uintptr_t)O.gl_diag, (uintptr_t)O.gl_upper, (uintptr_t)O.gg_diag, (uintptr_t)O.gg_upper,
            (uintptr_t)O.density, (uintptr_t)O.hole_density, (uintptr_t)O.transmission, (uintptr_t)O.current_left,
            (uintptr_t)O.current_right};
+  // scalars are baked into the captured launches: they are part of the key
+  for (double v : {P.eta, P.mu_left, P.mu_right, P.kt, P.sr_tol}) {
+    uint64_t bits;
+    memcpy(&bits, &v, sizeof bits);
+    key.v.push_back((uintptr_t)bits);
+  }
+  key.v.push_back((uintptr_t)P.sr_max_iterations);
+  key.v.push_back((uintptr_t)P.max_batch_size);
   GraphEntry* g = ctx->graphs.find(key);
   if (!g) {
-    g = ctx->graphs.insert(key);
+    g = ctx->graphs.insert(key, s);
     g->bytes = transport_ws_bytes(nb, b, ne);
-    cudaError_t e = cudaMalloc(&g->mem, g->bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      ctx->graphs.erase(key);
+    QTX_CUDA_TRY(cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming));
+    g->mem = qtx_malloc_async(g->bytes, s);
+    if (!g->mem) {
+      ctx->graphs.erase(key, s);
       throw QtxError(QTX_E_NOMEM, "transport graph: work space allocation failed");
     }
+    QTX_CUDA_TRY(cudaEventRecord(g->done, s));
   }
   TransportWS w = carve_transport_ws(g->mem, nb, b, ne);
   transport_couplings(w, reinterpret_cast<const cplx*>(P.h_upper), s);
   QTX_CUDA_TRY(cudaMemsetAsync(w.info, 0, sizeof(int) * nb * ne, s));
   all_converged = transport_contacts(ctx, w, P, O, 0, ne, s) && all_converged;
   if (!g->exec) {
+    std::lock_guard<std::mutex> capture_lock(g_capture_mutex);
     const int64_t before = ctx->launches;
     ctx->capturing = true;
     if (!ctx->capture_stream) QTX_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking));
@@ -1034,6 +1076,7 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
     ctx->launches = before;
   }
   QTX_CUDA_TRY(cudaGraphLaunch(g->exec, s));
+  QTX_CUDA_TRY(cudaEventRecord(g->done, s));
   ctx->launches += g->launches;
   ctx->graph_replays += 1;
   read_info_or_throw(ctx, w.info, (int64_t)nb * ne, s, "transport_solve");
@@ -1088,8 +1131,8 @@ qtx_status qtx_ctx_create(int device, qtx_ctx** out) {
     uint64_t thr = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
-  if (cudaMalloc(&c->d_scratch, 4096) != cudaSuccess || cudaMallocHost(&c->h_pinned, 4096) != cudaSuccess) {
-    cudaGetLastError();
+  c->h_pinned = pinned_take();
+  if (!c->h_pinned) {
     delete c;
     return QTX_E_NOMEM;
   }
@@ -1100,11 +1143,22 @@ qtx_status qtx_ctx_create(int device, qtx_ctx** out) {
 qtx_status qtx_ctx_destroy(qtx_ctx* ctx) {
   if (!ctx) return QTX_E_INVAL;
   cudaSetDevice(ctx->device);
-  cudaDeviceSynchronize();
-  ctx->graphs.clear();
+  // Work already enqueued by this context keeps running; the graph work spaces
+  // are freed in stream order after their last use, without a device-wide
+  // synchronisation (other threads may be capturing graphs meanwhile).
+  cudaStream_t rs = nullptr;
+  if (cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    rs = ctx->capture_stream;
+  }
+  ctx->graphs.clear(rs);
+  if (rs) {
+    cudaStreamSynchronize(rs);
+    if (rs != ctx->capture_stream) cudaStreamDestroy(rs);
+  }
   if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
-  cudaFree(ctx->d_scratch);
-  cudaFreeHost(ctx->h_pinned);
+  for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+  pinned_give(ctx->h_pinned);
   delete ctx;
   return QTX_OK;
 }
@@ -1121,8 +1175,10 @@ qtx_status qtx_ctx_trim(qtx_ctx* ctx) {
   return guarded(ctx, [&] {
     cudaMemPool_t pool;
     QTX_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+    std::lock_guard<std::mutex> capture_lock(g_capture_mutex);
     QTX_CUDA_TRY(cudaDeviceSynchronize());
-    ctx->graphs.clear();
+    ctx->graphs.clear(nullptr);
+    QTX_CUDA_TRY(cudaDeviceSynchronize());
     QTX_CUDA_TRY(cudaMemPoolTrimTo(pool, 0));
   });
 }
@@ -1130,6 +1186,10 @@ qtx_status qtx_ctx_trim(qtx_ctx* ctx) {
 int64_t qtx_launch_count(const qtx_ctx* ctx) { return ctx ? ctx->launches : -1; }
 
 int64_t qtx_graph_replays(const qtx_ctx* ctx) { return ctx ? ctx->graph_replays : -1; }
+
+qtx_status qtx_ctx_release_graphs(qtx_ctx* ctx, qtx_stream stream) {
+  return guarded(ctx, [&] { ctx->graphs.clear(static_cast<cudaStream_t>(stream)); });
+}
 
 qtx_status qtx_ctx_set_timing(qtx_ctx* ctx, int enable) {
   if (!ctx) return QTX_E_INVAL;

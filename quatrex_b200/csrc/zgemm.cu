@@ -211,11 +211,12 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_dmma_kernel(Params p) {
 
 template <int OPA, int OPB>
 void launch_t(const Params& p, cudaStream_t stream) {
-  static bool configured = false;
-  if (!configured) {
+  // thread-safe one-time opt-in to the large shared-memory carve-out
+  static const bool configured = [] {
     cudaFuncSetAttribute(zgemm_dmma_kernel<OPA, OPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    configured = true;
-  }
+    return true;
+  }();
+  (void)configured;
   dim3 grid(ceil_div_u(p.n, BN), ceil_div_u(p.m, BM), (unsigned)(p.batch < 65535 ? p.batch : 65535));
   zgemm_dmma_kernel<OPA, OPB><<<grid, THREADS, SMEM_BYTES, stream>>>(p);
 }

@@ -29,6 +29,8 @@
 #include <algorithm>
 #include <cstdlib>
 
+#include <mutex>
+
 #include "kernels.h"
 
 namespace {
@@ -36,6 +38,9 @@ namespace {
 constexpr int TM = 128, TN = 32, KC = 32;
 constexpr int MAX_S = 7;
 constexpr int THREADS = 160;  // warps 0-3 drain, warp 4 loads and issues MMAs
+constexpr int MAX_STAGES = 4;
+constexpr int MAX_SMEM = 227 * 1024;  // dynamic shared memory a CTA may opt into
+constexpr int BAR_BYTES = 256;        // barrier words behind the stages
 constexpr uint32_t TMEM_COLS = 512;
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // give up a wait after 2 s
 
@@ -57,164 +62,272 @@ __device__ __forceinline__ int core_off(int row, int k) {
 }
 
 // ---------------------------------------------------------------------------
-// split kernels
+// split kernel
 // ---------------------------------------------------------------------------
-// Exponents: for every row m of op(A) (or column n of op(B)) the power of two
-// bounding max_k max(|Re|, |Im|).  `along_k` says whether consecutive k are
-// adjacent in memory (then a warp reduces one row) or consecutive rows are
-// (then a thread walks one row).  Element (i, k) is at base[i * si + k * sk].
-__global__ void ozaki_exponent_kernel(int R, int K, int64_t batch, const cplx* base, int64_t si, int64_t sk,
-                                      int64_t sb, int along_k, int* expo) {
-  const int lane = threadIdx.x & 31;
-  if (along_k) {
-    const int wpb = blockDim.x >> 5;
-    for (int64_t g = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); g < batch * R; g += (int64_t)gridDim.x * wpb) {
-      const int64_t e = g / R;
-      const int i = (int)(g % R);
-      const cplx* row = base + e * sb + (int64_t)i * si;
-      double mx = 0;
-      for (int k = lane; k < K; k += 32) {
-        cplx v = row[(int64_t)k * sk];
-        mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
-      }
+// Two kernels split an operand into slices, one per memory layout.  Both cover
+// a group of consecutive rows of one batch entry (rows of op(A), or columns of
+// op(B)) and all of K, in chunks of KC k; the element (i, k) is
+// base[i * si + k * sk], conjugated when `conj`.  Pass 1 reduces each row's
+// exponent E (max < 2^E * 127/128, so that the first rounded slice stays in
+// [-127, 127]); pass 2 re-reads the rows (L2-resident by then), writes the
+// chunk's slices into shared memory in the UMMA image and copies the chunk out
+// with 16-byte stores.  NPARTS = 2: the A operand (Ar, Ai); NPARTS = 4: the B
+// operand (two concatenations, see b_block_bytes).
+//
+// Slice s is the nearest integer of 128 x (remainder of slice s - 1), taken
+// with the 1.5 * 2^52 shift on the FP64 adder (exact for |v| < 2^51; the
+// integer is the low word): |q_1| <= 127, |q_s| <= 64 after.
+constexpr double SPLIT_RND = 6755399441055744.0;
+
+// E of a row from its max |Re|, |Im|: 2^(E-1) <= max, max < 2^E * 127/128.
+__device__ __forceinline__ int split_exponent(double mx) {
+  int E = 0;
+  if (mx > 0) {
+    const double mant = frexp(mx, &E);
+    if (mant >= 127.0 / 128.0) ++E;
+  }
+  return E;
+}
+
+// Rows adjacent in memory: a block takes 32 rows; warp w of a chunk takes rows
+// 8 (w / 2) .. + 7 and k 16 (w % 2) .. + 15, lane l row l % 8 of those and the 4
+// consecutive k from 4 (l / 8), so every load of a warp reads 4 runs of 8
+// consecutive rows; the 4 slice bytes of a thread are packed into one 32-bit
+// word per slice and part and stored conflict-free (32 rows = 1 KiB per slice
+// and part).
+constexpr int SPLIT_ROWS = 32;
+
+template <int S, int NPARTS>
+__global__ void __launch_bounds__(256) ozaki_split_rows_kernel(int R, int K, int64_t batch, const cplx* base, int64_t si,
+                                                          int64_t sk, int64_t sb, int conj, int KT, int TR, int* expo,
+                                                          signed char* out) {
+  constexpr int NSEG = NPARTS * S;  // 1 KiB segments per chunk: A 2S, B 4S
+  __shared__ __align__(16) uint32_t stage[NSEG * 256];
+  __shared__ double wmax[8][8];
+  __shared__ double rscale[SPLIT_ROWS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int Rt = (R + TR - 1) / TR;
+  const int64_t rblocks = (int64_t)Rt * (TR / SPLIT_ROWS);
+  const int blk_bytes = (NPARTS == 2 ? 2 * S * TR * KC : 2 * S * 2 * TR * KC);
+  const int rr = (warp >> 1) * 8 + (lane & 7);         // row within the block
+  const int k0 = (warp & 1) * 16 + (lane >> 3) * 4;    // first of 4 k within the chunk
+  const int woff = core_off(rr, k0) >> 2;              // word offset within a 1 KiB segment
+  for (int64_t blk = blockIdx.x; blk < batch * rblocks; blk += gridDim.x) {
+    const int64_t e = blk / rblocks;
+    const int r0 = (int)(blk % rblocks) * SPLIT_ROWS;
+    const int i = r0 + rr;
+    const cplx* row = base + e * sb + (int64_t)i * si;
+    // pass 1: row maxima
+    double m = 0.0;
+    if (i < R) {
+      for (int kc = 0; kc < KT; ++kc) {
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      int E = 0;
-      if (mx > 0) frexp(mx, &E);
-      if (lane == 0) expo[g] = E;
-    }
-  } else {
-    // 32 consecutive rows per block (coalesced), 8 threads share the K range
-    __shared__ double part[8][33];
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int64_t ngroups = batch * ((R + 31) / 32);
-    for (int64_t gb = blockIdx.x; gb < ngroups; gb += gridDim.x) {
-      const int64_t e = gb / ((R + 31) / 32);
-      const int i = (int)(gb % ((R + 31) / 32)) * 32 + tx;
-      double mx = 0;
-      if (i < R) {
-        const cplx* row = base + e * sb + (int64_t)i * si;
-        for (int k = ty; k < K; k += 8) {
-          cplx v = row[(int64_t)k * sk];
-          mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+        for (int jj = 0; jj < 4; ++jj) {
+          const int k = kc * KC + k0 + jj;
+          if (k < K) {
+            const cplx v = row[(int64_t)k * sk];
+            m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+          }
         }
       }
-      part[ty][tx] = mx;
+    }
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 8));
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 16));
+    if (lane < 8) wmax[warp][lane] = m;
+    __syncthreads();
+    if (tid < SPLIT_ROWS) {
+      const int rh = tid >> 3, rl = tid & 7;
+      const double mx = fmax(wmax[2 * rh][rl], wmax[2 * rh + 1][rl]);
+      const int E = split_exponent(mx);
+      if (r0 + tid < R) expo[e * R + r0 + tid] = E;
+      rscale[tid] = ldexp(1.0, -E);
+    }
+    __syncthreads();
+    const double scale = rscale[rr];
+    // pass 2: slices, chunk by chunk
+    const int it = r0 / TR, rin = r0 % TR;
+    for (int kc = 0; kc < KT; ++kc) {
+      uint32_t wr[S], wi[S], wn[S];
+#pragma unroll
+      for (int sl = 0; sl < S; ++sl) wr[sl] = wi[sl] = wn[sl] = 0;
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int k = kc * KC + k0 + jj;
+        const cplx v = (i < R && k < K) ? row[(int64_t)k * sk] : cmk(0, 0);
+        double re = v.x * scale;
+        double im = (conj ? -v.y : v.y) * scale;
+#pragma unroll
+        for (int sl = 0; sl < S; ++sl) {
+          const double vr = re * 128.0, vi = im * 128.0;
+          const double yr = vr + SPLIT_RND, yi = vi + SPLIT_RND;
+          re = vr - (yr - SPLIT_RND);
+          im = vi - (yi - SPLIT_RND);
+          const int qr = __double2loint(yr), qi = __double2loint(yi);
+          wr[sl] |= (uint32_t)(qr & 0xFF) << (8 * jj);
+          wi[sl] |= (uint32_t)(qi & 0xFF) << (8 * jj);
+          if (NPARTS == 4) wn[sl] |= (uint32_t)((-qi) & 0xFF) << (8 * jj);
+        }
+      }
+#pragma unroll
+      for (int sl = 0; sl < S; ++sl) {
+        if (NPARTS == 2) {
+          // A: Ar slices, then Ai slices
+          stage[(0 * S + sl) * 256 + woff] = wr[sl];
+          stage[(1 * S + sl) * 256 + woff] = wi[sl];
+        } else {
+          // B: cat 0 = [Br | Bi], cat 1 = [-Bi | Br]; segment 2 (c S + sl) + half
+          stage[((0 * S + sl) * 2 + 0) * 256 + woff] = wr[sl];
+          stage[((0 * S + sl) * 2 + 1) * 256 + woff] = wi[sl];
+          stage[((1 * S + sl) * 2 + 0) * 256 + woff] = wn[sl];
+          stage[((1 * S + sl) * 2 + 1) * 256 + woff] = wr[sl];
+        }
+      }
       __syncthreads();
-      if (ty == 0) {
-        for (int q = 1; q < 8; ++q) mx = fmax(mx, part[q][tx]);
-        int E = 0;
-        if (mx > 0) frexp(mx, &E);
-        if (i < R) expo[e * R + i] = E;
+      signed char* g = out + ((e * Rt + it) * (int64_t)KT + kc) * blk_bytes + (rin >> 3) * 256;
+      for (int q = tid; q < NSEG * 64; q += 256) {
+        const int seg = q >> 6, w16 = q & 63;
+        const int64_t goff = (NPARTS == 2) ? (int64_t)seg * TR * KC
+                                           : (int64_t)(seg >> 1) * 2 * TR * KC + (seg & 1) * (TR / 8) * 256;
+        *reinterpret_cast<int4*>(g + goff + w16 * 16) = *reinterpret_cast<const int4*>(stage + seg * 256 + w16 * 4);
       }
       __syncthreads();
     }
   }
 }
 
-// Slices of 16 consecutive k of one row i of the operand (rows of op(A), or
-// columns of op(B)): one thread, one 16-byte store per slice and part.  The
-// element (i, k) is base[i * si + k * sk], conjugated when `conj`.  Threads are
-// ordered with i fastest when `i_fast` (rows adjacent in memory) and with the
-// k-group fastest otherwise, so the reads of a warp are coalesced either way.
-// NPARTS = 2: the A operand (Ar, Ai); NPARTS = 4: the B operand (two
-// concatenations, see b_block_bytes).
-// The 16 scaled remainders stay in registers and the slices are produced one
-// at a time (S compile-time).
+// k adjacent in memory: a block takes 16 rows; element q of a chunk (thread q
+// and q + 256) is row q / 32, k q % 32, so every load of a warp reads 32
+// consecutive k of one row; the slice bytes go to shared memory one by one.
+constexpr int SPLIT_KROWS = 16;
+
 template <int S, int NPARTS>
-__global__ void __launch_bounds__(256) ozaki_slice_kernel(int R, int K, int64_t batch, const cplx* base, int64_t si,
-                                                          int64_t sk, int64_t sb, int conj, int i_fast, int KT,
-                                                          int TR, const int* expo, signed char* out) {
+__global__ void __launch_bounds__(256) ozaki_split_k_kernel(int R, int K, int64_t batch, const cplx* base, int64_t si,
+                                                            int64_t sk, int64_t sb, int conj, int KT, int TR,
+                                                            int* expo, signed char* out) {
+  constexpr int NSEG = NPARTS * S;  // 512-byte segments per chunk (16 rows)
+  __shared__ __align__(16) signed char stage[NSEG * 512];
+  __shared__ double rscale[SPLIT_KROWS];
+  __shared__ double wmax[SPLIT_KROWS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int Rt = (R + TR - 1) / TR;
-  const int groups = KT * (KC / 16);
-  const int64_t rows = (int64_t)Rt * TR;
-  const int64_t total = batch * rows * groups;
+  const int64_t rblocks = (int64_t)Rt * (TR / SPLIT_KROWS);
   const int blk_bytes = (NPARTS == 2 ? 2 * S * TR * KC : 2 * S * 2 * TR * KC);
-  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = g / (rows * groups);
-    const int64_t rem = g % (rows * groups);
-    int i, grp;
-    if (i_fast) {
-      grp = (int)(rem / rows);
-      i = (int)(rem % rows);
-    } else {
-      i = (int)(rem / groups);
-      grp = (int)(rem % groups);
-    }
-    const int k0 = grp * 16;
-    const int E = (i < R) ? expo[e * R + i] : 0;
-    const double scale = ldexp(1.0, -E);
-    const cplx* row = base + e * sb + (int64_t)i * si;
-    double re[16], im[16];
-#pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-      const int k = k0 + kk;
-      cplx v = (i < R && k < K) ? row[(int64_t)k * sk] : cmk(0, 0);
-      re[kk] = v.x * scale;
-      im[kk] = (conj ? -v.y : v.y) * scale;
-    }
-    const int it = i / TR, r = i % TR;
-    const int kc = k0 / KC, kk0 = k0 % KC;
-    signed char* blk = out + ((e * Rt + it) * (int64_t)KT + kc) * blk_bytes + core_off(r, kk0);
-#pragma unroll
-    for (int sl = 0; sl < S; ++sl) {
-      uint32_t wr[4] = {0, 0, 0, 0}, wi[4] = {0, 0, 0, 0}, wn[4] = {0, 0, 0, 0};
-#pragma unroll
-      for (int kk = 0; kk < 16; ++kk) {
-        const double vr = re[kk] * 128.0, vi = im[kk] * 128.0;
-        const double tr = trunc(vr), ti = trunc(vi);
-        re[kk] = vr - tr;
-        im[kk] = vi - ti;
-        const int qr = (int)tr, qi = (int)ti;
-        const int sh = (kk & 3) * 8;
-        wr[kk >> 2] |= (uint32_t)(qr & 0xFF) << sh;
-        wi[kk >> 2] |= (uint32_t)(qi & 0xFF) << sh;
-        wn[kk >> 2] |= (uint32_t)((-qi) & 0xFF) << sh;
+  // a warp holds rows warp and warp + 8, one k per lane
+  const int rr0 = warp, rr1 = warp + 8, kk = lane;
+  for (int64_t blk = blockIdx.x; blk < batch * rblocks; blk += gridDim.x) {
+    const int64_t e = blk / rblocks;
+    const int r0 = (int)(blk % rblocks) * SPLIT_KROWS;
+    const cplx* mat = base + e * sb;
+    double m0 = 0.0, m1 = 0.0;
+    for (int kc = 0; kc < KT; ++kc) {
+      const int k = kc * KC + kk;
+      if (k < K) {
+        if (r0 + rr0 < R) {
+          const cplx v = mat[(int64_t)(r0 + rr0) * si + (int64_t)k * sk];
+          m0 = fmax(m0, fmax(fabs(v.x), fabs(v.y)));
+        }
+        if (r0 + rr1 < R) {
+          const cplx v = mat[(int64_t)(r0 + rr1) * si + (int64_t)k * sk];
+          m1 = fmax(m1, fmax(fabs(v.x), fabs(v.y)));
+        }
       }
-      if (NPARTS == 2) {
-        // A: Ar slices, then Ai slices
-        *reinterpret_cast<int4*>(blk + (0 * S + sl) * TR * KC) = make_int4(wr[0], wr[1], wr[2], wr[3]);
-        *reinterpret_cast<int4*>(blk + (1 * S + sl) * TR * KC) = make_int4(wi[0], wi[1], wi[2], wi[3]);
-      } else {
-        // B: cat 0 = [Br | Bi], cat 1 = [-Bi | Br]; each slice is 2 TR rows
-        const int slice_bytes = 2 * TR * KC;
-        const int half = (TR / 8) * 256;  // byte offset of row TR in the core-matrix layout
-        *reinterpret_cast<int4*>(blk + (0 * S + sl) * slice_bytes) = make_int4(wr[0], wr[1], wr[2], wr[3]);
-        *reinterpret_cast<int4*>(blk + (0 * S + sl) * slice_bytes + half) = make_int4(wi[0], wi[1], wi[2], wi[3]);
-        *reinterpret_cast<int4*>(blk + (1 * S + sl) * slice_bytes) = make_int4(wn[0], wn[1], wn[2], wn[3]);
-        *reinterpret_cast<int4*>(blk + (1 * S + sl) * slice_bytes + half) = make_int4(wr[0], wr[1], wr[2], wr[3]);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, off));
+      m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, off));
+    }
+    if (lane == 0) {
+      wmax[rr0] = m0;
+      wmax[rr1] = m1;
+    }
+    __syncthreads();
+    if (tid < SPLIT_KROWS) {
+      const int E = split_exponent(wmax[tid]);
+      if (r0 + tid < R) expo[e * R + r0 + tid] = E;
+      rscale[tid] = ldexp(1.0, -E);
+    }
+    __syncthreads();
+    const int it = r0 / TR, rin = r0 % TR;
+    for (int kc = 0; kc < KT; ++kc) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int rr = j ? rr1 : rr0;
+        const int i = r0 + rr, k = kc * KC + kk;
+        const cplx v = (i < R && k < K) ? mat[(int64_t)i * si + (int64_t)k * sk] : cmk(0, 0);
+        double re = v.x * rscale[rr];
+        double im = (conj ? -v.y : v.y) * rscale[rr];
+        const int off = core_off(rr, kk);
+#pragma unroll
+        for (int sl = 0; sl < S; ++sl) {
+          const double vr = re * 128.0, vi = im * 128.0;
+          const double yr = vr + SPLIT_RND, yi = vi + SPLIT_RND;
+          re = vr - (yr - SPLIT_RND);
+          im = vi - (yi - SPLIT_RND);
+          const int qr = __double2loint(yr), qi = __double2loint(yi);
+          if (NPARTS == 2) {
+            stage[(0 * S + sl) * 512 + off] = (signed char)qr;
+            stage[(1 * S + sl) * 512 + off] = (signed char)qi;
+          } else {
+            stage[((0 * S + sl) * 2 + 0) * 512 + off] = (signed char)qr;
+            stage[((0 * S + sl) * 2 + 1) * 512 + off] = (signed char)qi;
+            stage[((1 * S + sl) * 2 + 0) * 512 + off] = (signed char)(-qi);
+            stage[((1 * S + sl) * 2 + 1) * 512 + off] = (signed char)qr;
+          }
+        }
       }
+      __syncthreads();
+      signed char* g = out + ((e * Rt + it) * (int64_t)KT + kc) * blk_bytes + (rin >> 3) * 256;
+      for (int q = tid; q < NSEG * 32; q += 256) {
+        const int seg = q >> 5, w16 = q & 31;
+        const int64_t goff = (NPARTS == 2) ? (int64_t)seg * TR * KC
+                                           : (int64_t)(seg >> 1) * 2 * TR * KC + (seg & 1) * (TR / 8) * 256;
+        *reinterpret_cast<int4*>(g + goff + w16 * 16) = *reinterpret_cast<const int4*>(stage + seg * 512 + w16 * 16);
+      }
+      __syncthreads();
     }
   }
 }
 
 template <int NPARTS>
-void launch_slices(int S, unsigned grid, cudaStream_t stream, int R, int K, int64_t batch, const cplx* base,
-                   int64_t si, int64_t sk, int64_t sb, int conj, int i_fast, int KT, int TR, const int* expo,
-                   signed char* out) {
-#define QTX_SLICE_CASE(SS)                                                                                       \
-  case SS:                                                                                                      \
-    ozaki_slice_kernel<SS, NPARTS><<<grid, 256, 0, stream>>>(R, K, batch, base, si, sk, sb, conj, i_fast, KT, TR, \
-                                                             expo, out);                                        \
+void launch_split(int S, cudaStream_t stream, int R, int K, int64_t batch, const cplx* base, int64_t si, int64_t sk,
+                  int64_t sb, int conj, bool rows_adjacent, int KT, int TR, int* expo, signed char* out) {
+  const int rows = rows_adjacent ? SPLIT_ROWS : SPLIT_KROWS;
+  const int64_t rblocks = (int64_t)((R + TR - 1) / TR) * (TR / rows);
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(batch * rblocks, 148 * 16));
+#define QTX_SPLIT_CASE(SS)                                                                                      \
+  case SS:                                                                                                     \
+    if (rows_adjacent)                                                                                         \
+      ozaki_split_rows_kernel<SS, NPARTS><<<grid, 256, 0, stream>>>(R, K, batch, base, si, sk, sb, conj, KT, TR, \
+                                                                    expo, out);                                \
+    else                                                                                                       \
+      ozaki_split_k_kernel<SS, NPARTS><<<grid, 256, 0, stream>>>(R, K, batch, base, si, sk, sb, conj, KT, TR,    \
+                                                                 expo, out);                                   \
     break;
   switch (S) {
-    QTX_SLICE_CASE(2)
-    QTX_SLICE_CASE(3)
-    QTX_SLICE_CASE(4)
-    QTX_SLICE_CASE(5)
-    QTX_SLICE_CASE(6)
-    QTX_SLICE_CASE(7)
+    QTX_SPLIT_CASE(2)
+    QTX_SPLIT_CASE(3)
+    QTX_SPLIT_CASE(4)
+    QTX_SPLIT_CASE(5)
+    QTX_SPLIT_CASE(6)
+    QTX_SPLIT_CASE(7)
     default:
       throw QtxError(QTX_E_INVAL, "mixed-precision GEMM: slice count outside 2..7");
   }
-#undef QTX_SLICE_CASE
-  qtx_check_launch("ozaki_slice_kernel");
+#undef QTX_SPLIT_CASE
+  qtx_check_launch("ozaki_split_kernel");
 }
 
 // ---------------------------------------------------------------------------
 // tcgen05 helpers
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Exact int32 -> double on the FP64 adder: the bit pattern 0x43300000:(v + 2^31)
+// is 2^52 + 2^31 + v.
+__device__ __forceinline__ double i32_to_f64(int v) {
+  return __hiloint2double(0x43300000, v ^ (int)0x80000000) - 4503601774854144.0;
+}
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
@@ -313,6 +426,7 @@ struct OzParams {
   const cplx* diag_shift;
   int* error_flag;
   int a_shared, b_shared;  // operand sliced once for every batch entry
+  int nst;                 // pipeline stages (2..MAX_STAGES), as many as fit in shared memory
 };
 
 // Persistent: one CTA per SM loops over output tiles (n-tile fastest, so
@@ -327,9 +441,10 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm_kernel(OzParams p) {
   const int abytes = a_block_bytes(S), bbytes = b_block_bytes(S);
   const int stage_bytes = ((abytes + bbytes + 1023) / 1024) * 1024;
   unsigned char* stage0 = smem_raw;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + 2 * stage_bytes);
-  uint64_t* empty = full + 2;
-  uint64_t* tmem_full = empty + 2;
+  const int NST = p.nst;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NST * stage_bytes);
+  uint64_t* empty = full + MAX_STAGES;
+  uint64_t* tmem_full = empty + MAX_STAGES;
   uint64_t* tmem_empty = tmem_full + 1;
   uint64_t* all_done = tmem_empty + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(all_done + 1);
@@ -340,10 +455,10 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm_kernel(OzParams p) {
   const int64_t ntiles = p.batch * tiles_per_e;
 
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], 1);
-    mbar_init(&empty[1], 1);
+    for (int q = 0; q < NST; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], 1);
+    }
     mbar_init(tmem_full, 1);
     mbar_init(tmem_empty, 128);
     mbar_init(all_done, 1);
@@ -384,10 +499,11 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm_kernel(OzParams p) {
       auto load = [&](int64_t c) {
         const signed char *a, *b;
         chunk_src(c, a, b);
-        unsigned char* st = stage0 + (c & 1) * stage_bytes;
-        mbar_expect_tx(&full[c & 1], (uint32_t)(abytes + bbytes));
-        bulk_g2s(st, a, (uint32_t)abytes, &full[c & 1]);
-        bulk_g2s(st + abytes, b, (uint32_t)bbytes, &full[c & 1]);
+        const int q = (int)(c % NST);
+        unsigned char* st = stage0 + q * stage_bytes;
+        mbar_expect_tx(&full[q], (uint32_t)(abytes + bbytes));
+        bulk_g2s(st, a, (uint32_t)abytes, &full[q]);
+        bulk_g2s(st + abytes, b, (uint32_t)bbytes, &full[q]);
         issued = c + 1;
       };
       auto prefetch = [&](int64_t c) {
@@ -397,21 +513,14 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm_kernel(OzParams p) {
         bulk_prefetch_l2(a, (uint32_t)abytes);
         bulk_prefetch_l2(b, (uint32_t)bbytes);
       };
-      // keep the next few chunk blocks on their way into L2
-      for (int64_t c = 1; c <= 3; ++c) prefetch(c);
-      if (total > 0) load(0);
+      // every stage filled up front, the next few chunk blocks on their way into L2
+      for (int64_t c = NST; c <= NST + 2; ++c) prefetch(c);
+      for (int64_t c = 0; c < NST && c < total; ++c) load(c);
       for (int64_t c = 0; c < total && ok; ++c) {
-        const int st = (int)(c & 1);
+        const int st = (int)(c % NST);
         const int64_t j = c / p.KT;  // local tile index
         const int kc = (int)(c % p.KT);
-        if (c + 1 < total) {
-          // stage (c+1)&1 was last read by the MMAs of chunk c-1
-          if (c >= 1) ok = mbar_wait(&empty[(c + 1) & 1], (uint32_t)(((c - 1) >> 1) & 1), abort_v);
-          if (!ok) break;
-          load(c + 1);
-          prefetch(c + 4);
-        }
-        ok = mbar_wait(&full[st], (uint32_t)((c >> 1) & 1), abort_v);
+        ok = mbar_wait(&full[st], (uint32_t)((c / NST) & 1), abort_v);
         if (!ok) break;
         consumed = c + 1;
         if (kc == 0 && j >= 1) {
@@ -446,12 +555,22 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm_kernel(OzParams p) {
         }
         umma_commit(&empty[st]);
         if (kc == p.KT - 1) umma_commit(tmem_full);
+        // Refill the stage of chunk c - 1 with chunk c - 1 + NST once its MMAs
+        // are done.  The MMAs of chunk c are already queued behind them, so the
+        // tensor pipe stays busy while this thread waits and copies.
+        const int64_t cn = c - 1 + NST;
+        if (c >= 1 && cn < total) {
+          ok = mbar_wait(&empty[(c - 1) % NST], (uint32_t)(((c - 1) / NST) & 1), abort_v);
+          if (!ok) break;
+          load(cn);
+          prefetch(cn + 3);
+        }
       }
       if (!ok) {
         *abort_v = 1;
         atomicExch(&g_mixed_wait_error, 1);
         // let the bulk copies already issued land before the CTA can exit
-        for (int64_t c = consumed; c < issued; ++c) mbar_wait(&full[c & 1], (uint32_t)((c >> 1) & 1));
+        for (int64_t c = consumed; c < issued; ++c) mbar_wait(&full[c % NST], (uint32_t)((c / NST) & 1));
       }
       // completes once every MMA issued above has finished
       umma_commit(all_done);
@@ -481,10 +600,10 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm_kernel(OzParams p) {
         int v[32];
         tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(l * 2) * TN, v);
 #pragma unroll
-        for (int jj = 0; jj < TN; ++jj) acc_re[jj] = fma((double)v[jj], scale, acc_re[jj]);
+        for (int jj = 0; jj < TN; ++jj) acc_re[jj] = fma(i32_to_f64(v[jj]), scale, acc_re[jj]);
         tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(l * 2 + 1) * TN, v);
 #pragma unroll
-        for (int jj = 0; jj < TN; ++jj) acc_im[jj] = fma((double)v[jj], scale, acc_im[jj]);
+        for (int jj = 0; jj < TN; ++jj) acc_im[jj] = fma(i32_to_f64(v[jj]), scale, acc_im[jj]);
       }
       // accumulators read: the next tile's MMAs may overwrite them
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -501,7 +620,15 @@ __global__ void __launch_bounds__(THREADS, 1) ozaki_gemm_kernel(OzParams p) {
           const int col = nt * TN + jj;
           if (col < p.N) {
             const int ex = ea + p.eb[(p.b_shared ? 0 : e) * p.N + col];
-            cplx v = cmul(p.alpha, cmk(ldexp(acc_re[jj], ex), ldexp(acc_im[jj], ex)));
+            cplx v;
+            if (ex >= -1022 && ex <= 1023) {
+              // 2^ex from its bit pattern: one multiply, the same rounding as ldexp
+              const double sc = __longlong_as_double((long long)(ex + 1023) << 52);
+              v = cmk(acc_re[jj] * sc, acc_im[jj] * sc);
+            } else {
+              v = cmk(ldexp(acc_re[jj], ex), ldexp(acc_im[jj], ex));
+            }
+            v = cmul(p.alpha, v);
             if (c) v = cfma(p.beta, c[col], v);
             if (c2) v = cfma(p.gamma, c2[col], v);
             if (p.diag_shift && row == col) v = cadd(v, p.diag_shift[e]);
@@ -555,10 +682,8 @@ void launch_zgemm_mixed(const GemmCall& g, cudaStream_t stream) {
   const size_t abytes = (size_t)a_batch * Mt * KT * a_block_bytes(S);
   const size_t bbytes = (size_t)b_batch * Nt * KT * b_block_bytes(S);
   const size_t ebytes = sizeof(int) * (size_t)(a_batch * g.m + b_batch * g.n) + sizeof(int);
-  unsigned char* buf = nullptr;
-  cudaError_t err = cudaMallocAsync(&buf, abytes + bbytes + ebytes + 512, stream);
-  if (err != cudaSuccess) {
-    cudaGetLastError();
+  unsigned char* buf = static_cast<unsigned char*>(qtx_malloc_async(abytes + bbytes + ebytes + 512, stream));
+  if (!buf) {
     throw QtxError(QTX_E_NOMEM, "mixed-precision GEMM: slice buffer allocation failed");
   }
   signed char* as = reinterpret_cast<signed char*>(buf);
@@ -573,20 +698,9 @@ void launch_zgemm_mixed(const GemmCall& g, cudaStream_t stream) {
     // op(B)[k][n]: op N -> b[k * ldb + n] (n adjacent); op C -> conj(b[n * ldb + k]) (k adjacent)
     const bool b_n = g.op_b == OP_N;
     const int64_t bsi = b_n ? 1 : g.b.ld, bsk = b_n ? g.b.ld : 1;
-    auto grid_of = [](int64_t work, int per_block) {
-      return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + per_block - 1) / per_block, 148 * 64));
-    };
-    ozaki_exponent_kernel<<<grid_of(a_batch * (int64_t)g.m * (a_n ? 32 : 8), 256), 256, 0, stream>>>(
-        g.m, g.k, a_batch, g.a.ptr, asi, ask, g.a.stride, a_n ? 1 : 0, ea);
-    qtx_check_launch("ozaki_exponent_kernel");
-    ozaki_exponent_kernel<<<grid_of(b_batch * (int64_t)g.n * (b_n ? 8 : 32), 256), 256, 0, stream>>>(
-        g.n, g.k, b_batch, g.b.ptr, bsi, bsk, g.b.stride, b_n ? 0 : 1, eb);
-    qtx_check_launch("ozaki_exponent_kernel");
-    const int groups = KT * (KC / 16);
-    launch_slices<2>(S, grid_of(a_batch * (int64_t)Mt * TM * groups, 256), stream, g.m, g.k, a_batch, g.a.ptr, asi,
-                     ask, g.a.stride, a_n ? 0 : 1, a_n ? 0 : 1, KT, TM, ea, as);
-    launch_slices<4>(S, grid_of(b_batch * (int64_t)Nt * TN * groups, 256), stream, g.n, g.k, b_batch, g.b.ptr, bsi,
-                     bsk, g.b.stride, b_n ? 0 : 1, b_n ? 1 : 0, KT, TN, eb, bs);
+    // rows of op(A) are adjacent in memory for op C, rows of op(B)^T (columns of op(B)) for op N
+    launch_split<2>(S, stream, g.m, g.k, a_batch, g.a.ptr, asi, ask, g.a.stride, a_n ? 0 : 1, !a_n, KT, TM, ea, as);
+    launch_split<4>(S, stream, g.n, g.k, b_batch, g.b.ptr, bsi, bsk, g.b.stride, b_n ? 0 : 1, b_n, KT, TN, eb, bs);
   }
   OzParams p;
   p.M = g.m; p.N = g.n; p.K = g.k; p.S = S; p.KT = KT; p.Mt = Mt; p.Nt = Nt; p.batch = g.batch;
@@ -598,11 +712,17 @@ void launch_zgemm_mixed(const GemmCall& g, cudaStream_t stream) {
   p.a_shared = a_batch == 1 && g.batch > 1;
   p.b_shared = b_batch == 1 && g.batch > 1;
   const int stage_bytes = ((a_block_bytes(S) + b_block_bytes(S) + 1023) / 1024) * 1024;
-  const size_t smem = 2 * (size_t)stage_bytes + 128;
-  static size_t configured = 0;
-  if (smem > configured) {
-    QTX_CUDA_TRY(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = smem;
+  // as many stages as fit next to the barrier words (S = 7: 2, S <= 6: 3)
+  p.nst = std::min<int>(MAX_STAGES, (MAX_SMEM - BAR_BYTES) / stage_bytes);
+  const size_t smem = (size_t)p.nst * stage_bytes + BAR_BYTES;
+  {
+    static std::mutex m;
+    static size_t configured = 0;
+    std::lock_guard<std::mutex> lk(m);
+    if (smem > configured) {
+      QTX_CUDA_TRY(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      configured = smem;
+    }
   }
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);

@@ -26,6 +26,8 @@
 // matrices); shared memory holds the panel (n x Wp, XOR-swizzled so that both
 // row-per-thread access and DMMA fragment loads are conflict-free), two slabs
 // of pivot rows and the permutation arrays.
+#include <mutex>
+
 #include "kernels.h"
 
 namespace {
@@ -397,10 +399,14 @@ void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const in
   if (n <= 0 || batch <= 0) return;
   if (n > 512) throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size above 512");
   size_t smem = inv_smem_bytes(n);
-  static size_t configured = 0;
-  if (smem > configured) {
-    cudaFuncSetAttribute(zinv_gj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = smem;
+  {
+    static std::mutex m;
+    static size_t configured = 0;
+    std::lock_guard<std::mutex> lk(m);
+    if (smem > configured) {
+      cudaFuncSetAttribute(zinv_gj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      configured = smem;
+    }
   }
   InvShape s = inv_shape(n);
   // every panel row / column must be owned by the elimination mapping

@@ -85,6 +85,20 @@ class TransportSolver:
                 out[k] = torch.empty((ne, 2), dtype=torch.int32, device=dev)
         return out
 
+    def release_graphs(self, stream=None) -> None:
+        """Drop the captured sweeps of this solver's context (stream-ordered free)."""
+        lib = _lib.load()
+        ctx = self.ctx if self.ctx is not None else _lib.context(self.cuda)
+        s = self._stream_handle(stream)
+        _lib.check(lib.qtx_ctx_release_graphs(ctx, s), ctx, "ctx_release_graphs")
+
+    def _stream_handle(self, stream=None):
+        if stream is None:
+            stream = self.stream
+        if stream is None:
+            return torch.cuda.current_stream(self.cuda).cuda_stream
+        return stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+
     def solve(self, energies, outputs: dict | None = None, keys=OUTPUT_KEYS, stream=None) -> dict:
         """Solve at the given energies (device or host array); returns the output dict."""
         e = energies if isinstance(energies, torch.Tensor) else torch.as_tensor(np.asarray(energies, dtype=np.float64))
@@ -107,12 +121,7 @@ class TransportSolver:
             mu_right=self.dev.mu_right, kt=self.dev.kt, sr_tol=self.dev.sr_tol,
             sr_max_iterations=self.dev.sr_max_iter, max_batch_size=self.max_batch_size)
         o = _lib.TransportOutputs(**{k: (outputs[k].data_ptr() if k in outputs else None) for k in OUTPUT_KEYS})
-        if stream is None:
-            stream = self.stream
-        if stream is None:
-            s = torch.cuda.current_stream(self.cuda).cuda_stream
-        else:
-            s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        s = self._stream_handle(stream)
         st = lib.qtx_transport_solve(ctx, ctypes.byref(p), ctypes.byref(o), _PRECISIONS[self.precision], flags, s)
         _lib.check(st, ctx, "transport_solve")
         return outputs

@@ -111,3 +111,26 @@ def test_autotuner_persists(tmp_path):
     assert os.path.exists(path)
     t2 = Autotuner(cache_path=path)
     assert t2.lookup(32, 16, "mixed") == json.load(open(path))[Autotuner.key(32, 16, "mixed")]
+
+
+def test_graph_scalars_in_key_and_release():
+    """A captured sweep is replayed only for the scalars it was captured with,
+    and released graphs are captured again on the next call."""
+    import dataclasses
+
+    dev = make_device(num_blocks=5, block_size=32, num_energies=6, seed=4)
+    s = TransportSolver(dev, max_batch_size=6, use_graph=True)
+    out = s.allocate_outputs(6, OBSERVABLE_KEYS)
+    s.solve(dev.energies, out)
+    dev2 = dataclasses.replace(dev, eta=1e-4, mu_left=dev.mu_left + 0.05)
+    s2 = TransportSolver(dev2, max_batch_size=6, use_graph=True, h_diag=s.h_diag, h_upper=s.h_upper)
+    s2._e_buf = s._e_buf  # same energy buffer: only the scalars differ from the first capture
+    got = s2.solve(dev.energies, out)
+    want = TransportSolver(dev2, max_batch_size=6).solve(dev.energies, keys=OBSERVABLE_KEYS)
+    for k in ("density", "transmission", "current_left"):
+        assert torch.equal(got[k], want[k]), k
+    s.release_graphs()
+    again = s.solve(dev.energies, out)
+    ref = TransportSolver(dev, max_batch_size=6).solve(dev.energies, keys=OBSERVABLE_KEYS)
+    for k in ("density", "transmission", "current_left"):
+        assert torch.equal(again[k], ref[k]), k
