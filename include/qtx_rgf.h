@@ -63,8 +63,9 @@ typedef int qtx_status;
 
 /* precision of the bulk block products */
 #define QTX_PREC_FP64 0        /* complex128 throughout */
-#define QTX_PREC_MIXED 1       /* bulk Schur/Keldysh products in 3xTF32 complex FP32 on tcgen05;
-                                  inverses, Sancho-Rubio and the refinement residual in FP64 */
+#define QTX_PREC_MIXED 1       /* bulk Schur/Keldysh products of the sweep as 7-bit integer slice
+                                  products on the INT8 tensor cores (tcgen05 kind::i8, exact INT32
+                                  accumulation, FP64 combine); block inverses and Sancho-Rubio in FP64 */
 
 /* flags of qtx_selected_solve */
 #define QTX_FLAG_RETURN_RETARDED 0x1u  /* write diagonal X^R blocks to xr (rgf.py:304-305, 403-404) */
@@ -224,6 +225,59 @@ typedef struct qtx_transport_outputs {
 
 qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,
                                int32_t precision, uint32_t flags, qtx_stream stream);
+
+/* Device bytes one qtx_transport_solve call allocates for itself (recursion
+ * state, couplings, Sancho-Rubio and, for QTX_PREC_MIXED, the slice buffers)
+ * when it processes `energies_per_call` energies at a time; H and the outputs
+ * are the caller's and not included.  Used for admission control. */
+size_t qtx_transport_footprint(int32_t num_blocks, int32_t block_size, int64_t energies_per_call,
+                               int32_t precision);
+
+/* ---------------------------------------------------------------------------
+ * Continuous-batching transport server (the serving form; no reference
+ * counterpart: the reference solves one request at a time).
+ *
+ * `slots` worker threads, each with its own context and CUDA stream, take
+ * requests in arrival order.  The oldest waiting request is admitted as soon
+ * as a slot is free and its footprint (qtx_transport_footprint) fits in
+ * `memory_budget` next to the running requests, so requests that arrive while
+ * others run overlap with them on the device.  A request whose footprint
+ * exceeds the whole budget is refused at submission (QTX_E_NOMEM).  The
+ * problem's device arrays (H, energies) and the outputs belong to the caller
+ * and must stay valid until the request has completed.
+ * ------------------------------------------------------------------------- */
+typedef struct qtx_server qtx_server;
+
+typedef struct qtx_server_config {
+  int32_t device;
+  int32_t slots;          /* concurrent requests (>= 1) */
+  size_t memory_budget;   /* device bytes the running requests may hold; 0 = half of the free memory */
+} qtx_server_config;
+
+typedef struct qtx_server_stats {
+  int64_t submitted, completed, failed, queued, running, peak_running;
+  int64_t solves;             /* energies of the completed requests */
+  size_t memory_in_use;       /* footprint of the running requests */
+  double p50_latency_s, p99_latency_s, mean_latency_s;  /* completion - submission */
+} qtx_server_stats;
+
+qtx_status qtx_server_create(const qtx_server_config* cfg, qtx_server** out);
+/* Finishes every request already submitted, then stops the workers. */
+qtx_status qtx_server_destroy(qtx_server* srv);
+/* Enqueue one request (precision and flags as for qtx_transport_solve; the
+ * problem's max_batch_size sets the energies per device call). */
+qtx_status qtx_server_submit(qtx_server* srv, const qtx_transport_problem* p, const qtx_transport_outputs* o,
+                             int32_t precision, uint32_t flags, int64_t* request_id);
+/* Wait up to timeout_ms (< 0: no limit) for request `request_id`.  Returns
+ * QTX_E_TIMEOUT if it has not completed, QTX_E_INVAL for an unknown or already
+ * collected id, else QTX_OK with the request's own status, latency and error
+ * text (err may be NULL); the request is collected. */
+qtx_status qtx_server_wait(qtx_server* srv, int64_t request_id, int64_t timeout_ms, qtx_status* request_status,
+                           double* latency_s, char* err, int32_t err_len);
+/* As qtx_server_wait, for whichever uncollected request completes first. */
+qtx_status qtx_server_wait_any(qtx_server* srv, int64_t timeout_ms, int64_t* request_id, qtx_status* request_status,
+                               double* latency_s, char* err, int32_t err_len);
+qtx_status qtx_server_get_stats(qtx_server* srv, qtx_server_stats* stats);
 
 /* Number of captured-sweep replays issued by this context (QTX_FLAG_GRAPH). */
 int64_t qtx_graph_replays(const qtx_ctx* ctx);

@@ -99,6 +99,18 @@ class TransportOutputs(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", c_int32), ("slots", c_int32), ("memory_budget", ctypes.c_size_t)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", c_int64), ("completed", c_int64), ("failed", c_int64), ("queued", c_int64),
+        ("running", c_int64), ("peak_running", c_int64), ("solves", c_int64), ("memory_in_use", ctypes.c_size_t),
+        ("p50_latency_s", c_double), ("p99_latency_s", c_double), ("mean_latency_s", c_double),
+    ]
+
+
 # (name, restype, argtypes) of every exported symbol, mirroring include/qtx_rgf.h
 SIGNATURES = {
     "qtx_version": (ctypes.c_char_p, []),
@@ -156,6 +168,24 @@ SIGNATURES = {
         c_int32,
         [c_void_p, ctypes.POINTER(TransportProblem), ctypes.POINTER(TransportOutputs), c_int32, c_uint32, c_void_p],
     ),
+    "qtx_transport_footprint": (ctypes.c_size_t, [c_int32, c_int32, c_int64, c_int32]),
+    "qtx_server_create": (c_int32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(c_void_p)]),
+    "qtx_server_destroy": (c_int32, [c_void_p]),
+    "qtx_server_submit": (
+        c_int32,
+        [c_void_p, ctypes.POINTER(TransportProblem), ctypes.POINTER(TransportOutputs), c_int32, c_uint32,
+         ctypes.POINTER(c_int64)],
+    ),
+    "qtx_server_wait": (
+        c_int32,
+        [c_void_p, c_int64, c_int64, ctypes.POINTER(c_int32), ctypes.POINTER(c_double), ctypes.c_char_p, c_int32],
+    ),
+    "qtx_server_wait_any": (
+        c_int32,
+        [c_void_p, c_int64, ctypes.POINTER(c_int64), ctypes.POINTER(c_int32), ctypes.POINTER(c_double),
+         ctypes.c_char_p, c_int32],
+    ),
+    "qtx_server_get_stats": (c_int32, [c_void_p, ctypes.POINTER(ServerStats)]),
 }
 
 _lib = None
@@ -221,6 +251,21 @@ def new_context(device: int) -> int:
 
 def destroy_context(ctx: int) -> None:
     load().qtx_ctx_destroy(ctx)
+
+
+def status_error(status: int, what: str, msg: str):
+    """The exception (or None for OK / not converged) of a status code."""
+    if status in (QTX_OK, QTX_E_NOT_CONVERGED):
+        return None
+    if status == QTX_E_INVAL:
+        return ValueError(f"{what}: {msg}")
+    if status == QTX_E_SINGULAR:
+        return np.linalg.LinAlgError(f"{what}: {msg}")
+    if status == QTX_E_NOMEM:
+        return MemoryError(f"{what}: {msg}")
+    if status == QTX_E_UNSUPPORTED:
+        return NotImplementedError(f"{what}: {msg}")
+    return QtxError(status, f"{what}: {msg}")
 
 
 def check(status: int, ctx: int, what: str) -> None:

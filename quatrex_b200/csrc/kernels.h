@@ -41,6 +41,9 @@ void launch_zgemm(const GemmCall& g, cudaStream_t stream);
 // INT32 accumulation (Ozaki scheme); see zgemm_ozaki.cu.
 void launch_zgemm_mixed(const GemmCall& g, cudaStream_t stream);
 bool mixed_supported(const GemmCall& g);
+// Device bytes of the slice buffers of one mixed GEMM (m x n x k, batch entries
+// per operand; an operand with batch stride 0 counts once).
+size_t mixed_workspace_bytes(int m, int n, int k, int64_t a_batch, int64_t b_batch);
 // Throws QTX_E_TIMEOUT (and clears the flag) if a mixed GEMM since the last
 // check gave up a pipeline wait.  Synchronises the stream.
 void mixed_check_error(cudaStream_t stream);

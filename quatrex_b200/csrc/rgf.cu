@@ -1187,6 +1187,16 @@ int64_t qtx_launch_count(const qtx_ctx* ctx) { return ctx ? ctx->launches : -1; 
 
 int64_t qtx_graph_replays(const qtx_ctx* ctx) { return ctx ? ctx->graph_replays : -1; }
 
+size_t qtx_transport_footprint(int32_t num_blocks, int32_t block_size, int64_t energies_per_call, int32_t precision) {
+  if (num_blocks < 2 || block_size < 1 || energies_per_call < 1) return 0;
+  const size_t b = (size_t)block_size, ne = (size_t)energies_per_call;
+  size_t bytes = transport_ws_bytes(num_blocks, block_size, energies_per_call);
+  bytes += sizeof(cplx) * 9 * b * b * ne + sizeof(int) * (2 * ne + 2);  // Sancho-Rubio
+  if (precision == QTX_PREC_MIXED)
+    bytes += mixed_workspace_bytes(block_size, block_size, block_size, energies_per_call, energies_per_call);
+  return bytes + (4u << 20);  // allocator granularity
+}
+
 qtx_status qtx_ctx_release_graphs(qtx_ctx* ctx, qtx_stream stream) {
   return guarded(ctx, [&] { ctx->graphs.clear(static_cast<cudaStream_t>(stream)); });
 }

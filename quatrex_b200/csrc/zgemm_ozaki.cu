@@ -659,6 +659,14 @@ int ozaki_slices() {
 
 bool mixed_supported(const GemmCall& g) { return g.k > 0 && g.k <= 16384; }
 
+size_t mixed_workspace_bytes(int m, int n, int k, int64_t a_batch, int64_t b_batch) {
+  const int S = ozaki_slices();
+  const int KT = (k + KC - 1) / KC;
+  const int Mt = (m + TM - 1) / TM, Nt = (n + TN - 1) / TN;
+  return (size_t)a_batch * Mt * KT * a_block_bytes(S) + (size_t)b_batch * Nt * KT * b_block_bytes(S) +
+         sizeof(int) * (size_t)(a_batch * m + b_batch * n) + 1024;
+}
+
 void mixed_check_error(cudaStream_t stream) {
   int flag = 0;
   QTX_CUDA_TRY(cudaMemcpyFromSymbolAsync(&flag, g_mixed_wait_error, sizeof(int), 0, cudaMemcpyDeviceToHost, stream));

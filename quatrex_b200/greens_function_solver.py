@@ -143,8 +143,9 @@ class RGF(GFSolver):
     max_batch_size : int, optional
         Maximum number of stack entries solved together, by default 100.
     precision : {"fp64", "mixed"}
-        "fp64": complex128 throughout.  "mixed": bulk block products in
-        3xTF32 complex FP32 on the tensor cores, inverses in FP64.
+        "fp64": complex128 throughout.  "mixed": bulk block products as
+        7-bit integer slice products on the INT8 tensor cores with exact
+        accumulation (Ozaki scheme), inverses in FP64.
     """
 
     def __init__(self, max_batch_size: int = 100, precision: str = "fp64") -> None:

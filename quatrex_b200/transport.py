@@ -26,6 +26,31 @@ OUTPUT_KEYS = ("gr_diag", "gr_upper", "gr_lower", "gl_diag", "gl_upper", "gg_dia
                "hole_density", "transmission", "current_left", "current_right", "sr_iterations")
 
 
+def allocate_outputs(num_blocks: int, block_size: int, num_energies: int, keys=OUTPUT_KEYS,
+                     cuda_device: int = 0) -> dict:
+    """Device output arrays of qtx_transport_solve for the given keys."""
+    nb, b, ne = int(num_blocks), int(block_size), int(num_energies)
+    dev = f"cuda:{cuda_device}"
+    shapes = {
+        "gr_diag": (ne, nb, b, b), "gr_upper": (ne, nb - 1, b, b), "gr_lower": (ne, nb - 1, b, b),
+        "gl_diag": (ne, nb, b, b), "gl_upper": (ne, nb - 1, b, b),
+        "gg_diag": (ne, nb, b, b), "gg_upper": (ne, nb - 1, b, b),
+    }
+    out = {}
+    for k in keys:
+        if k in shapes:
+            out[k] = torch.empty(shapes[k], dtype=torch.complex128, device=dev)
+        elif k in ("density", "hole_density"):
+            out[k] = torch.empty((ne, nb), dtype=torch.float64, device=dev)
+        elif k == "transmission":
+            out[k] = torch.empty((ne,), dtype=torch.float64, device=dev)
+        elif k in ("current_left", "current_right"):
+            out[k] = torch.empty((ne,), dtype=torch.complex128, device=dev)
+        elif k == "sr_iterations":
+            out[k] = torch.empty((ne, 2), dtype=torch.int32, device=dev)
+    return out
+
+
 class TransportSolver:
     """Device-resident transport solver for one ``TransportDevice``."""
 
@@ -64,26 +89,7 @@ class TransportSolver:
         return int(h + ws + sr + out)
 
     def allocate_outputs(self, num_energies: int, keys=OUTPUT_KEYS) -> dict:
-        nb, b, ne = self.nb, self.b, int(num_energies)
-        dev = f"cuda:{self.cuda}"
-        shapes = {
-            "gr_diag": (ne, nb, b, b), "gr_upper": (ne, nb - 1, b, b), "gr_lower": (ne, nb - 1, b, b),
-            "gl_diag": (ne, nb, b, b), "gl_upper": (ne, nb - 1, b, b),
-            "gg_diag": (ne, nb, b, b), "gg_upper": (ne, nb - 1, b, b),
-        }
-        out = {}
-        for k in keys:
-            if k in shapes:
-                out[k] = torch.empty(shapes[k], dtype=torch.complex128, device=dev)
-            elif k in ("density", "hole_density"):
-                out[k] = torch.empty((ne, nb), dtype=torch.float64, device=dev)
-            elif k == "transmission":
-                out[k] = torch.empty((ne,), dtype=torch.float64, device=dev)
-            elif k in ("current_left", "current_right"):
-                out[k] = torch.empty((ne,), dtype=torch.complex128, device=dev)
-            elif k == "sr_iterations":
-                out[k] = torch.empty((ne, 2), dtype=torch.int32, device=dev)
-        return out
+        return allocate_outputs(self.nb, self.b, num_energies, keys, self.cuda)
 
     def release_graphs(self, stream=None) -> None:
         """Drop the captured sweeps of this solver's context (stream-ordered free)."""

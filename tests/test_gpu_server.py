@@ -1,0 +1,109 @@
+"""The native continuous-batching server (qtx_server_*) through the C ABI:
+results equal a direct qtx_transport_solve of the same request, requests are
+collected by id or in completion order, statistics add up, and requests over
+the budget or malformed are refused at submission."""
+
+import ctypes
+
+import pytest
+import torch
+
+from quatrex_b200 import _lib
+from quatrex_b200.transport import TransportSolver, allocate_outputs
+from quatrex_b200.workloads import make_device
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("density", "transmission", "current_left", "sr_iterations")
+
+
+def _problem(dev, h_diag, h_upper, e, ne_call):
+    return _lib.TransportProblem(
+        num_blocks=dev.num_blocks, block_size=dev.block_size, num_energies=int(e.shape[0]),
+        h_diag=h_diag.data_ptr(), h_upper=h_upper.data_ptr(), energies=e.data_ptr(), eta=dev.eta,
+        mu_left=dev.mu_left, mu_right=dev.mu_right, kt=dev.kt, sr_tol=dev.sr_tol,
+        sr_max_iterations=dev.sr_max_iter, max_batch_size=ne_call)
+
+
+def _outputs(out):
+    return _lib.TransportOutputs(**{name: (out[name].data_ptr() if name in out else None)
+                                    for name, _ in _lib.TransportOutputs._fields_})
+
+
+def _server(slots=3, budget=0):
+    lib = _lib.load()
+    cfg = _lib.ServerConfig(device=torch.cuda.current_device(), slots=slots, memory_budget=budget)
+    h = ctypes.c_void_p()
+    assert lib.qtx_server_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.QTX_OK
+    return lib, h.value
+
+
+def test_native_server_matches_direct_solve():
+    lib, srv = _server()
+    devs = [make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=30 + i)
+            for i, (nb, b, ne) in enumerate([(5, 32, 9), (7, 16, 12), (4, 64, 6), (6, 32, 10)])]
+    keep, ids = [], []
+    try:
+        for d in devs:
+            h_diag = torch.from_numpy(d.h_diag).cuda()
+            h_upper = torch.from_numpy(d.h_upper).cuda()
+            e = torch.from_numpy(d.energies).cuda()
+            out = allocate_outputs(d.num_blocks, d.block_size, len(d.energies), KEYS, torch.cuda.current_device())
+            torch.cuda.synchronize()
+            p, o = _problem(d, h_diag, h_upper, e, 4), _outputs(out)
+            rid = ctypes.c_int64()
+            assert lib.qtx_server_submit(srv, ctypes.byref(p), ctypes.byref(o), _lib.QTX_PREC_FP64, 0,
+                                         ctypes.byref(rid)) == _lib.QTX_OK
+            keep.append((d, out, h_diag, h_upper, e, p, o))
+            ids.append(rid.value)
+        status, lat = ctypes.c_int32(), ctypes.c_double()
+        # the last one by id, the others in completion order
+        assert lib.qtx_server_wait(srv, ids[-1], -1, ctypes.byref(status), ctypes.byref(lat), None, 0) == 0
+        assert status.value == _lib.QTX_OK and lat.value > 0
+        got = {ids[-1]}
+        rid = ctypes.c_int64()
+        while len(got) < len(ids):
+            st = lib.qtx_server_wait_any(srv, 60000, ctypes.byref(rid), ctypes.byref(status), ctypes.byref(lat),
+                                         None, 0)
+            assert st == _lib.QTX_OK and status.value == _lib.QTX_OK
+            got.add(rid.value)
+        assert got == set(ids)
+        # collected ids are unknown afterwards
+        assert lib.qtx_server_wait(srv, ids[0], 0, ctypes.byref(status), ctypes.byref(lat), None, 0) == \
+            _lib.QTX_E_INVAL
+        stats = _lib.ServerStats()
+        assert lib.qtx_server_get_stats(srv, ctypes.byref(stats)) == 0
+        assert stats.submitted == stats.completed == len(devs) and stats.failed == 0
+        assert stats.solves == sum(len(d.energies) for d in devs)
+        assert stats.p99_latency_s >= stats.p50_latency_s > 0 and stats.running == 0 and stats.queued == 0
+    finally:
+        assert lib.qtx_server_destroy(srv) == 0
+    for d, out, *_ in keep:
+        ref = TransportSolver(d, max_batch_size=4).solve(d.energies, keys=KEYS)
+        for k in KEYS:
+            assert torch.equal(out[k], ref[k]), k
+
+
+def test_native_server_refuses_over_budget_and_bad_requests():
+    lib, srv = _server(slots=1, budget=1 << 20)
+    try:
+        d = make_device(num_blocks=6, block_size=64, num_energies=8, seed=3)
+        h_diag = torch.from_numpy(d.h_diag).cuda()
+        h_upper = torch.from_numpy(d.h_upper).cuda()
+        e = torch.from_numpy(d.energies).cuda()
+        out = allocate_outputs(6, 64, 8, KEYS, torch.cuda.current_device())
+        p, o = _problem(d, h_diag, h_upper, e, 8), _outputs(out)
+        rid = ctypes.c_int64()
+        need = lib.qtx_transport_footprint(6, 64, 8, _lib.QTX_PREC_FP64)
+        assert need > (1 << 20)
+        assert lib.qtx_server_submit(srv, ctypes.byref(p), ctypes.byref(o), 0, 0, ctypes.byref(rid)) == \
+            _lib.QTX_E_NOMEM
+        p.num_blocks = 1
+        assert lib.qtx_server_submit(srv, ctypes.byref(p), ctypes.byref(o), 0, 0, ctypes.byref(rid)) == \
+            _lib.QTX_E_INVAL
+        status, lat = ctypes.c_int32(), ctypes.c_double()
+        assert lib.qtx_server_wait_any(srv, 10, ctypes.byref(rid), ctypes.byref(status), ctypes.byref(lat),
+                                       None, 0) == _lib.QTX_E_TIMEOUT
+    finally:
+        assert lib.qtx_server_destroy(srv) == 0
+

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def _header_symbols():
     text = open(os.path.join(ROOT, "include", "qtx_rgf.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:qtx_status|const char\*|int64_t)\s+(qtx_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:qtx_status|const char\*|int64_t|size_t)\s+(qtx_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_header_symbol():
@@ -106,3 +106,16 @@ def test_set_get_block_and_zeros_like():
     z.blocks[1, 2] = val
     assert np.allclose(z.blocks[1, 2], val)
     assert np.allclose(z.to_dense()[2][3:6, 6:9], val)
+
+
+def test_transport_footprint_is_host_arithmetic():
+    """Admission footprint of one transport call: grows with the energies per
+    call and with the slice buffers of the mixed form; invalid shapes give 0."""
+    lib = _lib.load()
+    f8 = lib.qtx_transport_footprint(16, 64, 8, _lib.QTX_PREC_FP64)
+    f16 = lib.qtx_transport_footprint(16, 64, 16, _lib.QTX_PREC_FP64)
+    m16 = lib.qtx_transport_footprint(16, 64, 16, _lib.QTX_PREC_MIXED)
+    assert 0 < f8 < f16 < m16
+    # the recursion state alone: 3 nb + 20 block stacks of 16 b^2 bytes per energy
+    assert f16 - f8 >= 8 * (3 * 16 + 20) * 16 * 64 * 64
+    assert lib.qtx_transport_footprint(1, 64, 8, _lib.QTX_PREC_FP64) == 0
