@@ -39,6 +39,8 @@ sys.path.insert(0, ROOT)
 
 FP64_DMMA_PEAK_TFLOPS = 37.0  # measured on this pool's B200s: mma.sync m8n8k4 f64 issue-rate probe
 FP64_PEAK_SOURCE = "measured: DMMA issue-rate probe on B200 (profiles/fp64_peak_b200.md)"
+GEMM_TRAFFIC_BYTES = 373.1e6  # zgemm_dmma_kernel, b = 256, batch 128: 269.0 MB read + 104.1 MB written
+OZAKI_TRAFFIC_BYTES = 459.7e6  # ozaki_gemm_kernel, same shape: 352.7 MB read (slices) + 107.0 MB written
 
 
 def _workload(args):
@@ -296,7 +298,10 @@ def run_ours(args):
         "kernel": "zgemm_dmma_kernel", "bound": "tensor", "achieved": round(gemm_tflops, 3),
         "peak": FP64_DMMA_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": round(gemm_tflops / FP64_DMMA_PEAK_TFLOPS, 4),
         "peak_source": FP64_PEAK_SOURCE,
-        "traffic": None,
+        # DRAM bytes of one launch of this kernel at the bench shape (b = 256, 128 energies), from one ncu
+        # capture; the algorithmic minimum is 402.7 MB (A, B read, D written once)
+        "traffic": GEMM_TRAFFIC_BYTES,
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/zgemm_dmma_b256_batch128.md",
         "gemm_launches": gemm["launches"], "gemm_ms": round(gemm["ms"], 3),
         "gemm_share_of_step": round(gemm["ms"] / elapsed_ms, 4) if elapsed_ms > 0 else None,
         "inverse_ms": round(inv["ms"], 3), "inverse_launches": inv["launches"],
@@ -308,6 +313,8 @@ def run_ours(args):
     if args.precision == "mixed":
         roofline["kernel"] = ("complex GEMM class: ozaki_split + ozaki_gemm_kernel (INT8 tcgen05) in the sweep, "
                               "zgemm_dmma_kernel in Sancho-Rubio; FP64-equivalent flops")
+        roofline["traffic"] = OZAKI_TRAFFIC_BYTES
+        roofline["traffic_source"] = "ncu capture of ozaki_gemm_kernel, profiles/ozaki_gemm_b256_batch128.md"
 
     # ---- accuracy of the mixed form against the FP64 form (itself within 1e-10
     # of the oracle) on the first energies of the first step

@@ -34,8 +34,6 @@ namespace {
 
 constexpr int THREADS = 256;
 constexpr int NWARPS = THREADS / 32;
-constexpr int MAX_CPT = 32;  // panel columns per thread in the elimination
-constexpr int MAX_RPT = 2;   // panel rows per thread in the elimination
 
 struct InvShape {
   int w;    // panel width
@@ -102,12 +100,13 @@ __device__ __forceinline__ void argmax_combine(double& v, int& i, double v2, int
   }
 }
 
+template <int TPR, int RPT, int CPT>
 __global__ void __launch_bounds__(THREADS, 1)
     zinv_gj_kernel(int n, int64_t batch, const cplx* __restrict__ a_base, int64_t lda, int64_t sa,
                    cplx* x_base, int64_t ldx, int64_t sx, int* info, const int* active) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const InvShape shp = inv_shape(n);
-  const int W = shp.w, WP = shp.wp, CW = shp.cw, TPR = shp.tpr;
+  const int W = shp.w, WP = shp.wp, CW = shp.cw;
   const int LDR = CW + 2;
   cplx* P = reinterpret_cast<cplx*>(smem_raw);
   cplx* Rs = P + (size_t)n * WP;                 // two slabs of W x LDR (pivot rows, panel rows)
@@ -157,15 +156,43 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
       __syncthreads();
 
+      // The thread's panel entries live in registers during the elimination:
+      // reg[q][j] = P[r_own + q * rstride][c_own + j * TPR].  The column factor
+      // of a row comes from the lane of the row's group that holds column kk;
+      // the pivot row is broadcast through shared memory.
+      cplx reg[RPT][CPT];
+#pragma unroll
+      for (int q = 0; q < RPT; ++q)
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          const int r = r_own + q * rstride, c = c_own + j * TPR;
+          reg[q][j] = (r < n && c < w) ? P[pidx(r, c, WP)] : cmk(0, 0);
+        }
+      const int grp0 = lane - c_own;  // first lane of this row's group (groups never straddle warps)
+      // Column kk of the register rows is picked by static selects.  With 32
+      // register columns the loop stays rolled (one copy of its body fits the
+      // instruction cache); narrower rows unroll it.
+      constexpr int kKUnroll = CPT <= 16 ? 32 : 1;
+#pragma unroll kKUnroll
       for (int kk = 0; kk < w; ++kk) {
         const int k = k0 + kk;
+        cplx colv[RPT];
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          cplx v = cmk(0, 0);
+#pragma unroll
+          for (int j = 0; j < CPT; ++j)
+            if (c_own + j * TPR == kk) v = reg[q][j];
+          colv[q] = v;
+        }
         // pivot search: the owner of (r, kk) looks at row r if it is not a pivot yet
         double bv = -1.0;
         int bi = n;
-        if (c_own == (kk % TPR)) {
-          for (int q = 0; q < MAX_RPT; ++q) {
-            int r = r_own + q * rstride;
-            if (r < n && !s_rowflag[r]) argmax_combine(bv, bi, cabs1(P[pidx(r, kk, WP)]), r);
+        if (c_own == kk % TPR) {
+#pragma unroll
+          for (int q = 0; q < RPT; ++q) {
+            const int r = r_own + q * rstride;
+            if (r < n && !s_rowflag[r]) argmax_combine(bv, bi, cabs1(colv[q]), r);
           }
         }
 #pragma unroll
@@ -174,30 +201,40 @@ __global__ void __launch_bounds__(THREADS, 1)
           int i2 = __shfl_down_sync(0xffffffffu, bi, off);
           argmax_combine(bv, bi, v2, i2);
         }
+        // factors of this thread's rows (column kk, from the group's owner lane)
+        cplx f[RPT];
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          const double fx = __shfl_sync(0xffffffffu, colv[q].x, grp0 + kk % TPR);
+          const double fy = __shfl_sync(0xffffffffu, colv[q].y, grp0 + kk % TPR);
+          f[q] = cmk(fx, fy);
+        }
         const int slot = (kk & 1) * NWARPS;
         if (lane == 0) {
           red_v[slot + warp] = bv;
           red_i[slot + warp] = bi;
         }
-        __syncthreads();  // S1: partial maxima and the previous column's writes are visible
+        __syncthreads();  // S1: partial maxima visible; every read of the previous pivot row done
         double v = red_v[slot];
         int p = red_i[slot];
         for (int q = 1; q < NWARPS; ++q) argmax_combine(v, p, red_v[slot + q], red_i[slot + q]);
-        const cplx piv = P[pidx(p, kk, WP)];
-        if (piv.x == 0.0 && piv.y == 0.0 && !zero_pivot) zero_pivot = k + 1;
-        const cplx d = crecip(piv);
-        // read phase: the owners of the pivot row copy it aside; every thread
-        // reads the factors of its rows
-        cplx f[MAX_RPT];
+        // the owners of the pivot row publish it
 #pragma unroll
-        for (int q = 0; q < MAX_RPT; ++q) {
-          int r = r_own + q * rstride;
-          f[q] = (r < n) ? P[pidx(r, kk, WP)] : cmk(0, 0);
+        for (int q = 0; q < RPT; ++q) {
+          if (r_own + q * rstride == p) {
+#pragma unroll
+            for (int j = 0; j < CPT; ++j) {
+              const int c = c_own + j * TPR;
+              if (c < w) pbuf[c] = reg[q][j];
+            }
+          }
         }
-        for (int c = tid; c < w; c += THREADS) pbuf[c] = P[pidx(p, c, WP)];
         // the flag is read by the next column's pivot search, which follows S2
         if (tid == 0) s_rowflag[p] = 1;
-        __syncthreads();  // S2: all reads of this column done
+        __syncthreads();  // S2: the pivot row is in pbuf
+        const cplx piv = pbuf[kk];
+        if (piv.x == 0.0 && piv.y == 0.0 && !zero_pivot) zero_pivot = k + 1;
+        const cplx d = crecip(piv);
         if (tid == 0) {
           // classic row-swap semantics: position k receives row p
           int qpos = row2pos[p];
@@ -209,28 +246,33 @@ __global__ void __launch_bounds__(THREADS, 1)
           perm[k] = qpos;
         }
 #pragma unroll
-        for (int q = 0; q < MAX_RPT; ++q) {
-          int r = r_own + q * rstride;
+        for (int q = 0; q < RPT; ++q) {
+          const int r = r_own + q * rstride;
           if (r >= n) continue;
           if (r == p) {
-#pragma unroll 8
-            for (int j = 0; j < MAX_CPT; ++j) {
-              int c = c_own + j * TPR;
-              if (c < w) P[pidx(r, c, WP)] = (c == kk) ? d : cmul(pbuf[c], d);
+#pragma unroll
+            for (int j = 0; j < CPT; ++j) {
+              const int c = c_own + j * TPR;
+              if (c < w) reg[q][j] = (c == kk) ? d : cmul(pbuf[c], d);
             }
           } else {
             const cplx fd = cmul(f[q], d);
-#pragma unroll 8
-            for (int j = 0; j < MAX_CPT; ++j) {
-              int c = c_own + j * TPR;
-              if (c < w) {
-                cplx* pp = &P[pidx(r, c, WP)];
-                *pp = (c == kk) ? cmk(-fd.x, -fd.y) : cfms(fd, pbuf[c], *pp);
-              }
+#pragma unroll
+            for (int j = 0; j < CPT; ++j) {
+              const int c = c_own + j * TPR;
+              if (c < w) reg[q][j] = (c == kk) ? cmk(-fd.x, -fd.y) : cfms(fd, pbuf[c], reg[q][j]);
             }
           }
         }
       }
+      // panel back to shared memory for the update
+#pragma unroll
+      for (int q = 0; q < RPT; ++q)
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          const int r = r_own + q * rstride, c = c_own + j * TPR;
+          if (r < n && c < w) P[pidx(r, c, WP)] = reg[q][j];
+        }
       __syncthreads();
 
       // ---- 3. rank-w update of the other columns, slabs of CW columns.
@@ -395,27 +437,42 @@ __global__ void __launch_bounds__(THREADS, 1)
 
 }  // namespace
 
-void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t stream) {
-  if (n <= 0 || batch <= 0) return;
-  if (n > 512) throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size above 512");
-  size_t smem = inv_smem_bytes(n);
+namespace {
+
+template <int TPR, int RPT, int CPT>
+void launch_inv_t(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, size_t smem,
+                  cudaStream_t stream) {
   {
     static std::mutex m;
     static size_t configured = 0;
     std::lock_guard<std::mutex> lk(m);
     if (smem > configured) {
-      cudaFuncSetAttribute(zinv_gj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(zinv_gj_kernel<TPR, RPT, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       configured = smem;
     }
   }
-  InvShape s = inv_shape(n);
-  // every panel row / column must be owned by the elimination mapping
-  int rows_per_thread = (n + (THREADS / s.tpr) - 1) / (THREADS / s.tpr);
-  int cols_per_thread = (s.w + s.tpr - 1) / s.tpr;
-  if (rows_per_thread > MAX_RPT || cols_per_thread > MAX_CPT)
-    throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size outside the supported shapes");
   int grid = (int)(batch < 65535 ? batch : 65535);
-  zinv_gj_kernel<<<grid, THREADS, smem, stream>>>(n, batch, a.ptr, a.ld, a.stride, x.ptr, x.ld, x.stride, info,
-                                                  active);
+  zinv_gj_kernel<TPR, RPT, CPT><<<grid, THREADS, smem, stream>>>(n, batch, a.ptr, a.ld, a.stride, x.ptr, x.ld,
+                                                                  x.stride, info, active);
+}
+
+}  // namespace
+
+void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t stream) {
+  if (n <= 0 || batch <= 0) return;
+  if (n > 512) throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size above 512");
+  const size_t smem = inv_smem_bytes(n);
+  const InvShape s = inv_shape(n);
+  // every panel row / column must be owned by the elimination mapping
+  const int rpt = (n + (THREADS / s.tpr) - 1) / (THREADS / s.tpr);
+  const int cpt = (s.w + s.tpr - 1) / s.tpr;
+  // (threads per row, rows per thread) -> instance with enough register columns
+  if (s.tpr == 1 && rpt == 1 && cpt <= 32) launch_inv_t<1, 1, 32>(n, batch, a, x, info, active, smem, stream);
+  else if (s.tpr == 1 && rpt == 2 && cpt <= 16) launch_inv_t<1, 2, 16>(n, batch, a, x, info, active, smem, stream);
+  else if (s.tpr == 2 && rpt == 1 && cpt <= 16) launch_inv_t<2, 1, 16>(n, batch, a, x, info, active, smem, stream);
+  else if (s.tpr == 4 && rpt == 1 && cpt <= 4) launch_inv_t<4, 1, 4>(n, batch, a, x, info, active, smem, stream);
+  else if (s.tpr == 8 && rpt == 1 && cpt <= 4) launch_inv_t<8, 1, 4>(n, batch, a, x, info, active, smem, stream);
+  else if (s.tpr == 16 && rpt == 1 && cpt <= 1) launch_inv_t<16, 1, 1>(n, batch, a, x, info, active, smem, stream);
+  else throw QtxError(QTX_E_UNSUPPORTED, "qtx inverse: block size outside the supported shapes");
   qtx_check_launch("zinv_gj_kernel");
 }

@@ -69,7 +69,7 @@ def test_zgemm_broadcast_operand():
     assert _rel(d, a @ b) < 1e-13
 
 
-@pytest.mark.parametrize("n", [1, 2, 4, 8, 31, 64, 100, 128, 256, 300, 512])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 8, 16, 24, 31, 48, 64, 96, 100, 128, 200, 256, 257, 300, 512])
 def test_inverse_matches_lapack(n):
     rng = np.random.default_rng(n)
     batch = 5
