@@ -74,9 +74,9 @@ inline size_t inv_smem_bytes(int n) {
   InvShape s = inv_shape(n);
   size_t panel = (size_t)n * s.wp * sizeof(cplx);
   size_t slabs = (size_t)slab_elems(n, s) * sizeof(cplx);
-  size_t ints = (size_t)(3 * n + 4) * sizeof(int);
+  size_t ints = (size_t)(3 * n + 32 + 4) * sizeof(int);
   size_t red = 2 * NWARPS * (sizeof(double) + sizeof(int));
-  size_t pivrow = (size_t)s.wp * sizeof(cplx);
+  size_t pivrow = (size_t)2 * NWARPS * s.wp * sizeof(cplx);  // pivot candidates, two column parities
   return panel + slabs + ints + red + pivrow + 256;
 }
 
@@ -91,6 +91,19 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
       : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// 1 / z by Smith's scaled division (R. L. Smith, CACM 5(8), 1962) with one
+// reciprocal and one quotient.
+__device__ __forceinline__ cplx crecip_pivot(cplx z) {
+  if (fabs(z.x) >= fabs(z.y)) {
+    const double r = z.y / z.x;
+    const double t = 1.0 / (z.x + z.y * r);
+    return cmk(t, -r * t);
+  }
+  const double r = z.x / z.y;
+  const double t = 1.0 / (z.x * r + z.y);
+  return cmk(r * t, -t);
 }
 
 __device__ __forceinline__ void argmax_combine(double& v, int& i, double v2, int i2) {
@@ -115,11 +128,12 @@ __global__ void __launch_bounds__(THREADS, 1)
   int* perm = row2pos + n;                       // swap partner of each column (final unscramble)
   // doubles after the int arrays: round the offset up to 16 bytes (3n ints is
   // not a multiple of 8 bytes for odd n)
-  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(perm + n) + 15) & ~uintptr_t(15));
+  int* pivs = perm + n;                          // pivot row of each column of the current panel
+  double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(pivs + 32) + 15) & ~uintptr_t(15));
   int* red_i = reinterpret_cast<int*>(red_v + 2 * NWARPS);
-  cplx* pbuf = reinterpret_cast<cplx*>(red_i + 2 * NWARPS + 2);  // copy of the pivot row (16-byte aligned below)
-  pbuf = reinterpret_cast<cplx*>((reinterpret_cast<uintptr_t>(pbuf) + 15) & ~uintptr_t(15));
-  __shared__ int s_rowflag[1024];                // row already a pivot (n <= 1024)
+  // per warp and column parity: the panel row of the warp's pivot candidate
+  cplx* cand = reinterpret_cast<cplx*>(red_i + 2 * NWARPS + 2);
+  cand = reinterpret_cast<cplx*>((reinterpret_cast<uintptr_t>(cand) + 15) & ~uintptr_t(15));
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -140,7 +154,6 @@ __global__ void __launch_bounds__(THREADS, 1)
         X[(int64_t)r * ldx + c] = A[(int64_t)r * lda + c];
       }
     }
-    for (int r = tid; r < n; r += THREADS) s_rowflag[r] = 0;
     __syncthreads();
 
     for (int k0 = 0; k0 < n; k0 += W) {
@@ -169,100 +182,196 @@ __global__ void __launch_bounds__(THREADS, 1)
           reg[q][j] = (r < n && c < w) ? P[pidx(r, c, WP)] : cmk(0, 0);
         }
       const int grp0 = lane - c_own;  // first lane of this row's group (groups never straddle warps)
-      // Column kk of the register rows is picked by static selects.  With 32
-      // register columns the loop stays rolled (one copy of its body fits the
-      // instruction cache); narrower rows unroll it.
-      constexpr int kKUnroll = CPT <= 16 ? 32 : 1;
-#pragma unroll kKUnroll
-      for (int kk = 0; kk < w; ++kk) {
-        const int k = k0 + kk;
-        cplx colv[RPT];
+      // rows before k0 are the pivots of earlier panels (rows are in the new order now)
+      if constexpr (CPT == 1) {
+        // One column per lane: lane c_own holds column c_own of the rows
+        // r_own + q * rstride; the factors of column kk come by shuffle from
+        // the lane that holds it, the pivot row is one shared-memory word per
+        // lane.  One barrier per column (each warp publishes its candidate's
+        // row before it).
+        uint32_t used_bits = 0;
 #pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          cplx v = cmk(0, 0);
+        for (int q = 0; q < RPT; ++q)
+          if (r_own + q * rstride < k0) used_bits |= 1u << q;
+#pragma unroll 1
+        for (int kk = 0; kk < w; ++kk) {
+          const int k = k0 + kk;
+          const int src = grp0 + kk % TPR;
+          double bv = -1.0;
+          int bi = n;
+          if (c_own == kk % TPR) {
 #pragma unroll
-          for (int j = 0; j < CPT; ++j)
-            if (c_own + j * TPR == kk) v = reg[q][j];
-          colv[q] = v;
-        }
-        // pivot search: the owner of (r, kk) looks at row r if it is not a pivot yet
-        double bv = -1.0;
-        int bi = n;
-        if (c_own == kk % TPR) {
+            for (int q = 0; q < RPT; ++q) {
+              const int r = r_own + q * rstride;
+              if (r < n && !((used_bits >> q) & 1u)) argmax_combine(bv, bi, cabs1(reg[q][0]), r);
+            }
+          }
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            double v2 = __shfl_xor_sync(0xffffffffu, bv, off);
+            int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
+            argmax_combine(bv, bi, v2, i2);
+          }
+          const int par = kk & 1;
+          cplx* my_cand = cand + (size_t)(par * NWARPS + warp) * WP;
+#pragma unroll
+          for (int q = 0; q < RPT; ++q)
+            if (r_own + q * rstride == bi && c_own < w) my_cand[c_own] = reg[q][0];
+          const int slot = par * NWARPS;
+          if (lane == 0) {
+            red_v[slot + warp] = bv;
+            red_i[slot + warp] = bi;
+          }
+          __syncthreads();  // candidates of every warp visible
+          double v = red_v[slot];
+          int p = red_i[slot], pw = 0;
+          for (int q = 1; q < NWARPS; ++q) {
+            const double vq = red_v[slot + q];
+            const int iq = red_i[slot + q];
+            if (vq > v || (vq == v && iq < p)) {
+              v = vq;
+              p = iq;
+              pw = q;
+            }
+          }
+          const cplx* prow = cand + (size_t)(par * NWARPS + pw) * WP;
+          const cplx piv = prow[kk];
+          if (piv.x == 0.0 && piv.y == 0.0 && !zero_pivot) zero_pivot = k + 1;
+          const cplx d = crecip_pivot(piv);
+          if (tid == 0) pivs[kk] = p;
+          const cplx pc = c_own < w ? prow[c_own] : cmk(0, 0);
+          const cplx pd = cmul(pc, d);
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
+            // every lane takes part in the shuffle, whatever its row
+            const double fx = __shfl_sync(0xffffffffu, reg[q][0].x, src);
+            const double fy = __shfl_sync(0xffffffffu, reg[q][0].y, src);
             const int r = r_own + q * rstride;
-            if (r < n && !s_rowflag[r]) argmax_combine(bv, bi, cabs1(colv[q]), r);
-          }
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          double v2 = __shfl_down_sync(0xffffffffu, bv, off);
-          int i2 = __shfl_down_sync(0xffffffffu, bi, off);
-          argmax_combine(bv, bi, v2, i2);
-        }
-        // factors of this thread's rows (column kk, from the group's owner lane)
-        cplx f[RPT];
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          const double fx = __shfl_sync(0xffffffffu, colv[q].x, grp0 + kk % TPR);
-          const double fy = __shfl_sync(0xffffffffu, colv[q].y, grp0 + kk % TPR);
-          f[q] = cmk(fx, fy);
-        }
-        const int slot = (kk & 1) * NWARPS;
-        if (lane == 0) {
-          red_v[slot + warp] = bv;
-          red_i[slot + warp] = bi;
-        }
-        __syncthreads();  // S1: partial maxima visible; every read of the previous pivot row done
-        double v = red_v[slot];
-        int p = red_i[slot];
-        for (int q = 1; q < NWARPS; ++q) argmax_combine(v, p, red_v[slot + q], red_i[slot + q]);
-        // the owners of the pivot row publish it
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          if (r_own + q * rstride == p) {
-#pragma unroll
-            for (int j = 0; j < CPT; ++j) {
-              const int c = c_own + j * TPR;
-              if (c < w) pbuf[c] = reg[q][j];
+            if (r >= n || c_own >= w) continue;
+            if (r == p) {
+              used_bits |= 1u << q;
+              reg[q][0] = (c_own == kk) ? d : pd;
+            } else {
+              const cplx fd = cmul(cmk(fx, fy), d);
+              reg[q][0] = (c_own == kk) ? cmk(-fd.x, -fd.y) : cfms(fd, pc, reg[q][0]);
             }
           }
         }
-        // the flag is read by the next column's pivot search, which follows S2
-        if (tid == 0) s_rowflag[p] = 1;
-        __syncthreads();  // S2: the pivot row is in pbuf
-        const cplx piv = pbuf[kk];
-        if (piv.x == 0.0 && piv.y == 0.0 && !zero_pivot) zero_pivot = k + 1;
-        const cplx d = crecip(piv);
-        if (tid == 0) {
-          // classic row-swap semantics: position k receives row p
-          int qpos = row2pos[p];
-          int rk = pos2row[k];
+      } else {
+        bool used[RPT];
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) used[q] = r_own + q * rstride < k0;
+        // One barrier per column: every warp publishes the panel row of its own
+        // best candidate before the barrier, so afterwards the winner's row is
+        // read directly.  Column kk of the register rows is picked by static
+        // selects; with 32 register columns the loop stays rolled (one copy of
+        // its body fits the instruction cache), narrower rows unroll it.
+        constexpr int kKUnroll = (CPT >= 2 && CPT <= 16) ? 32 : 1;
+#pragma unroll kKUnroll
+        for (int kk = 0; kk < w; ++kk) {
+          const int k = k0 + kk;
+          cplx colv[RPT];
+#pragma unroll
+          for (int q = 0; q < RPT; ++q) {
+            cplx v = cmk(0, 0);
+#pragma unroll
+            for (int j = 0; j < CPT; ++j)
+              if (c_own + j * TPR == kk) v = reg[q][j];
+            colv[q] = v;
+          }
+          // pivot search: the owner of (r, kk) looks at row r if it is not a pivot yet
+          double bv = -1.0;
+          int bi = n;
+          if (c_own == kk % TPR) {
+#pragma unroll
+            for (int q = 0; q < RPT; ++q) {
+              const int r = r_own + q * rstride;
+              if (r < n && !used[q]) argmax_combine(bv, bi, cabs1(colv[q]), r);
+            }
+          }
+          // butterfly: every lane ends with the warp's best candidate
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            double v2 = __shfl_xor_sync(0xffffffffu, bv, off);
+            int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
+            argmax_combine(bv, bi, v2, i2);
+          }
+          // factors of this thread's rows (column kk, from the group's owner lane)
+          cplx f[RPT];
+#pragma unroll
+          for (int q = 0; q < RPT; ++q) {
+            const double fx = __shfl_sync(0xffffffffu, colv[q].x, grp0 + kk % TPR);
+            const double fy = __shfl_sync(0xffffffffu, colv[q].y, grp0 + kk % TPR);
+            f[q] = cmk(fx, fy);
+          }
+          const int par = kk & 1;
+          cplx* my_cand = cand + (size_t)(par * NWARPS + warp) * WP;
+#pragma unroll
+          for (int q = 0; q < RPT; ++q) {
+            if (r_own + q * rstride == bi) {
+#pragma unroll
+              for (int j = 0; j < CPT; ++j) {
+                const int c = c_own + j * TPR;
+                if (c < w) my_cand[c] = reg[q][j];
+              }
+            }
+          }
+          const int slot = par * NWARPS;
+          if (lane == 0) {
+            red_v[slot + warp] = bv;
+            red_i[slot + warp] = bi;
+          }
+          __syncthreads();  // S: candidates of every warp visible
+          double v = red_v[slot];
+          int p = red_i[slot], pw = 0;
+          for (int q = 1; q < NWARPS; ++q) {
+            const double vq = red_v[slot + q];
+            const int iq = red_i[slot + q];
+            if (vq > v || (vq == v && iq < p)) {
+              v = vq;
+              p = iq;
+              pw = q;
+            }
+          }
+          const cplx* prow = cand + (size_t)(par * NWARPS + pw) * WP;
+          const cplx piv = prow[kk];
+          if (piv.x == 0.0 && piv.y == 0.0 && !zero_pivot) zero_pivot = k + 1;
+          const cplx d = crecip_pivot(piv);
+          if (tid == 0) pivs[kk] = p;
+#pragma unroll
+          for (int q = 0; q < RPT; ++q) {
+            const int r = r_own + q * rstride;
+            if (r >= n) continue;
+            if (r == p) {
+              used[q] = true;
+#pragma unroll
+              for (int j = 0; j < CPT; ++j) {
+                const int c = c_own + j * TPR;
+                if (c < w) reg[q][j] = (c == kk) ? d : cmul(prow[c], d);
+              }
+            } else {
+              const cplx fd = cmul(f[q], d);
+#pragma unroll
+              for (int j = 0; j < CPT; ++j) {
+                const int c = c_own + j * TPR;
+                if (c < w) reg[q][j] = (c == kk) ? cmk(-fd.x, -fd.y) : cfms(fd, prow[c], reg[q][j]);
+              }
+            }
+          }
+        }
+      }
+      // classic row-swap semantics of the panel's pivots: position k0 + kk
+      // receives row pivs[kk], the displaced row goes to the pivot's position
+      if (tid == 0) {
+        for (int kk = 0; kk < w; ++kk) {
+          const int k = k0 + kk, p = pivs[kk];
+          const int qpos = row2pos[p];
+          const int rk = pos2row[k];
           pos2row[k] = p;
           row2pos[p] = k;
           pos2row[qpos] = rk;
           row2pos[rk] = qpos;
           perm[k] = qpos;
-        }
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          const int r = r_own + q * rstride;
-          if (r >= n) continue;
-          if (r == p) {
-#pragma unroll
-            for (int j = 0; j < CPT; ++j) {
-              const int c = c_own + j * TPR;
-              if (c < w) reg[q][j] = (c == kk) ? d : cmul(pbuf[c], d);
-            }
-          } else {
-            const cplx fd = cmul(f[q], d);
-#pragma unroll
-            for (int j = 0; j < CPT; ++j) {
-              const int c = c_own + j * TPR;
-              if (c < w) reg[q][j] = (c == kk) ? cmk(-fd.x, -fd.y) : cfms(fd, pbuf[c], reg[q][j]);
-            }
-          }
         }
       }
       // panel back to shared memory for the update
@@ -397,7 +506,6 @@ __global__ void __launch_bounds__(THREADS, 1)
         X[(int64_t)i * ldx + k0 + c] = P[pidx(pos2row[i], c, WP)];
       }
       // rows are now in the new order: the pivot rows so far sit at positions < k0 + w
-      for (int r = tid; r < n; r += THREADS) s_rowflag[r] = (r < k0 + w) ? 1 : 0;
       __syncthreads();
     }
 
