@@ -34,9 +34,14 @@
  *    contiguous slice of that row (src/qttools/datastructures/dsdbcoo.py:285-319).
  *    qtx_btd_desc describes, for each of the 3*nb-2 blocks, where its slice
  *    starts and how its entries map into the dense block.
- *  - All data pointers are DEVICE pointers unless QTX_FLAG_HOST_BUFFERS is set,
- *    in which case they are host pointers (pinned memory is fastest) and the
- *    library streams the energy batches through the device itself.
+ *  - All data pointers are DEVICE pointers unless QTX_FLAG_HOST_BUFFERS is set
+ *    (qtx_selected_inv / qtx_selected_solve): then the data rows, the OBC
+ *    blocks and the current are HOST pointers (the block_index arrays of a
+ *    qtx_btd_desc stay device pointers) and the library streams the stack
+ *    through the device in energy batches: two device staging sets, uploads
+ *    and downloads on a copy stream overlapping the solve, the host ranges
+ *    page-locked for the call when the driver allows; the call returns when
+ *    every output is back in host memory.
  *  - Nothing is synchronous unless stated: work is enqueued on `stream`.
  *  - No exception crosses the ABI; every call returns a qtx_status and the
  *    context keeps a text message (qtx_last_error).

@@ -1084,9 +1084,144 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
 }
 
 // ---------------------------------------------------------------------------
-// host-buffer streaming for qtx_selected_solve (QTX_FLAG_HOST_BUFFERS)
+// host-buffer streaming for qtx_selected_inv / qtx_selected_solve
+// (QTX_FLAG_HOST_BUFFERS)
 // ---------------------------------------------------------------------------
+// The stack is processed in energy batches: the batch's rows of every array
+// are copied into one of two device staging sets on a copy stream, solved on
+// the caller's stream and copied back on the copy stream, so that the upload
+// of batch q + 1 and the download of batch q - 1 overlap the solve of batch q
+// (when the host arrays are page-locked: the library page-locks them for the
+// call when it can).  Device memory is bounded by two staging sets and the
+// solver's own work space of one batch, whatever the stack size.
 size_t desc_row_bytes(const qtx_btd_desc* d) { return sizeof(cplx) * (size_t)d->stack_stride; }
+
+// Page-locks a host range for the duration of a call (no-op if it already is
+// or if the driver refuses).
+struct HostPin {
+  void* p = nullptr;
+  HostPin() = default;
+  HostPin(const void* ptr, size_t bytes) {
+    if (!ptr || !bytes) return;
+    if (cudaHostRegister(const_cast<void*>(ptr), bytes, cudaHostRegisterDefault) == cudaSuccess) p = const_cast<void*>(ptr);
+    else cudaGetLastError();
+  }
+  HostPin(const HostPin&) = delete;
+  HostPin& operator=(const HostPin&) = delete;
+  HostPin(HostPin&& o) noexcept : p(o.p) { o.p = nullptr; }
+  ~HostPin() {
+    if (p) cudaHostUnregister(p);
+  }
+};
+
+// One host array of the call: rows of `row_bytes`, `rows` of them.
+struct HostArr {
+  const char* h = nullptr;  // host base
+  char* hw = nullptr;       // writable host base (outputs)
+  size_t row_bytes = 0;
+  bool in = false, out = false;
+  char* dev[2] = {nullptr, nullptr};
+};
+
+// Energies per streamed batch: two staging sets plus the solver's work space
+// (about (3 nb + 20) bmax^2 complex per energy) in 70 % of the free memory.
+int64_t host_batch(int64_t max_batch, int64_t NE, size_t staging_per_energy, int nb, int bmax) {
+  size_t free_b = 0, total_b = 0;
+  QTX_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  const size_t ws = sizeof(cplx) * (size_t)(3 * nb + 20) * bmax * bmax;
+  const size_t per = 2 * staging_per_energy + ws;
+  int64_t ne = (int64_t)((double)free_b * 0.7 / (double)std::max<size_t>(per, 1));
+  ne = std::max<int64_t>(1, std::min<int64_t>({ne, max_batch, NE}));
+  return ne;
+}
+
+// Streams `solve(e0, ne, set)` over the stack.  `arrs` are the per-energy
+// arrays (inputs copied up, outputs copied down; outputs are also copied up so
+// that entries the solver does not write keep their values).
+template <typename F>
+void stream_host_batches(std::vector<HostArr>& arrs, int64_t NE, int64_t ne_b, cudaStream_t s, F&& solve) {
+  size_t per_set = 0;
+  for (auto& a : arrs) per_set += ((a.row_bytes * ne_b + 255) / 256) * 256;
+  DevBuf staging(2 * per_set, s);
+  for (int set = 0; set < 2; ++set) {
+    char* cur = staging.as<char>() + set * per_set;
+    for (auto& a : arrs) {
+      a.dev[set] = cur;
+      cur += ((a.row_bytes * ne_b + 255) / 256) * 256;
+    }
+  }
+  std::vector<HostPin> pins;
+  for (auto& a : arrs) pins.emplace_back(a.out ? a.hw : a.h, a.row_bytes * NE);
+  cudaStream_t cs = nullptr;
+  QTX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaEvent_t up[2] = {nullptr, nullptr}, solved = nullptr;
+  auto cleanup = [&] {
+    cudaStreamSynchronize(cs);
+    for (auto& e : up)
+      if (e) cudaEventDestroy(e);
+    if (solved) cudaEventDestroy(solved);
+    cudaStreamDestroy(cs);
+  };
+  try {
+    QTX_CUDA_TRY(cudaEventCreateWithFlags(&up[0], cudaEventDisableTiming));
+    QTX_CUDA_TRY(cudaEventCreateWithFlags(&up[1], cudaEventDisableTiming));
+    QTX_CUDA_TRY(cudaEventCreateWithFlags(&solved, cudaEventDisableTiming));
+    // the staging memory was allocated on s: the copy stream starts after it
+    QTX_CUDA_TRY(cudaEventRecord(solved, s));
+    QTX_CUDA_TRY(cudaStreamWaitEvent(cs, solved, 0));
+    auto upload = [&](int64_t e0, int64_t ne, int set) {
+      for (auto& a : arrs)
+        if (a.in || a.out)
+          QTX_CUDA_TRY(cudaMemcpyAsync(a.dev[set], (a.out ? a.hw : a.h) + e0 * a.row_bytes, ne * a.row_bytes,
+                                       cudaMemcpyHostToDevice, cs));
+      QTX_CUDA_TRY(cudaEventRecord(up[set], cs));
+    };
+    const int64_t nbatch = (NE + ne_b - 1) / ne_b;
+    if (nbatch > 0) upload(0, std::min(ne_b, NE), 0);
+    for (int64_t q = 0; q < nbatch; ++q) {
+      const int set = (int)(q & 1);
+      const int64_t e0 = q * ne_b, ne = std::min(ne_b, NE - e0);
+      // the next batch's upload is queued behind this set's previous download
+      if (q + 1 < nbatch) upload(e0 + ne_b, std::min(ne_b, NE - e0 - ne_b), set ^ 1);
+      QTX_CUDA_TRY(cudaStreamWaitEvent(s, up[set], 0));
+      solve(e0, ne, set);  // ends with a synchronisation of s
+      QTX_CUDA_TRY(cudaEventRecord(solved, s));
+      QTX_CUDA_TRY(cudaStreamWaitEvent(cs, solved, 0));
+      for (auto& a : arrs)
+        if (a.out)
+          QTX_CUDA_TRY(cudaMemcpyAsync(a.hw + e0 * a.row_bytes, a.dev[set], ne * a.row_bytes,
+                                       cudaMemcpyDeviceToHost, cs));
+    }
+    QTX_CUDA_TRY(cudaStreamSynchronize(cs));
+  } catch (...) {
+    cleanup();
+    throw;
+  }
+  cleanup();
+  // staging is freed on s after everything queued on it
+}
+
+// qtx_btd_desc of one streamed batch: the same blocks, ne rows
+qtx_btd_desc batch_desc(const qtx_btd_desc* d, int64_t ne) {
+  qtx_btd_desc b = *d;
+  b.stack_size = ne;
+  return b;
+}
+
+// per-block OBC arrays (host pointers, (stack, b_i, b_i)) as streamed arrays
+void add_obc_arrays(std::vector<HostArr>& arrs, const void* const* obc, const qtx_btd_desc* d,
+                    std::vector<int>& which) {
+  if (!obc) return;
+  for (int i = 0; i < d->num_blocks; ++i) {
+    if (!obc[i]) continue;
+    HostArr a;
+    a.h = reinterpret_cast<const char*>(obc[i]);
+    a.row_bytes = sizeof(cplx) * (size_t)d->block_sizes[i] * d->block_sizes[i];
+    a.in = true;
+    which.push_back(i);
+    arrs.push_back(a);
+  }
+}
 
 template <typename F>
 qtx_status guarded(qtx_ctx* ctx, F&& f) {
@@ -1264,11 +1399,37 @@ qtx_status qtx_selected_inv(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const void
     validate_desc(out_desc, "out");
     check_same_blocks(a_desc, out_desc, "out");
     if (!a || !out) throw QtxError(QTX_E_INVAL, "qtx_selected_inv: null data");
-    if (flags & QTX_FLAG_HOST_BUFFERS) throw QtxError(QTX_E_UNSUPPORTED, "qtx_selected_inv: host buffers");
     if (max_batch_size < 1) throw QtxError(QTX_E_INVAL, "qtx_selected_inv: max_batch_size < 1");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (flags & QTX_FLAG_HOST_BUFFERS) {
+      const int nb = a_desc->num_blocks;
+      const int bmax = *std::max_element(a_desc->block_sizes, a_desc->block_sizes + nb);
+      std::vector<HostArr> arrs(2);
+      arrs[0].h = reinterpret_cast<const char*>(a);
+      arrs[0].row_bytes = desc_row_bytes(a_desc);
+      arrs[0].in = true;
+      arrs[1].hw = reinterpret_cast<char*>(out);
+      arrs[1].row_bytes = desc_row_bytes(out_desc);
+      arrs[1].out = true;
+      std::vector<int> obc_i;
+      add_obc_arrays(arrs, obc_retarded, a_desc, obc_i);
+      size_t per_e = 0;
+      for (auto& x : arrs) per_e += x.row_bytes;
+      const int64_t NE = a_desc->stack_size;
+      const int64_t ne_b = host_batch(max_batch_size, NE, per_e, nb, bmax);
+      stream_host_batches(arrs, NE, ne_b, s, [&](int64_t, int64_t ne, int set) {
+        qtx_btd_desc ad = batch_desc(a_desc, ne), od = batch_desc(out_desc, ne);
+        std::vector<const void*> obc(nb, nullptr);
+        for (size_t q = 0; q < obc_i.size(); ++q) obc[obc_i[q]] = arrs[2 + q].dev[set];
+        Btd A{&ad, reinterpret_cast<cplx*>(arrs[0].dev[set])};
+        Btd O{&od, reinterpret_cast<cplx*>(arrs[1].dev[set])};
+        selected_inv_impl(ctx, A, obc_retarded ? obc.data() : nullptr, O, ne, precision, s);
+      });
+      return;
+    }
     Btd A{a_desc, const_cast<cplx*>(reinterpret_cast<const cplx*>(a))};
     Btd O{out_desc, reinterpret_cast<cplx*>(out)};
-    selected_inv_impl(ctx, A, obc_retarded, O, max_batch_size, precision, reinterpret_cast<cudaStream_t>(stream));
+    selected_inv_impl(ctx, A, obc_retarded, O, max_batch_size, precision, s);
   });
 }
 
@@ -1299,7 +1460,74 @@ qtx_status qtx_selected_solve(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const vo
     if (!a || !sigma_lesser || !sigma_greater || !xl || !xg)
       throw QtxError(QTX_E_INVAL, "qtx_selected_solve: null data");
     if (max_batch_size < 1) throw QtxError(QTX_E_INVAL, "qtx_selected_solve: max_batch_size < 1");
-    if (flags & QTX_FLAG_HOST_BUFFERS) throw QtxError(QTX_E_UNSUPPORTED, "qtx_selected_solve: host buffers");
+    if (flags & QTX_FLAG_HOST_BUFFERS) {
+      cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+      const int nb = a_desc->num_blocks;
+      const int bmax = *std::max_element(a_desc->block_sizes, a_desc->block_sizes + nb);
+      const bool want_xr = xr_desc && xr;
+      const bool want_cur = (flags & QTX_FLAG_RETURN_CURRENT) != 0;
+      std::vector<HostArr> arrs;
+      auto add = [&](const qtx_btd_desc* d, const void* p, bool is_out) {
+        HostArr h;
+        h.row_bytes = desc_row_bytes(d);
+        if (is_out) {
+          h.hw = reinterpret_cast<char*>(const_cast<void*>(p));
+          h.out = true;
+        } else {
+          h.h = reinterpret_cast<const char*>(p);
+          h.in = true;
+        }
+        arrs.push_back(h);
+      };
+      add(a_desc, a, false);
+      add(sl_desc, sigma_lesser, false);
+      add(sg_desc, sigma_greater, false);
+      add(xl_desc, xl, true);
+      add(xg_desc, xg, true);
+      if (want_xr) add(xr_desc, xr, true);
+      if (want_cur) {
+        HostArr h;
+        h.hw = reinterpret_cast<char*>(current);
+        h.row_bytes = sizeof(cplx) * (size_t)(nb - 1);
+        h.out = true;
+        arrs.push_back(h);
+      }
+      const size_t first_obc = arrs.size();
+      std::vector<int> oi_r, oi_l, oi_g;
+      add_obc_arrays(arrs, obc ? obc->retarded : nullptr, a_desc, oi_r);
+      add_obc_arrays(arrs, obc ? obc->lesser : nullptr, a_desc, oi_l);
+      add_obc_arrays(arrs, obc ? obc->greater : nullptr, a_desc, oi_g);
+      size_t per_e = 0;
+      for (auto& x : arrs) per_e += x.row_bytes;
+      const int64_t NE = a_desc->stack_size;
+      const int64_t ne_b = host_batch(max_batch_size, NE, per_e, nb, bmax);
+      stream_host_batches(arrs, NE, ne_b, s, [&](int64_t, int64_t ne, int set) {
+        qtx_btd_desc ad = batch_desc(a_desc, ne), sld = batch_desc(sl_desc, ne), sgd = batch_desc(sg_desc, ne);
+        qtx_btd_desc xld = batch_desc(xl_desc, ne), xgd = batch_desc(xg_desc, ne);
+        qtx_btd_desc xrd = want_xr ? batch_desc(xr_desc, ne) : qtx_btd_desc{};
+        std::vector<const void*> r(nb, nullptr), l(nb, nullptr), g(nb, nullptr);
+        size_t q = first_obc;
+        for (int i : oi_r) r[i] = arrs[q++].dev[set];
+        for (int i : oi_l) l[i] = arrs[q++].dev[set];
+        for (int i : oi_g) g[i] = arrs[q++].dev[set];
+        qtx_obc ob{oi_r.empty() ? nullptr : r.data(), oi_l.empty() ? nullptr : l.data(),
+                   oi_g.empty() ? nullptr : g.data()};
+        SolveArgs S;
+        S.a = Btd{&ad, reinterpret_cast<cplx*>(arrs[0].dev[set])};
+        S.sl = Btd{&sld, reinterpret_cast<cplx*>(arrs[1].dev[set])};
+        S.sg = Btd{&sgd, reinterpret_cast<cplx*>(arrs[2].dev[set])};
+        S.xl = Btd{&xld, reinterpret_cast<cplx*>(arrs[3].dev[set])};
+        S.xg = Btd{&xgd, reinterpret_cast<cplx*>(arrs[4].dev[set])};
+        S.xr = want_xr ? Btd{&xrd, reinterpret_cast<cplx*>(arrs[5].dev[set])} : Btd{};
+        S.obc = obc ? &ob : nullptr;
+        S.current = want_cur ? reinterpret_cast<cplx*>(arrs[want_xr ? 6 : 5].dev[set]) : nullptr;
+        S.flags = flags & ~QTX_FLAG_HOST_BUFFERS;
+        S.max_batch = ne;
+        S.precision = precision;
+        selected_solve_impl(ctx, S, s);
+      });
+      return;
+    }
     SolveArgs S;
     S.a = Btd{a_desc, const_cast<cplx*>(reinterpret_cast<const cplx*>(a))};
     S.sl = Btd{sl_desc, const_cast<cplx*>(reinterpret_cast<const cplx*>(sigma_lesser))};

@@ -3,9 +3,13 @@
 Mirrors ``src/qttools/greens_function_solver/solver.py`` (``OBCBlocks``
 ``:12-28``, ``GFSolver`` ``:31-113``) and ``rgf.py`` (``RGF`` ``:10-414``):
 same class names, method signatures, argument meaning, return conventions and
-errors.  Every call runs on the current CUDA device through the C ABI; host
-(NumPy) matrices are copied to the device and the outputs copied back.  There
-is no CPU path: without the built library or a CUDA device the calls raise.
+errors.  Every call runs on the current CUDA device through the C ABI.  When every
+operand is a host (NumPy) array the library streams the stack through the
+device in energy batches (``QTX_FLAG_HOST_BUFFERS``: two device staging sets,
+uploads and downloads overlapping the solve), so stacks larger than the
+device memory work; mixed host/device operands are staged through the device
+whole.  There is no CPU path: without the built library or a CUDA device the
+calls raise.
 
 Behaviour notes (upstream file:line):
 
@@ -69,14 +73,37 @@ def _device_index() -> int:
     return torch.cuda.current_device()
 
 
-class _Operand:
-    """A DSDBSparse-like matrix staged for one C call."""
+def _is_host(x) -> bool:
+    if x is None:
+        return True
+    if isinstance(x, torch.Tensor):
+        return not x.is_cuda
+    return True
 
-    def __init__(self, m, device: int, writable: bool):
+
+class _Operand:
+    """A DSDBSparse-like matrix staged for one C call (``host``: passed as a
+    host pointer for the streamed host-buffer mode)."""
+
+    def __init__(self, m, device: int, writable: bool, host: bool = False):
         self.m = m
         self.layout = layout_of(m)
         data = m.data
         self.host_array = None
+        self.host = host
+        if host:
+            arr = data.numpy() if isinstance(data, torch.Tensor) else np.asarray(data)
+            if arr.dtype != np.complex128:
+                raise TypeError("DSDBSparse data must be complex128")
+            self.host_array = arr
+            self.h = np.ascontiguousarray(arr)  # the caller's array itself when contiguous
+            self.orig = data
+            self.writable = writable
+            self.stack_shape = tuple(self.h.shape[:-1])
+            self.stack_size = int(math.prod(self.stack_shape)) if self.stack_shape else 1
+            self.nnz = int(self.h.shape[-1])
+            self.desc, self.keep = self.layout.desc(self.stack_size, self.nnz, device)
+            return
         if isinstance(data, torch.Tensor):
             if data.dtype != torch.complex128:
                 raise TypeError("DSDBSparse data must be complex128")
@@ -99,10 +126,14 @@ class _Operand:
 
     @property
     def ptr(self) -> int:
-        return self.t.data_ptr()
+        return self.h.ctypes.data if self.host else self.t.data_ptr()
 
     def write_back(self) -> None:
         if not self.writable:
+            return
+        if self.host:
+            if self.h is not self.host_array:
+                self.host_array[...] = self.h.reshape(self.host_array.shape)
             return
         if self.host_array is not None:
             self.host_array[...] = self.t.cpu().numpy().reshape(self.host_array.shape)
@@ -110,7 +141,7 @@ class _Operand:
             self.orig.copy_(self.t)
 
 
-def _obc_ptrs(blocks, nb: int, stack_size: int, device: int, keep: list):
+def _obc_ptrs(blocks, nb: int, stack_size: int, device: int, keep: list, host: bool = False):
     if blocks is None or all(b is None for b in blocks):
         return None
     if len(blocks) != nb:
@@ -119,6 +150,14 @@ def _obc_ptrs(blocks, nb: int, stack_size: int, device: int, keep: list):
     for b in blocks:
         if b is None:
             ptrs.append(0)
+            continue
+        if host:
+            h = np.ascontiguousarray(b.numpy() if isinstance(b, torch.Tensor) else np.asarray(b),
+                                     dtype=np.complex128)
+            if h.size // (h.shape[-1] * h.shape[-2]) != stack_size:
+                raise ValueError("OBC block stack size differs from the system matrix")
+            keep.append(h)
+            ptrs.append(h.ctypes.data)
             continue
         t = b if isinstance(b, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(np.asarray(b)))
         t = t.to(device=f"cuda:{device}", dtype=torch.complex128).contiguous()
@@ -166,12 +205,14 @@ class RGF(GFSolver):
         if obc_blocks is None:
             obc_blocks = OBCBlocks(num_blocks=a.num_blocks)
         x = out if out is not None else _zeros_like(a)
-        A = _Operand(a, dev, writable=False)
-        X = _Operand(x, dev, writable=True)
+        host = all(_is_host(m.data) for m in (a, x)) and all(_is_host(b) for b in obc_blocks.retarded)
+        A = _Operand(a, dev, writable=False, host=host)
+        X = _Operand(x, dev, writable=True, host=host)
         keep: list = []
-        obc_r = _obc_ptrs(obc_blocks.retarded, a.num_blocks, A.stack_size, dev, keep)
+        obc_r = _obc_ptrs(obc_blocks.retarded, a.num_blocks, A.stack_size, dev, keep, host)
+        flags = _lib.QTX_FLAG_HOST_BUFFERS if host else 0
         st = lib.qtx_selected_inv(ctx, ctypes.byref(A.desc), A.ptr, obc_r, ctypes.byref(X.desc), X.ptr,
-                                  self._batch(A), _PRECISIONS[self.precision], 0, _stream())
+                                  self._batch(A), _PRECISIONS[self.precision], flags, _stream())
         _lib.check(st, ctx, "RGF.selected_inv")
         X.write_back()
         if out is None:
@@ -199,19 +240,22 @@ class RGF(GFSolver):
             xl = _zeros_like(a)
             xg = _zeros_like(a)
             xr = _zeros_like(a) if return_retarded else None
-        A = _Operand(a, dev, writable=False)
-        SL = _Operand(sigma_lesser, dev, writable=False)
-        SG = _Operand(sigma_greater, dev, writable=False)
-        XL = _Operand(xl, dev, writable=True)
-        XG = _Operand(xg, dev, writable=True)
-        XR = _Operand(xr, dev, writable=True) if xr is not None else None
+        mats = [a, sigma_lesser, sigma_greater, xl, xg] + ([xr] if xr is not None else [])
+        host = all(_is_host(m.data) for m in mats) and all(
+            _is_host(b) for blocks in (obc_blocks.retarded, obc_blocks.lesser, obc_blocks.greater) for b in blocks)
+        A = _Operand(a, dev, writable=False, host=host)
+        SL = _Operand(sigma_lesser, dev, writable=False, host=host)
+        SG = _Operand(sigma_greater, dev, writable=False, host=host)
+        XL = _Operand(xl, dev, writable=True, host=host)
+        XG = _Operand(xg, dev, writable=True, host=host)
+        XR = _Operand(xr, dev, writable=True, host=host) if xr is not None else None
         keep: list = []
         obc = _lib.Obc(
-            retarded=_obc_ptrs(obc_blocks.retarded, nb, A.stack_size, dev, keep),
-            lesser=_obc_ptrs(obc_blocks.lesser, nb, A.stack_size, dev, keep),
-            greater=_obc_ptrs(obc_blocks.greater, nb, A.stack_size, dev, keep),
+            retarded=_obc_ptrs(obc_blocks.retarded, nb, A.stack_size, dev, keep, host),
+            lesser=_obc_ptrs(obc_blocks.lesser, nb, A.stack_size, dev, keep, host),
+            greater=_obc_ptrs(obc_blocks.greater, nb, A.stack_size, dev, keep, host),
         )
-        flags = 0
+        flags = _lib.QTX_FLAG_HOST_BUFFERS if host else 0
         if return_retarded:
             flags |= _lib.QTX_FLAG_RETURN_RETARDED
         if getattr(xl, "symmetry", False):
@@ -219,18 +263,23 @@ class RGF(GFSolver):
         current = None
         if return_current:
             flags |= _lib.QTX_FLAG_RETURN_CURRENT
-            current = torch.zeros(A.stack_shape + (nb - 1,), dtype=torch.complex128, device=f"cuda:{dev}")
+            if host:
+                current = np.zeros(A.stack_shape + (nb - 1,), dtype=np.complex128)
+            else:
+                current = torch.zeros(A.stack_shape + (nb - 1,), dtype=torch.complex128, device=f"cuda:{dev}")
+        cur_ptr = None
+        if current is not None:
+            cur_ptr = current.ctypes.data if host else current.data_ptr()
         st = lib.qtx_selected_solve(
             ctx, ctypes.byref(A.desc), A.ptr, ctypes.byref(SL.desc), SL.ptr, ctypes.byref(SG.desc), SG.ptr,
             ctypes.byref(obc), ctypes.byref(XL.desc), XL.ptr, ctypes.byref(XG.desc), XG.ptr,
             ctypes.byref(XR.desc) if XR else None, XR.ptr if XR else None,
-            current.data_ptr() if current is not None else None, self._batch(A), _PRECISIONS[self.precision],
-            flags, _stream())
+            cur_ptr, self._batch(A), _PRECISIONS[self.precision], flags, _stream())
         _lib.check(st, ctx, "RGF.selected_solve")
         for op in (XL, XG, XR):
             if op is not None:
                 op.write_back()
-        if current is not None and A.host_array is not None:
+        if current is not None and not host and A.host_array is not None:
             current = current.cpu().numpy()
         if out is None:
             if return_retarded:
