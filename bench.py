@@ -477,13 +477,79 @@ def run_serve(args):
     return 0
 
 
+def run_dropin(args):
+    """Drop-in plugin path: RGF.selected_solve (return_retarded) on DSDBCOO
+    matrices of the seeded device, once with NumPy (host) data -- streamed
+    through the device by QTX_FLAG_HOST_BUFFERS, host<->device copies inside
+    the timed region -- and once with device-resident data."""
+    import torch
+
+    from quatrex_b200.datastructures import DSDBCOO
+    from quatrex_b200.greens_function_solver import RGF, OBCBlocks
+    from quatrex_b200.obc import SanchoRubio, contact_self_energies
+    from quatrex_b200.workloads import make_device
+
+    nb, b, ne = args.dropin_blocks, args.dropin_block_size, args.dropin_energies
+    dev = make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=1234)
+    d, u, lo = dev.system_blocks()
+    A = DSDBCOO.from_blocks(d, u, lo)
+    Z = DSDBCOO.zeros_like(A)
+    e = dev.energies
+    sr = SanchoRubio(dev.sr_max_iter, dev.sr_tol)
+    g_left = sr(d[0], u[0], lo[0])
+    g_right = sr(d[-1], lo[-1], u[-1])
+    f_left = 1.0 / (1.0 + np.exp((e - dev.mu_left) / dev.kt))
+    f_right = 1.0 / (1.0 + np.exp((e - dev.mu_right) / dev.kt))
+    sig_l = contact_self_energies(g_left, lo[0], u[0], f_left)
+    sig_r = contact_self_energies(g_right, u[-1], lo[-1], f_right)
+    ob = OBCBlocks(nb)
+    ob.retarded[0], ob.lesser[0], ob.greater[0] = sig_l
+    ob.retarded[-1], ob.lesser[-1], ob.greater[-1] = sig_r
+    solver = RGF(max_batch_size=args.dropin_batch)
+    lines = {}
+    for where in ("host", "device"):
+        if where == "host":
+            a_, z_, obc = A, Z, ob
+        else:
+            a_, z_ = A.to("cuda"), Z.to("cuda")
+            obc = OBCBlocks(nb)
+            for lst_in, lst_out in ((ob.retarded, obc.retarded), (ob.lesser, obc.lesser), (ob.greater, obc.greater)):
+                for i, x in enumerate(lst_in):
+                    lst_out[i] = None if x is None else torch.from_numpy(x).cuda()
+        outs = [DSDBCOO.zeros_like(a_) for _ in range(3)]
+        for _ in range(args.warmup):
+            solver.selected_solve(a_, z_, z_, obc_blocks=obc, out=outs, return_retarded=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            solver.selected_solve(a_, z_, z_, obc_blocks=obc, out=outs, return_retarded=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        lines[where] = ne * args.steps / dt
+    row_bytes = A.data.shape[-1] * 16
+    print(json.dumps({
+        "metric": "rgf_energy_solves_per_s", "impl": "ours", "workload": "dropin_selected_solve",
+        "value": lines["device"], "unit": "solves/s",
+        "e2e": {"value": lines["host"], "unit": "solves/s", "h2d_bytes_per_step": int(6 * ne * row_bytes),
+                "d2h_bytes_per_step": int(3 * ne * row_bytes),
+                "path": "NumPy DSDBCOO -> QTX_FLAG_HOST_BUFFERS (streamed batches)"},
+        "config": {"num_blocks": nb, "block_size": b, "energies": ne, "max_batch_size": args.dropin_batch,
+                   "outputs": "G^<, G^> (all BTD blocks), G^R diagonal", "steps": args.steps},
+    }), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["large", "small", "uneven", "serve"], default="large")
+    ap.add_argument("--workload", choices=["large", "small", "uneven", "serve", "dropin"], default="large")
+    ap.add_argument("--dropin-blocks", type=int, default=16)
+    ap.add_argument("--dropin-block-size", type=int, default=64)
+    ap.add_argument("--dropin-energies", type=int, default=32)
+    ap.add_argument("--dropin-batch", type=int, default=32)
     ap.add_argument("--instances", type=int, default=8, help="uneven workload: number of instances")
     ap.add_argument("--streams", type=int, default=4, help="uneven/serve: concurrent streams (slots)")
     ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
@@ -502,6 +568,8 @@ def main():
         return run_uneven(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "dropin":
+        return run_dropin(args)
     return run_ours(args)
 
 

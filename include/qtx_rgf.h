@@ -39,9 +39,9 @@
  *    blocks and the current are HOST pointers (the block_index arrays of a
  *    qtx_btd_desc stay device pointers) and the library streams the stack
  *    through the device in energy batches: two device staging sets, uploads
- *    and downloads on a copy stream overlapping the solve, the host ranges
- *    page-locked for the call when the driver allows; the call returns when
- *    every output is back in host memory.
+ *    and downloads on a copy stream overlapping the solve when the host
+ *    arrays are page-locked by the caller; the call returns when every output
+ *    is back in host memory.
  *  - Nothing is synchronous unless stated: work is enqueued on `stream`.
  *  - No exception crosses the ABI; every call returns a qtx_status and the
  *    context keeps a text message (qtx_last_error).

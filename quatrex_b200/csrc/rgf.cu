@@ -1091,28 +1091,12 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
 // are copied into one of two device staging sets on a copy stream, solved on
 // the caller's stream and copied back on the copy stream, so that the upload
 // of batch q + 1 and the download of batch q - 1 overlap the solve of batch q
-// (when the host arrays are page-locked: the library page-locks them for the
-// call when it can).  Device memory is bounded by two staging sets and the
-// solver's own work space of one batch, whatever the stack size.
+// when the caller's arrays are page-locked.  From pageable arrays the driver
+// stages every copy and the host waits for it; page-locking them inside the
+// call was measured slower than that (4.6 vs 5.2 solves/s at nb = 64,
+// b = 256), so the library does not.  Device memory is bounded by two staging
+// sets and the solver's own work space of one batch, whatever the stack size.
 size_t desc_row_bytes(const qtx_btd_desc* d) { return sizeof(cplx) * (size_t)d->stack_stride; }
-
-// Page-locks a host range for the duration of a call (no-op if it already is
-// or if the driver refuses).
-struct HostPin {
-  void* p = nullptr;
-  HostPin() = default;
-  HostPin(const void* ptr, size_t bytes) {
-    if (!ptr || !bytes) return;
-    if (cudaHostRegister(const_cast<void*>(ptr), bytes, cudaHostRegisterDefault) == cudaSuccess) p = const_cast<void*>(ptr);
-    else cudaGetLastError();
-  }
-  HostPin(const HostPin&) = delete;
-  HostPin& operator=(const HostPin&) = delete;
-  HostPin(HostPin&& o) noexcept : p(o.p) { o.p = nullptr; }
-  ~HostPin() {
-    if (p) cudaHostUnregister(p);
-  }
-};
 
 // One host array of the call: rows of `row_bytes`, `rows` of them.
 struct HostArr {
@@ -1150,8 +1134,6 @@ void stream_host_batches(std::vector<HostArr>& arrs, int64_t NE, int64_t ne_b, c
       cur += ((a.row_bytes * ne_b + 255) / 256) * 256;
     }
   }
-  std::vector<HostPin> pins;
-  for (auto& a : arrs) pins.emplace_back(a.out ? a.hw : a.h, a.row_bytes * NE);
   cudaStream_t cs = nullptr;
   QTX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   cudaEvent_t up[2] = {nullptr, nullptr}, solved = nullptr;
