@@ -231,6 +231,19 @@ typedef struct qtx_transport_outputs {
 qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,
                                int32_t precision, uint32_t flags, qtx_stream stream);
 
+/* Block-sorting permutation of a COO pattern on the device (DSDBCOO
+ * construction, <- compute_block_sort_index,
+ * src/qttools/kernels/datastructure/cupy/dsdbcoo.py:234-298): rows, cols
+ * (device int64, nnz entries, global indices) are assigned to the blocks of
+ * block_sizes (host [num_blocks]); sort_index (device int64, nnz) receives the
+ * stable permutation that orders the entries by block row, then block column
+ * (original order kept within a block), block_nnz (host int64 [nb * nb],
+ * row-major over (i, j)) the entries of each block.  An index outside the
+ * matrix gives QTX_E_INVAL.  num_blocks <= 4096.  Synchronous. */
+qtx_status qtx_block_sort_index(qtx_ctx* ctx, int64_t nnz, const int64_t* rows, const int64_t* cols,
+                                int32_t num_blocks, const int32_t* block_sizes, int64_t* sort_index,
+                                int64_t* block_nnz, qtx_stream stream);
+
 /* Device bytes one qtx_transport_solve call allocates for itself (recursion
  * state, couplings, Sancho-Rubio and, for QTX_PREC_MIXED, the slice buffers)
  * when it processes `energies_per_call` energies at a time; H and the outputs

@@ -126,6 +126,36 @@ def block_sort_index(rows: np.ndarray, cols: np.ndarray, block_sizes) -> np.ndar
     return np.lexsort((bc, br)).astype(np.int64)
 
 
+def block_sort_index_device(rows, cols, block_sizes, device=None):
+    """The same permutation as ``block_sort_index``, computed on the device
+    (``qtx_block_sort_index``: block keys by binary search, stable radix sort);
+    returns (sort_index as a device int64 tensor, per-block counts as a host
+    (nb, nb) int64 array).  Raises ValueError for an index outside the matrix."""
+    import ctypes
+
+    from quatrex_b200 import _lib
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("quatrex_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
+    dev = torch.cuda.current_device() if device is None else torch.device(device).index or 0
+    r = torch.as_tensor(rows, dtype=torch.int64).to(f"cuda:{dev}").contiguous()
+    c = torch.as_tensor(cols, dtype=torch.int64).to(f"cuda:{dev}").contiguous()
+    sizes = np.ascontiguousarray(np.asarray(block_sizes), dtype=np.int32)
+    nb = len(sizes)
+    out = torch.empty(r.shape[0], dtype=torch.int64, device=f"cuda:{dev}")
+    counts = np.zeros(nb * nb, dtype=np.int64)
+    lib = _lib.load()
+    ctx = _lib.context(dev)
+    st = lib.qtx_block_sort_index(ctx, int(r.shape[0]), r.data_ptr(), c.data_ptr(), nb,
+                                  sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), out.data_ptr(),
+                                  counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                  torch.cuda.current_stream(dev).cuda_stream)
+    if st == _lib.QTX_E_INVAL:
+        raise ValueError("qtx_block_sort_index: an index lies outside the matrix (or bad block sizes)")
+    _lib.check(st, ctx, "qtx_block_sort_index")
+    return out, counts.reshape(nb, nb)
+
+
 class _BlockIndexer:
     def __init__(self, m: "DSDBCOO"):
         self.m = m
@@ -195,6 +225,13 @@ class DSDBCOO:
         if symmetry:
             coo = sparse.triu(coo, format="coo")
         coo.sum_duplicates()
+        if device is not None and torch.device(device).type == "cuda":
+            # block sorting and the broadcast over the stack on the device
+            order, _ = block_sort_index_device(coo.row, coo.col, block_sizes, device)
+            order_h = order.cpu().numpy()
+            vals = torch.as_tensor(coo.data.astype(np.complex128)).to(order.device)[order]
+            data = vals.expand(tuple(global_stack_shape) + (vals.shape[0],)).contiguous()
+            return cls(data, coo.row[order_h], coo.col[order_h], block_sizes, global_stack_shape, symmetry)
         order = block_sort_index(coo.row, coo.col, block_sizes)
         rows, cols, vals = coo.row[order], coo.col[order], coo.data[order].astype(np.complex128)
         data = np.broadcast_to(vals, tuple(global_stack_shape) + (len(vals),)).copy()

@@ -147,3 +147,30 @@ def test_contact_self_energies_match_oracle():
     assert _rel(sr, ref["retarded"][0]) < 1e-12
     assert _rel(sl, ref["lesser"][0]) < 1e-12
     assert _rel(sg, ref["greater"][0]) < 1e-12
+
+
+@pytest.mark.parametrize("sizes", [[3, 5, 4, 6], [8] * 12, [1, 2, 1, 3, 2]])
+def test_block_sort_index_device_matches_host(sizes):
+    """DSDBCOO construction on the device: the same stable block-sorting
+    permutation as the host rule (and upstream's compute_block_sort_index),
+    per-block counts, and an index outside the matrix refused."""
+    from quatrex_b200.datastructures import block_sort_index, block_sort_index_device
+
+    rng = np.random.default_rng(len(sizes))
+    n = int(np.sum(sizes))
+    # random pattern with entries in every block pair (not only the band), shuffled order
+    m = (rng.random((n, n)) < 0.3).astype(np.complex128)
+    r, c = np.nonzero(m)
+    perm = rng.permutation(len(r))
+    r, c = r[perm], c[perm]
+    got, counts = block_sort_index_device(r, c, sizes)
+    want = block_sort_index(r, c, sizes)
+    assert np.array_equal(got.cpu().numpy(), want)
+    offs = np.concatenate(([0], np.cumsum(sizes)))
+    br = np.searchsorted(offs, r, side="right") - 1
+    bc = np.searchsorted(offs, c, side="right") - 1
+    ref = np.zeros((len(sizes), len(sizes)), dtype=np.int64)
+    np.add.at(ref, (br, bc), 1)
+    assert np.array_equal(counts, ref)
+    with pytest.raises(ValueError):
+        block_sort_index_device(np.array([0, n]), np.array([0, 0]), sizes)
