@@ -244,6 +244,18 @@ qtx_status qtx_block_sort_index(qtx_ctx* ctx, int64_t nnz, const int64_t* rows, 
                                 int32_t num_blocks, const int32_t* block_sizes, int64_t* sort_index,
                                 int64_t* block_nnz, qtx_stream stream);
 
+/* System matrix on DSDBSparse data rows, all operands in one entry order:
+ * a[e, q] = (E_e + i eta) S_q - V_r [q on the diagonal, r its row] - Sigma[e, q] - H_q
+ * (<- ElectronSolver._assemble_system_matrix, src/quatrex/electron/solver.py:388-410,
+ * with _btd_subtract :26-51).  rows, cols: device int64 [nnz] (global indices
+ * of the entries); overlap: device [nnz] or NULL for S = I; potential: device
+ * double [N] or NULL; hamiltonian: device [nnz]; sigma: device
+ * (num_energies, stride_sigma) or NULL; a: device (num_energies, stride_a). */
+qtx_status qtx_assemble_system(qtx_ctx* ctx, int64_t nnz, int64_t num_energies, const double* energies,
+                               double eta, const int64_t* rows, const int64_t* cols, const void* overlap,
+                               const double* potential, const void* hamiltonian, const void* sigma,
+                               int64_t stride_sigma, void* a, int64_t stride_a, qtx_stream stream);
+
 /* Device bytes one qtx_transport_solve call allocates for itself (recursion
  * state, couplings, Sancho-Rubio and, for QTX_PREC_MIXED, the slice buffers)
  * when it processes `energies_per_call` energies at a time; H and the outputs

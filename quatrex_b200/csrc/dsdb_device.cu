@@ -58,6 +58,30 @@ __global__ void __launch_bounds__(KEY_THREADS) block_key_kernel(int64_t nnz, con
   }
 }
 
+// A(E) = (E + i eta) S - diag(V) - Sigma(E) - H on the data rows of one
+// DSDBSparse pattern (all operands in the same entry order); S = I when
+// `overlap` is null (entries with row == col), the potential applies to the
+// diagonal entries.  One thread per (energy, entry), 2-D grid-stride.
+__global__ void assemble_system_kernel(int64_t nnz, int64_t ne, const double* __restrict__ energies, double eta,
+                                       const int64_t* __restrict__ rows, const int64_t* __restrict__ cols,
+                                       const cplx* __restrict__ overlap, const double* __restrict__ potential,
+                                       const cplx* __restrict__ h, const cplx* __restrict__ sigma,
+                                       int64_t stride_sigma, cplx* __restrict__ a, int64_t stride_a) {
+  for (int64_t e = blockIdx.y; e < ne; e += gridDim.y) {
+    const cplx z = cmk(energies[e], eta);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += (int64_t)gridDim.x * blockDim.x) {
+      const bool diag = rows[q] == cols[q];
+      cplx v;
+      if (overlap) v = cmul(z, overlap[q]);
+      else v = diag ? z : cmk(0, 0);
+      if (potential && diag) v.x -= potential[rows[q]];
+      v = csub(v, h[q]);
+      if (sigma) v = csub(v, sigma[e * stride_sigma + q]);
+      a[e * stride_a + q] = v;
+    }
+  }
+}
+
 struct DevMem {
   void* p = nullptr;
   cudaStream_t s = nullptr;
@@ -139,6 +163,31 @@ extern "C" qtx_status qtx_block_sort_index(qtx_ctx* ctx, int64_t nnz, const int6
     QTX_CUDA_TRY(cudaStreamSynchronize(s));
     if (h_bad) return QTX_E_INVAL;
     for (size_t k = 0; k < nkeys; ++k) block_nnz[k] = (int64_t)h_counts[k];
+    return QTX_OK;
+  } catch (const QtxError& e) {
+    return e.code;
+  }
+}
+
+extern "C" qtx_status qtx_assemble_system(qtx_ctx* ctx, int64_t nnz, int64_t num_energies, const double* energies,
+                                          double eta, const int64_t* rows, const int64_t* cols, const void* overlap,
+                                          const double* potential, const void* hamiltonian, const void* sigma,
+                                          int64_t stride_sigma, void* a, int64_t stride_a, qtx_stream stream) {
+  (void)ctx;
+  if (nnz < 0 || num_energies < 0 || (nnz > 0 && num_energies > 0 && (!energies || !rows || !cols || !hamiltonian ||
+                                                                        !a || stride_a < nnz)) ||
+      (sigma && stride_sigma < nnz))
+    return QTX_E_INVAL;
+  if (nnz == 0 || num_energies == 0) return QTX_OK;
+  try {
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const unsigned gx = (unsigned)std::min<int64_t>((nnz + 255) / 256, 148 * 8);
+    const unsigned gy = (unsigned)std::min<int64_t>(num_energies, 65535);
+    assemble_system_kernel<<<dim3(gx, gy), 256, 0, s>>>(
+        nnz, num_energies, energies, eta, rows, cols, reinterpret_cast<const cplx*>(overlap), potential,
+        reinterpret_cast<const cplx*>(hamiltonian), reinterpret_cast<const cplx*>(sigma), stride_sigma,
+        reinterpret_cast<cplx*>(a), stride_a);
+    qtx_check_launch("assemble_system_kernel");
     return QTX_OK;
   } catch (const QtxError& e) {
     return e.code;

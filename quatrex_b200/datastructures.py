@@ -156,6 +156,47 @@ def block_sort_index_device(rows, cols, block_sizes, device=None):
     return out, counts.reshape(nb, nb)
 
 
+def assemble_system(energies, eta: float, hamiltonian: "DSDBCOO", overlap: "DSDBCOO | None" = None,
+                    potential=None, sigma: "DSDBCOO | None" = None) -> "DSDBCOO":
+    """A(E) = (E + i eta) S - diag(V) - Sigma(E) - H on the device for every
+    energy (``ElectronSolver._assemble_system_matrix``,
+    ``src/quatrex/electron/solver.py:388-410``): S = I when ``overlap`` is None;
+    H and S are energy independent (one data row), Sigma has one row per energy;
+    all matrices share the entry order of ``hamiltonian``."""
+    from quatrex_b200 import _lib
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("quatrex_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
+    dev = torch.cuda.current_device()
+    cuda = f"cuda:{dev}"
+
+    def row(m):
+        d = m.data if isinstance(m.data, torch.Tensor) else torch.as_tensor(np.asarray(m.data))
+        return d.to(cuda, dtype=torch.complex128).reshape(-1, d.shape[-1])
+
+    e = torch.as_tensor(np.asarray(energies, dtype=np.float64)).to(cuda).contiguous()
+    ne = int(e.shape[0])
+    h = row(hamiltonian)[0].contiguous()
+    nnz = int(h.shape[0])
+    rows = torch.as_tensor(np.asarray(hamiltonian.rows, dtype=np.int64)).to(cuda)
+    cols = torch.as_tensor(np.asarray(hamiltonian.cols, dtype=np.int64)).to(cuda)
+    s = row(overlap)[0].contiguous() if overlap is not None else None
+    v = torch.as_tensor(np.asarray(potential, dtype=np.float64)).to(cuda) if potential is not None else None
+    sg = row(sigma).contiguous() if sigma is not None else None
+    if sg is not None and sg.shape[0] != ne:
+        raise ValueError("sigma needs one data row per energy")
+    out = torch.empty((ne, nnz), dtype=torch.complex128, device=cuda)
+    lib = _lib.load()
+    ctx = _lib.context(dev)
+    st = lib.qtx_assemble_system(ctx, nnz, ne, e.data_ptr(), float(eta), rows.data_ptr(), cols.data_ptr(),
+                                 s.data_ptr() if s is not None else None, v.data_ptr() if v is not None else None,
+                                 h.data_ptr(), sg.data_ptr() if sg is not None else None, nnz, out.data_ptr(), nnz,
+                                 torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(st, ctx, "qtx_assemble_system")
+    return DSDBCOO(out, hamiltonian.rows, hamiltonian.cols, hamiltonian.block_sizes, (ne,),
+                   getattr(hamiltonian, "symmetry", False))
+
+
 class _BlockIndexer:
     def __init__(self, m: "DSDBCOO"):
         self.m = m

@@ -174,3 +174,34 @@ def test_block_sort_index_device_matches_host(sizes):
     assert np.array_equal(counts, ref)
     with pytest.raises(ValueError):
         block_sort_index_device(np.array([0, n]), np.array([0, 0]), sizes)
+
+
+@pytest.mark.parametrize("with_overlap", [False, True])
+def test_assemble_system_matches_formula(with_overlap):
+    """A(E) = (E + i eta) S - diag(V) - Sigma(E) - H on the data rows."""
+    from scipy import sparse
+
+    from quatrex_b200.datastructures import DSDBCOO, assemble_system
+
+    rng = np.random.default_rng(3)
+    sizes = np.array([3, 4, 3])
+    n = int(sizes.sum())
+    band = np.abs(np.subtract.outer(np.arange(n), np.arange(n))) <= 3
+    hm = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) * band
+    hm = hm + hm.conj().T + np.eye(n)
+    H = DSDBCOO.from_sparray(sparse.coo_matrix(hm), sizes, (1,))
+    S = None
+    sm = np.eye(n)
+    if with_overlap:
+        sm = np.eye(n) + 0.1 * band * rng.standard_normal((n, n))
+        S = DSDBCOO(np.asarray(sm[H.rows, H.cols], dtype=np.complex128)[None], H.rows, H.cols, sizes, (1,))
+    e = np.array([-0.5, 0.1, 0.7])
+    v = rng.standard_normal(n)
+    sig = (rng.standard_normal((3, H.rows.size)) + 1j * rng.standard_normal((3, H.rows.size)))
+    SG = DSDBCOO(sig, H.rows, H.cols, sizes, (3,))
+    A = assemble_system(e, 1e-3, H, overlap=S, potential=v, sigma=SG)
+    got = A.data.cpu().numpy()
+    for k in range(3):
+        full = (e[k] + 1e-3j) * sm - np.diag(v) - hm
+        want = full[H.rows, H.cols] - sig[k]
+        assert np.allclose(got[k], want, rtol=0, atol=1e-13)
