@@ -294,7 +294,8 @@ typedef struct qtx_server_stats {
 qtx_status qtx_server_create(const qtx_server_config* cfg, qtx_server** out);
 /* Finishes every request already submitted, then stops the workers. */
 qtx_status qtx_server_destroy(qtx_server* srv);
-/* Enqueue one request (precision and flags as for qtx_transport_solve; the
+/* Enqueue one request (precision and flags as for qtx_transport_solve, except
+ * that QTX_FLAG_GRAPH is ignored: every request has its own buffers; the
  * problem's max_batch_size sets the energies per device call). */
 qtx_status qtx_server_submit(qtx_server* srv, const qtx_transport_problem* p, const qtx_transport_outputs* o,
                              int32_t precision, uint32_t flags, int64_t* request_id);

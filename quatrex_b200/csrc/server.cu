@@ -208,7 +208,9 @@ qtx_status qtx_server_submit(qtx_server* srv, const qtx_transport_problem* p, co
   req->p = *p;
   req->o = *o;
   req->precision = precision;
-  req->flags = flags;
+  // every request brings its own buffers, so a captured sweep would never be
+  // replayed and its work space would escape the admission budget
+  req->flags = flags & ~QTX_FLAG_GRAPH;
   const int64_t ne_call = p->max_batch_size > 0 ? std::min(p->max_batch_size, p->num_energies) : p->num_energies;
   req->footprint = qtx_transport_footprint(p->num_blocks, p->block_size, ne_call, precision);
   std::lock_guard<std::mutex> lk(srv->m);
