@@ -3,12 +3,15 @@
 
 Workload (the single-GPU scale-up): a seeded block-tridiagonal device with
 nb = 64 blocks of b = 256 orbitals, 1024 energies on [-2, 2], complex128.
-One step = one batch of energies (default 128) through the full hot path:
+One step = one batch of energies (by default one energy per SM, 148 on a
+B200: the block inverse runs one matrix per SM, so the batch fills exactly
+one wave of it) through the full hot path:
 A(E) = (E + i eta) I - H formed on the device, Sancho-Rubio for both contacts
 (tol 1e-12), contact self-energies, the RGF selected solve returning the
 diagonal and first off-diagonal blocks of G^R, G^< and G^>, per-block density,
 contact currents and the Caroli transmission.  With the defaults
-(--steps 8, 128 energies per step) the timed region covers all 1024 energies.
+(--steps 7, 148 energies per step) the timed region covers all 1024 energies
+(1036 solves; steps wrap around the energy grid).
 
 value: whole-job solves/s with H resident in HBM; e2e: the same through the
 public API with H and the energies copied from pinned host memory and the
@@ -218,6 +221,8 @@ def run_ours(args):
     cfg = _workload(args)
     dev = make_device(**cfg)
     E = args.energies_per_step
+    if E <= 0:
+        E = torch.cuda.get_device_properties(local).multi_processor_count
     nb, b = cfg["num_blocks"], cfg["block_size"]
     solver = TransportSolver(dev, max_batch_size=E, precision=args.precision, cuda_device=local)
     energies_all = torch.from_numpy(dev.energies).to(f"cuda:{local}")
@@ -542,7 +547,7 @@ def run_dropin(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=7)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["large", "small", "uneven", "serve", "dropin"], default="large")
@@ -556,7 +561,8 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serve workload: Poisson arrival rate (1/s)")
     ap.add_argument("--uneven-precision", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--energies-per-step", type=int, default=128)
+    ap.add_argument("--energies-per-step", type=int, default=0,
+                    help="energies per step (0: one per SM of the device)")
     ap.add_argument("--cpu-energies", type=int, default=3)
     ap.add_argument("--ref-energies-per-step", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
