@@ -3,8 +3,9 @@
 For a key it times a short probe device (the seeded generator at the key's
 block size, few blocks) over the candidate settings
 
-* energies per device call (the batch the kernels see; bounded by a memory
-  budget),
+* energies per device call (the batch the kernels see; powers of two and
+  148, one per SM of a B200, which fills one wave of the block inverse;
+  bounded by a memory budget),
 * the GEMM path: FP64 DMMA or the INT8 split-product path (for a "mixed" key
   both paths satisfy the accuracy contract, so the faster one wins; a "fp64"
   key only uses DMMA),
@@ -39,7 +40,7 @@ def _bucket(n: int) -> int:
 
 class Autotuner:
     def __init__(self, cache_path: str | None = None, memory_budget: int | None = None,
-                 candidates_ne=(8, 16, 32, 64, 128, 256), probe_blocks: int = 6, repeats: int = 2):
+                 candidates_ne=(8, 16, 32, 64, 128, 148, 256), probe_blocks: int = 6, repeats: int = 2):
         self.cache_path = cache_path
         self.memory_budget = memory_budget
         self.candidates_ne = tuple(candidates_ne)
