@@ -38,10 +38,11 @@
  *    (qtx_selected_inv / qtx_selected_solve): then the data rows, the OBC
  *    blocks and the current are HOST pointers (the block_index arrays of a
  *    qtx_btd_desc stay device pointers) and the library streams the stack
- *    through the device in energy batches: two device staging sets, uploads
- *    and downloads on a copy stream overlapping the solve when the host
- *    arrays are page-locked by the caller; the call returns when every output
- *    is back in host memory.
+ *    through the device in energy batches: two device staging sets, a copy
+ *    thread moving the caller's (pageable) rows through a ring of page-locked
+ *    slots (512 MiB per context, taken from a process-wide pool at the first
+ *    such call and kept) while the solver runs; the call returns when every
+ *    output is back in host memory.
  *  - Nothing is synchronous unless stated: work is enqueued on `stream`.
  *  - No exception crosses the ABI; every call returns a qtx_status and the
  *    context keeps a text message (qtx_last_error).

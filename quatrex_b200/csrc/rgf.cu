@@ -12,8 +12,13 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <condition_variable>
+#include <deque>
+#include <exception>
+#include <functional>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.h"
@@ -126,6 +131,51 @@ void pinned_give(int* p) {
   g_pinned_free.push_back(p);
 }
 
+// Ring of page-locked host slots for the host-buffer streaming: every
+// host<->device copy of that mode goes through it (the DMA engines read and
+// write page-locked memory at full speed; the caller's arrays are pageable).
+// Rings come from a process-wide pool and are never freed: cudaFreeHost may
+// synchronise the device.
+struct PinRing {
+  static constexpr int kSlots = 8;
+  static constexpr size_t kSlotBytes = 64u << 20;
+  char* base = nullptr;
+  cudaEvent_t ev[kSlots] = {};  // last DMA from / to each slot
+  char* slot(int i) const { return base + (size_t)i * kSlotBytes; }
+};
+std::mutex g_ring_mutex;
+std::vector<PinRing*> g_ring_free;
+PinRing* ring_take() {
+  {
+    std::lock_guard<std::mutex> lk(g_ring_mutex);
+    if (!g_ring_free.empty()) {
+      PinRing* r = g_ring_free.back();
+      g_ring_free.pop_back();
+      return r;
+    }
+  }
+  PinRing* r = new PinRing();
+  if (cudaMallocHost(reinterpret_cast<void**>(&r->base), PinRing::kSlots * PinRing::kSlotBytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete r;
+    return nullptr;
+  }
+  for (auto& e : r->ev) {
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      e = nullptr;
+    }
+  }
+  return r;
+}
+void ring_give(PinRing* r) {
+  if (!r) return;
+  for (auto& e : r->ev)
+    if (e) cudaEventSynchronize(e);
+  std::lock_guard<std::mutex> lk(g_ring_mutex);
+  g_ring_free.push_back(r);
+}
+
 struct qtx_ctx {
   int device = 0;
   GraphCache graphs;
@@ -136,6 +186,7 @@ struct qtx_ctx {
   int64_t launches = 0;
   size_t mem_limit = 0;
   int* h_pinned = nullptr;     // pinned host word (process-wide pool)
+  PinRing* ring = nullptr;     // page-locked staging of the host-buffer mode (process-wide pool)
   bool timing = false;
   std::vector<TimedLaunch> timed;
   std::vector<cudaEvent_t> event_pool;
@@ -1088,14 +1139,15 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
 // (QTX_FLAG_HOST_BUFFERS)
 // ---------------------------------------------------------------------------
 // The stack is processed in energy batches: the batch's rows of every array
-// are copied into one of two device staging sets on a copy stream, solved on
-// the caller's stream and copied back on the copy stream, so that the upload
-// of batch q + 1 and the download of batch q - 1 overlap the solve of batch q
-// when the caller's arrays are page-locked.  From pageable arrays the driver
-// stages every copy and the host waits for it; page-locking them inside the
-// call was measured slower than that (4.6 vs 5.2 solves/s at nb = 64,
-// b = 256), so the library does not.  Device memory is bounded by two staging
-// sets and the solver's own work space of one batch, whatever the stack size.
+// are copied into one of two device staging sets, solved on the caller's
+// stream and copied back, so that the upload of batch q + 1 and the download
+// of batch q - 1 overlap the solve of batch q.  The copies run on a copy
+// thread through the context's ring of page-locked slots (host memcpy over a
+// few threads, then DMA), because the caller's arrays are pageable: through
+// the driver's own staging they ran at about 10 GB/s, and page-locking them
+// for each call (cudaHostRegister) was slower still.  Device memory is
+// bounded by two staging sets and the solver's own work space of one batch,
+// whatever the stack size.
 size_t desc_row_bytes(const qtx_btd_desc* d) { return sizeof(cplx) * (size_t)d->stack_stride; }
 
 // One host array of the call: rows of `row_bytes`, `rows` of them.
@@ -1119,11 +1171,142 @@ int64_t host_batch(int64_t max_batch, int64_t NE, size_t staging_per_energy, int
   return ne;
 }
 
+// Copies between the caller's pageable arrays and device memory through a
+// PinRing: host memcpy into a slot (split over a few host threads), then an
+// async DMA on `cs`; a slot is reused only after its previous DMA completed.
+// Downloads keep up to kSlots - 1 DMAs in flight ahead of the host copies.
+struct RingCopier {
+  PinRing& R;
+  cudaStream_t cs;
+  int next = 0;
+  struct Pending {
+    int slot;
+    char* host;
+    size_t len;
+  };
+  std::deque<Pending> pending;
+
+  static void memcpy_mt(char* dst, const char* src, size_t n) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>({8, (size_t)std::max(1u, hw / 2), n / (4u << 20) + 1});
+    if (nt <= 1) {
+      memcpy(dst, src, n);
+      return;
+    }
+    std::vector<std::thread> th;
+    const size_t part = (n + nt - 1) / nt;
+    for (size_t t = 0; t < nt; ++t) {
+      const size_t off = t * part;
+      if (off >= n) break;
+      const size_t len = std::min(part, n - off);
+      th.emplace_back([=] { memcpy(dst + off, src + off, len); });
+    }
+    for (auto& x : th) x.join();
+  }
+  int take_slot() {
+    const int sl = next;
+    next = (next + 1) % PinRing::kSlots;
+    // a pending download in this slot is copied out first
+    while (!pending.empty() && std::any_of(pending.begin(), pending.end(), [&](const Pending& p) { return p.slot == sl; }))
+      drain_one();
+    QTX_CUDA_TRY(cudaEventSynchronize(R.ev[sl]));
+    return sl;
+  }
+  void upload(char* dev, const char* host, size_t n) {
+    for (size_t off = 0; off < n; off += PinRing::kSlotBytes) {
+      const size_t len = std::min(PinRing::kSlotBytes, n - off);
+      const int sl = take_slot();
+      memcpy_mt(R.slot(sl), host + off, len);
+      QTX_CUDA_TRY(cudaMemcpyAsync(dev + off, R.slot(sl), len, cudaMemcpyHostToDevice, cs));
+      QTX_CUDA_TRY(cudaEventRecord(R.ev[sl], cs));
+    }
+  }
+  void download(char* host, const char* dev, size_t n) {
+    for (size_t off = 0; off < n; off += PinRing::kSlotBytes) {
+      const size_t len = std::min(PinRing::kSlotBytes, n - off);
+      if ((int)pending.size() >= PinRing::kSlots - 1) drain_one();
+      const int sl = take_slot();
+      QTX_CUDA_TRY(cudaMemcpyAsync(R.slot(sl), dev + off, len, cudaMemcpyDeviceToHost, cs));
+      QTX_CUDA_TRY(cudaEventRecord(R.ev[sl], cs));
+      pending.push_back({sl, host + off, len});
+    }
+  }
+  void drain_one() {
+    Pending p = pending.front();
+    pending.pop_front();
+    QTX_CUDA_TRY(cudaEventSynchronize(R.ev[p.slot]));
+    memcpy_mt(p.host, R.slot(p.slot), p.len);
+  }
+  void drain_all() {
+    while (!pending.empty()) drain_one();
+  }
+};
+
+// One host thread running copy tasks in order (uploads and downloads of the
+// streamed batches) while the calling thread runs the solver.
+struct CopyWorker {
+  std::mutex m;
+  std::condition_variable cv;
+  std::deque<std::function<void()>> tasks;
+  bool stop = false;
+  std::exception_ptr error;
+  int64_t done = 0, posted = 0;
+  std::thread th;
+  CopyWorker() : th([this] { run(); }) {}
+  ~CopyWorker() {
+    {
+      std::lock_guard<std::mutex> lk(m);
+      stop = true;
+    }
+    cv.notify_all();
+    th.join();
+  }
+  void run() {
+    for (;;) {
+      std::function<void()> f;
+      {
+        std::unique_lock<std::mutex> lk(m);
+        cv.wait(lk, [&] { return stop || !tasks.empty(); });
+        if (tasks.empty()) return;
+        f = std::move(tasks.front());
+        tasks.pop_front();
+      }
+      try {
+        if (!error) f();
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(m);
+        if (!error) error = std::current_exception();
+      }
+      {
+        std::lock_guard<std::mutex> lk(m);
+        ++done;
+      }
+      cv.notify_all();
+    }
+  }
+  int64_t post(std::function<void()> f) {
+    std::lock_guard<std::mutex> lk(m);
+    tasks.push_back(std::move(f));
+    cv.notify_all();
+    return ++posted;
+  }
+  // wait until task number `ticket` (1-based) has run; rethrows its failure
+  void wait(int64_t ticket) {
+    std::unique_lock<std::mutex> lk(m);
+    cv.wait(lk, [&] { return done >= ticket; });
+    if (error) std::rethrow_exception(error);
+  }
+};
+
 // Streams `solve(e0, ne, set)` over the stack.  `arrs` are the per-energy
 // arrays (inputs copied up, outputs copied down; outputs are also copied up so
-// that entries the solver does not write keep their values).
+// that entries the solver does not write keep their values).  With the
+// context's PinRing, a copy thread uploads batch q + 1 and downloads batch
+// q - 1 through page-locked slots while the solver runs batch q; without one
+// (page-locked memory refused) the copies go straight from the pageable arrays.
 template <typename F>
-void stream_host_batches(std::vector<HostArr>& arrs, int64_t NE, int64_t ne_b, cudaStream_t s, F&& solve) {
+void stream_host_batches(qtx_ctx* ctx, std::vector<HostArr>& arrs, int64_t NE, int64_t ne_b, cudaStream_t s,
+                         F&& solve) {
   size_t per_set = 0;
   for (auto& a : arrs) per_set += ((a.row_bytes * ne_b + 255) / 256) * 256;
   DevBuf staging(2 * per_set, s);
@@ -1134,6 +1317,10 @@ void stream_host_batches(std::vector<HostArr>& arrs, int64_t NE, int64_t ne_b, c
       cur += ((a.row_bytes * ne_b + 255) / 256) * 256;
     }
   }
+  if (!ctx->ring) ctx->ring = ring_take();
+  bool use_ring = ctx->ring != nullptr;
+  if (use_ring)
+    for (auto e : ctx->ring->ev) use_ring = use_ring && e != nullptr;
   cudaStream_t cs = nullptr;
   QTX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   cudaEvent_t up[2] = {nullptr, nullptr}, solved = nullptr;
@@ -1144,6 +1331,7 @@ void stream_host_batches(std::vector<HostArr>& arrs, int64_t NE, int64_t ne_b, c
     if (solved) cudaEventDestroy(solved);
     cudaStreamDestroy(cs);
   };
+  const int64_t nbatch = (NE + ne_b - 1) / ne_b;
   try {
     QTX_CUDA_TRY(cudaEventCreateWithFlags(&up[0], cudaEventDisableTiming));
     QTX_CUDA_TRY(cudaEventCreateWithFlags(&up[1], cudaEventDisableTiming));
@@ -1151,28 +1339,59 @@ void stream_host_batches(std::vector<HostArr>& arrs, int64_t NE, int64_t ne_b, c
     // the staging memory was allocated on s: the copy stream starts after it
     QTX_CUDA_TRY(cudaEventRecord(solved, s));
     QTX_CUDA_TRY(cudaStreamWaitEvent(cs, solved, 0));
-    auto upload = [&](int64_t e0, int64_t ne, int set) {
-      for (auto& a : arrs)
-        if (a.in || a.out)
-          QTX_CUDA_TRY(cudaMemcpyAsync(a.dev[set], (a.out ? a.hw : a.h) + e0 * a.row_bytes, ne * a.row_bytes,
-                                       cudaMemcpyHostToDevice, cs));
-      QTX_CUDA_TRY(cudaEventRecord(up[set], cs));
-    };
-    const int64_t nbatch = (NE + ne_b - 1) / ne_b;
-    if (nbatch > 0) upload(0, std::min(ne_b, NE), 0);
-    for (int64_t q = 0; q < nbatch; ++q) {
-      const int set = (int)(q & 1);
-      const int64_t e0 = q * ne_b, ne = std::min(ne_b, NE - e0);
-      // the next batch's upload is queued behind this set's previous download
-      if (q + 1 < nbatch) upload(e0 + ne_b, std::min(ne_b, NE - e0 - ne_b), set ^ 1);
-      QTX_CUDA_TRY(cudaStreamWaitEvent(s, up[set], 0));
-      solve(e0, ne, set);  // ends with a synchronisation of s
-      QTX_CUDA_TRY(cudaEventRecord(solved, s));
-      QTX_CUDA_TRY(cudaStreamWaitEvent(cs, solved, 0));
-      for (auto& a : arrs)
-        if (a.out)
-          QTX_CUDA_TRY(cudaMemcpyAsync(a.hw + e0 * a.row_bytes, a.dev[set], ne * a.row_bytes,
-                                       cudaMemcpyDeviceToHost, cs));
+    if (use_ring) {
+      RingCopier rc{*ctx->ring, cs};
+      CopyWorker w;
+      auto upload = [&](int64_t e0, int64_t ne, int set) {
+        return w.post([&, e0, ne, set] {
+          for (auto& a : arrs)
+            if (a.in || a.out) rc.upload(a.dev[set], (a.out ? a.hw : a.h) + e0 * a.row_bytes, ne * a.row_bytes);
+          QTX_CUDA_TRY(cudaEventRecord(up[set], cs));
+        });
+      };
+      auto download = [&](int64_t e0, int64_t ne, int set) {
+        return w.post([&, e0, ne, set] {
+          for (auto& a : arrs)
+            if (a.out) rc.download(a.hw + e0 * a.row_bytes, a.dev[set], ne * a.row_bytes);
+          rc.drain_all();
+        });
+      };
+      int64_t t_cur = nbatch > 0 ? upload(0, std::min(ne_b, NE), 0) : 0, t_last = t_cur;
+      for (int64_t q = 0; q < nbatch; ++q) {
+        const int set = (int)(q & 1);
+        const int64_t e0 = q * ne_b, ne = std::min(ne_b, NE - e0);
+        // queued behind the download of batch q - 1, which last read set ^ 1
+        int64_t t_next = 0;
+        if (q + 1 < nbatch) t_next = upload(e0 + ne_b, std::min(ne_b, NE - e0 - ne_b), set ^ 1);
+        w.wait(t_cur);
+        QTX_CUDA_TRY(cudaStreamWaitEvent(s, up[set], 0));
+        solve(e0, ne, set);  // ends with a synchronisation of s
+        t_last = download(e0, ne, set);
+        t_cur = t_next;
+      }
+      w.wait(t_last);
+    } else {
+      auto upload = [&](int64_t e0, int64_t ne, int set) {
+        for (auto& a : arrs)
+          if (a.in || a.out)
+            QTX_CUDA_TRY(cudaMemcpyAsync(a.dev[set], (a.out ? a.hw : a.h) + e0 * a.row_bytes, ne * a.row_bytes,
+                                         cudaMemcpyHostToDevice, cs));
+        QTX_CUDA_TRY(cudaEventRecord(up[set], cs));
+      };
+      if (nbatch > 0) upload(0, std::min(ne_b, NE), 0);
+      for (int64_t q = 0; q < nbatch; ++q) {
+        const int set = (int)(q & 1);
+        const int64_t e0 = q * ne_b, ne = std::min(ne_b, NE - e0);
+        if (q + 1 < nbatch) upload(e0 + ne_b, std::min(ne_b, NE - e0 - ne_b), set ^ 1);
+        QTX_CUDA_TRY(cudaStreamWaitEvent(s, up[set], 0));
+        solve(e0, ne, set);  // ends with a synchronisation of s
+        QTX_CUDA_TRY(cudaEventRecord(solved, s));
+        QTX_CUDA_TRY(cudaStreamWaitEvent(cs, solved, 0));
+        for (auto& a : arrs)
+          if (a.out)
+            QTX_CUDA_TRY(cudaMemcpyAsync(a.hw + e0 * a.row_bytes, a.dev[set], ne * a.row_bytes,
+                                         cudaMemcpyDeviceToHost, cs));
+      }
     }
     QTX_CUDA_TRY(cudaStreamSynchronize(cs));
   } catch (...) {
@@ -1276,6 +1495,7 @@ qtx_status qtx_ctx_destroy(qtx_ctx* ctx) {
   if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
   for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
   pinned_give(ctx->h_pinned);
+  ring_give(ctx->ring);
   delete ctx;
   return QTX_OK;
 }
@@ -1399,7 +1619,7 @@ qtx_status qtx_selected_inv(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const void
       for (auto& x : arrs) per_e += x.row_bytes;
       const int64_t NE = a_desc->stack_size;
       const int64_t ne_b = host_batch(max_batch_size, NE, per_e, nb, bmax);
-      stream_host_batches(arrs, NE, ne_b, s, [&](int64_t, int64_t ne, int set) {
+      stream_host_batches(ctx, arrs, NE, ne_b, s, [&](int64_t, int64_t ne, int set) {
         qtx_btd_desc ad = batch_desc(a_desc, ne), od = batch_desc(out_desc, ne);
         std::vector<const void*> obc(nb, nullptr);
         for (size_t q = 0; q < obc_i.size(); ++q) obc[obc_i[q]] = arrs[2 + q].dev[set];
@@ -1483,7 +1703,7 @@ qtx_status qtx_selected_solve(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const vo
       for (auto& x : arrs) per_e += x.row_bytes;
       const int64_t NE = a_desc->stack_size;
       const int64_t ne_b = host_batch(max_batch_size, NE, per_e, nb, bmax);
-      stream_host_batches(arrs, NE, ne_b, s, [&](int64_t, int64_t ne, int set) {
+      stream_host_batches(ctx, arrs, NE, ne_b, s, [&](int64_t, int64_t ne, int set) {
         qtx_btd_desc ad = batch_desc(a_desc, ne), sld = batch_desc(sl_desc, ne), sgd = batch_desc(sg_desc, ne);
         qtx_btd_desc xld = batch_desc(xl_desc, ne), xgd = batch_desc(xg_desc, ne);
         qtx_btd_desc xrd = want_xr ? batch_desc(xr_desc, ne) : qtx_btd_desc{};
