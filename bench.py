@@ -396,16 +396,19 @@ def run_uneven(args):
         for prec in ("fp64", "mixed"):
             cmd = [sys.executable, os.path.abspath(__file__), "--workload", "uneven", "--instances",
                    str(args.instances), "--streams", str(args.streams), "--uneven-precision", prec]
+            if args.no_group:
+                cmd.append("--no-group")
             rc = rc or subprocess.call(cmd)
         return rc
     for prec in (args.uneven_precision,):
         tuner = Autotuner(cache_path=os.path.join(ROOT, "_build", "autotune.json"))
-        bt = BatchedTransport(precision=prec, streams=args.streams, tuner=tuner)
+        bt = BatchedTransport(precision=prec, streams=args.streams, tuner=tuner, group_small=not args.no_group)
         try:
             # warm-up outside the timed region: tune every (b, batch, precision)
             # key the instances use, then run the smallest instance once
-            for x in insts:
-                bt.choice_for(x)
+            for kind, idx in bt.jobs(insts):
+                if kind == "one":
+                    bt.choice_for(insts[idx[0]])
             bt.run([min(insts, key=lambda x: x.device.block_size * x.device.num_blocks)])
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -414,7 +417,8 @@ def run_uneven(args):
             dt = time.perf_counter() - t0
             per_instance = [{"b": x.device.block_size, "nb": x.device.num_blocks, "ne": len(x.energies),
                              "seconds": round(r["seconds"], 3),
-                             "choice": {k: v for k, v in bt.choice_for(x).items() if k != "probe_solves_per_s"}}
+                             "choice": ({"path": "grouped persistent launch (fp64)"} if r["grouped"] else
+                                        {k: v for k, v in bt.choice_for(x).items() if k != "probe_solves_per_s"})}
                             for x, r in zip(insts, res)]
         finally:
             bt.close()
@@ -422,6 +426,7 @@ def run_uneven(args):
                       "precision": prec, "value": total_solves(insts) / dt, "unit": "solves/s",
                       "seconds": dt, "instances": len(insts), "solves": total_solves(insts),
                       "alg_tflops": total_flops(insts) / dt / 1e12, "streams": args.streams,
+                      "grouped_small": not args.no_group,
                       "per_instance": per_instance})
         print(json.dumps(lines[-1]), flush=True)
     return 0
@@ -560,6 +565,8 @@ def main():
     ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serve workload: Poisson arrival rate (1/s)")
     ap.add_argument("--uneven-precision", choices=["both", "fp64", "mixed"], default="both")
+    ap.add_argument("--no-group", action="store_true",
+                    help="uneven: solve b <= 64 instances one by one instead of one grouped launch per block size")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--energies-per-step", type=int, default=0,
                     help="energies per step (0: one per SM of the device)")

@@ -232,6 +232,27 @@ typedef struct qtx_transport_outputs {
 qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,
                                int32_t precision, uint32_t flags, qtx_stream stream);
 
+/* Grouped transport solve (the batching form's persistent launch): every
+ * energy of `count` generator-form problems that share one block size
+ * b <= 64 (each its own number of blocks, H, energy grid, contacts and
+ * outputs, as for qtx_transport_solve) in ONE persistent kernel launch.  Each
+ * CTA takes the next (problem, energy) pair and runs its whole solve
+ * (Sancho-Rubio of both leads, contact self-energies, forward and backward
+ * sweeps, observables); pairs are handed out longest problem first.
+ * max_batch_size is ignored.  precision must be QTX_PREC_FP64 (the INT8
+ * split products only pay off at b >= 512).  Synchronous (returns when the
+ * outputs are written); QTX_E_NOT_CONVERGED as for qtx_transport_solve;
+ * QTX_E_UNSUPPORTED for b > 64, QTX_E_INVAL for mixed block sizes. */
+qtx_status qtx_transport_solve_grouped(qtx_ctx* ctx, int32_t count, const qtx_transport_problem* problems,
+                                       const qtx_transport_outputs* outputs, int32_t precision, uint32_t flags,
+                                       qtx_stream stream);
+
+/* Device bytes one qtx_transport_solve_grouped call allocates (descriptors
+ * and one work space per resident CTA); H and the outputs are the caller's.
+ * 0 for an unsupported block size. */
+size_t qtx_transport_grouped_footprint(int32_t count, const int32_t* num_blocks, const int64_t* num_energies,
+                                       int32_t block_size);
+
 /* Block-sorting permutation of a COO pattern on the device (DSDBCOO
  * construction, <- compute_block_sort_index,
  * src/qttools/kernels/datastructure/cupy/dsdbcoo.py:234-298): rows, cols

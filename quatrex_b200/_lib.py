@@ -169,6 +169,13 @@ SIGNATURES = {
         [c_void_p, ctypes.POINTER(TransportProblem), ctypes.POINTER(TransportOutputs), c_int32, c_uint32, c_void_p],
     ),
     "qtx_transport_footprint": (ctypes.c_size_t, [c_int32, c_int32, c_int64, c_int32]),
+    "qtx_transport_solve_grouped": (
+        c_int32,
+        [c_void_p, c_int32, ctypes.POINTER(TransportProblem), ctypes.POINTER(TransportOutputs), c_int32, c_uint32,
+         c_void_p],
+    ),
+    "qtx_transport_grouped_footprint": (
+        ctypes.c_size_t, [c_int32, ctypes.POINTER(c_int32), ctypes.POINTER(c_int64), c_int32]),
     "qtx_assemble_system": (
         c_int32, [c_void_p, c_int64, c_int64, c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                   c_void_p, c_int64, c_void_p, c_int64, c_void_p]),

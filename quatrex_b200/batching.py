@@ -1,12 +1,16 @@
 """Uneven batches of transport instances on one GPU.
 
-Instances differ in block size, number of blocks and energy grid.  Each is
-solved by a worker that owns a CUDA stream and its own library context, so
-several instances run on the device at the same time (small instances alone
-cannot fill 148 SMs); instances are handed out longest first.  Per instance
-the energy grid is cut into device calls of the size the autotuner picked for
-(block size, number of energies, precision), and the sweep of every full-size
-call is a replayed CUDA graph when the tuner found that faster.
+Instances differ in block size, number of blocks and energy grid.  The
+instances of each block size b <= 64 run together in ONE persistent launch
+(qtx_transport_solve_grouped: every (instance, energy) pair of the group is a
+work item of one kernel, a CTA solves a whole energy, pairs are handed out
+longest instance first).  Larger instances are solved one by one: per
+instance the energy grid is cut into device calls of the size the autotuner
+picked for (block size, number of energies, precision), and the sweep of every
+full-size call is a replayed CUDA graph when the tuner found that faster.
+Each job (a group or a large instance) runs on a worker that owns a CUDA
+stream and its own library context, so several jobs share the device; jobs
+are handed out longest first.
 
 Only observables travel back to the host (per-block density and hole
 density, transmission, contact currents, Sancho-Rubio iteration counts); the
@@ -26,7 +30,8 @@ import torch
 
 from quatrex_b200 import _lib
 from quatrex_b200.autotune import Autotuner
-from quatrex_b200.transport import TransportSolver
+from quatrex_b200.transport import (GROUPED_MAX_BLOCK_SIZE, TransportSolver, grouped_footprint_bytes,
+                                    solve_grouped)
 from quatrex_b200.workloads import TransportDevice
 
 OBSERVABLE_KEYS = ("density", "hole_density", "transmission", "current_left", "current_right", "sr_iterations")
@@ -87,6 +92,19 @@ class Worker:
         self.busy_s += time.perf_counter() - t0
         return {k: torch.cat(v).numpy() for k, v in results.items()}
 
+    def solve_group(self, devs: list[TransportDevice], energies: list, keys=OBSERVABLE_KEYS) -> list[dict]:
+        """Every energy of several instances of one block size in one
+        persistent launch on this worker's stream; returns host arrays."""
+        t0 = time.perf_counter()
+        dev = f"cuda:{self.cuda}"
+        with torch.cuda.stream(self.stream):
+            hs = [(torch.from_numpy(d.h_diag).to(dev), torch.from_numpy(d.h_upper).to(dev)) for d in devs]
+            outs = solve_grouped(devs, [np.asarray(e, dtype=np.float64) for e in energies], keys=keys,
+                                 cuda_device=self.cuda, hamiltonians=hs, ctx=self.ctx, stream=self.stream)
+            res = [{k: v.cpu().numpy() for k, v in out.items()} for out in outs]
+        self.busy_s += time.perf_counter() - t0
+        return res
+
 
 @dataclass
 class Instance:
@@ -98,8 +116,12 @@ class BatchedTransport:
     """Solve a list of uneven instances with ``streams`` concurrent workers."""
 
     def __init__(self, precision: str = "fp64", streams: int = 4, tuner: Autotuner | None = None,
-                 cuda_device: int | None = None, keys=OBSERVABLE_KEYS, memory_budget: int | None = None):
+                 cuda_device: int | None = None, keys=OBSERVABLE_KEYS, memory_budget: int | None = None,
+                 group_small: bool = True):
         self.precision = precision
+        # instances with b <= 64 share one persistent launch per block size
+        # (FP64 products: the INT8 split products only pay off at b >= 512)
+        self.group_small = group_small
         self.cuda = torch.cuda.current_device() if cuda_device is None else cuda_device
         if memory_budget is None:
             free, _ = torch.cuda.mem_get_info(self.cuda)
@@ -141,29 +163,69 @@ class BatchedTransport:
         return TransportSolver.footprint_bytes(inst.device.num_blocks, inst.device.block_size,
                                                min(ne_call, len(inst.energies)), ("density", "transmission"))
 
+    def group_footprint(self, members: list[Instance]) -> int:
+        """Device bytes of one grouped launch: its work space, H and the outputs."""
+        b = members[0].device.block_size
+        ws = grouped_footprint_bytes([m.device.num_blocks for m in members], [len(m.energies) for m in members], b)
+        h = sum(16 * b * b * (3 * m.device.num_blocks) for m in members)
+        out = sum(64 * len(m.energies) * (m.device.num_blocks + 2) for m in members)
+        return int(ws + h + out)
+
+    def jobs(self, instances: list[Instance]) -> list[tuple[str, list[int]]]:
+        """("group", members) per block size <= 64 when grouping, else ("one", [i]);
+        longest first."""
+        groups: dict[int, list[int]] = {}
+        singles = []
+        for i, x in enumerate(instances):
+            b = x.device.block_size
+            if self.group_small and b <= GROUPED_MAX_BLOCK_SIZE and len(x.energies) > 0:
+                groups.setdefault(b, []).append(i)
+            else:
+                singles.append(i)
+        cost = lambda idx: sum(instance_flops(instances[i].device, len(instances[i].energies)) for i in idx)
+        out = [("group", idx) for idx in groups.values()] + [("one", [i]) for i in singles]
+        return sorted(out, key=lambda j: -cost(j[1]))
+
     def run(self, instances: list[Instance]) -> list[dict]:
-        """Results in input order; each dict also holds 'seconds' (wall time on its worker)."""
-        order = sorted(range(len(instances)),
-                       key=lambda i: -instance_flops(instances[i].device, len(instances[i].energies)))
+        """Results in input order; each dict also holds 'seconds' (wall time of
+        its job on its worker: the whole group's for grouped instances) and
+        'grouped' (whether it ran in a grouped launch)."""
+        jobs = self.jobs(instances)
         # tune every key up front (serially), so workers only read the table
-        for i in order:
-            self.choice_for(instances[i])
+        for kind, idx in jobs:
+            if kind == "one":
+                self.choice_for(instances[idx[0]])
         results: list[dict | None] = [None] * len(instances)
 
-        def job(i):
-            choice = self.choice_for(instances[i])
-            fp = self.footprint(instances[i], int(choice["energies_per_call"]))
+        def job(j):
+            kind, idx = j
+            if kind == "one":
+                choice = self.choice_for(instances[idx[0]])
+                fp = self.footprint(instances[idx[0]], int(choice["energies_per_call"]))
+            else:
+                fp = self.group_footprint([instances[i] for i in idx])
             with self._cv:
-                # admission by device-memory footprint next to the instances already running
+                # admission by device-memory footprint next to the jobs already running
                 while self._used + fp > self.budget and self._used > 0:
                     self._cv.wait()
                 self._used += fp
             w = self._take()
             try:
                 t0 = time.perf_counter()
-                r = w.solve(instances[i].device, instances[i].energies, self.precision, choice, self.keys)
-                r["seconds"] = time.perf_counter() - t0
-                results[i] = r
+                if kind == "one":
+                    r = w.solve(instances[idx[0]].device, instances[idx[0]].energies, self.precision, choice,
+                                self.keys)
+                    r["seconds"] = time.perf_counter() - t0
+                    r["grouped"] = False
+                    results[idx[0]] = r
+                else:
+                    rs = w.solve_group([instances[i].device for i in idx], [instances[i].energies for i in idx],
+                                       self.keys)
+                    dt = time.perf_counter() - t0
+                    for i, r in zip(idx, rs):
+                        r["seconds"] = dt
+                        r["grouped"] = True
+                        results[i] = r
             finally:
                 self._give(w)
                 with self._cv:
@@ -171,7 +233,7 @@ class BatchedTransport:
                     self._cv.notify_all()
 
         with ThreadPoolExecutor(max_workers=len(self.workers)) as ex:
-            list(ex.map(job, order))
+            list(ex.map(job, jobs))
         return results
 
 

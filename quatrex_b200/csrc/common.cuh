@@ -40,6 +40,18 @@ __host__ __device__ __forceinline__ cplx crecip(cplx z) {
     return cmk(r / den, -1.0 / den);
   }
 }
+// 1 / z of a pivot, Smith's scaling with one reciprocal and one quotient (the
+// Gauss-Jordan inverses share it, so they agree on every pivot).
+__host__ __device__ __forceinline__ cplx crecip_pivot(cplx z) {
+  if (fabs(z.x) >= fabs(z.y)) {
+    const double r = z.y / z.x;
+    const double t = 1.0 / (z.x + z.y * r);
+    return cmk(t, -r * t);
+  }
+  const double r = z.x / z.y;
+  const double t = 1.0 / (z.x * r + z.y);
+  return cmk(r * t, -t);
+}
 __host__ __device__ __forceinline__ double cabs1(cplx z) { return fabs(z.x) + fabs(z.y); }
 
 // Per-context launch counter (host side), incremented by every launch helper.

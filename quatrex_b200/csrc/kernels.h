@@ -102,3 +102,32 @@ void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream);
 void launch_residual_norm(int n, int64_t batch, MatView x_ref, MatView x, double* abs_res, double* rel_res,
                           cudaStream_t stream);
 void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t stream);
+
+// One generator-form problem of a grouped transport solve, as the persistent
+// kernel reads it (rgf_grouped.cu).  Pairs item0 .. item0 + num_energies - 1 of
+// the launch's work list are this problem's energies.
+struct GroupedProblem {
+  int nb = 0, b = 0;
+  int64_t num_energies = 0, item0 = 0;
+  const cplx* h_diag = nullptr;   // (nb, b, b)
+  const cplx* h_upper = nullptr;  // (nb - 1, b, b)
+  const double* energies = nullptr;
+  double eta = 0, mu_left = 0, mu_right = 0, kt = 0, sr_tol = 0;
+  int sr_max_iterations = 0;
+  cplx *gr_diag = nullptr, *gr_upper = nullptr, *gr_lower = nullptr;
+  cplx *gl_diag = nullptr, *gl_upper = nullptr, *gg_diag = nullptr, *gg_upper = nullptr;
+  double *density = nullptr, *hole_density = nullptr, *transmission = nullptr;
+  cplx *current_left = nullptr, *current_right = nullptr;
+  int* sr_iterations = nullptr;
+};
+// Largest block size of the grouped solve.
+constexpr int GROUPED_MAX_B = 64;
+// CTAs of the persistent launch for `items` pairs of block size b (never more
+// than fit on the device at once), and the work-space elements of one CTA.
+int grouped_grid(int b, int64_t items);
+int64_t grouped_ws_elems(int max_nb, int b);
+// flags (device int, zeroed by the caller): bit 0 a zero pivot in a sweep
+// inverse, bit 1 a Sancho-Rubio iteration that did not converge.
+void launch_transport_grouped(int b, const GroupedProblem* problems, int count, int64_t items,
+                              unsigned long long* counter, int* flags, cplx* ws, int64_t ws_elems, int max_nb, int grid,
+                              cudaStream_t stream);

@@ -1135,6 +1135,99 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
 }
 
 // ---------------------------------------------------------------------------
+// Grouped transport solve: every energy of several problems of one block size
+// in one persistent launch (rgf_grouped.cu).
+// ---------------------------------------------------------------------------
+struct GroupedPlan {
+  std::vector<GroupedProblem> problems;  // longest first
+  int64_t items = 0;
+  int max_nb = 0, b = 0;
+};
+
+GroupedPlan grouped_plan(int32_t count, const qtx_transport_problem* p, const qtx_transport_outputs* o) {
+  GroupedPlan plan;
+  plan.b = p[0].block_size;
+  if (plan.b < 1 || plan.b > GROUPED_MAX_B)
+    throw QtxError(QTX_E_UNSUPPORTED, "qtx_transport_solve_grouped: block size must be 1..64");
+  std::vector<int> order(count);
+  for (int q = 0; q < count; ++q) {
+    const qtx_transport_problem& x = p[q];
+    if (x.block_size != plan.b) throw QtxError(QTX_E_INVAL, "qtx_transport_solve_grouped: mixed block sizes");
+    if (x.num_blocks < 2 || x.num_energies < 0 || !x.h_diag || !x.h_upper || (x.num_energies > 0 && !x.energies) ||
+        x.kt <= 0 || x.sr_max_iterations < 1)
+      throw QtxError(QTX_E_INVAL, "qtx_transport_solve_grouped: bad problem");
+    order[q] = q;
+  }
+  // longest problems first: their pairs are handed out first
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return p[x].num_blocks > p[y].num_blocks; });
+  for (int q : order) {
+    const qtx_transport_problem& x = p[q];
+    const qtx_transport_outputs& y = o[q];
+    GroupedProblem g;
+    g.nb = x.num_blocks;
+    g.b = x.block_size;
+    g.num_energies = x.num_energies;
+    g.item0 = plan.items;
+    g.h_diag = reinterpret_cast<const cplx*>(x.h_diag);
+    g.h_upper = reinterpret_cast<const cplx*>(x.h_upper);
+    g.energies = x.energies;
+    g.eta = x.eta;
+    g.mu_left = x.mu_left;
+    g.mu_right = x.mu_right;
+    g.kt = x.kt;
+    g.sr_tol = x.sr_tol;
+    g.sr_max_iterations = x.sr_max_iterations;
+    g.gr_diag = reinterpret_cast<cplx*>(y.gr_diag);
+    g.gr_upper = reinterpret_cast<cplx*>(y.gr_upper);
+    g.gr_lower = reinterpret_cast<cplx*>(y.gr_lower);
+    g.gl_diag = reinterpret_cast<cplx*>(y.gl_diag);
+    g.gl_upper = reinterpret_cast<cplx*>(y.gl_upper);
+    g.gg_diag = reinterpret_cast<cplx*>(y.gg_diag);
+    g.gg_upper = reinterpret_cast<cplx*>(y.gg_upper);
+    g.density = y.density;
+    g.hole_density = y.hole_density;
+    g.transmission = y.transmission;
+    g.current_left = reinterpret_cast<cplx*>(y.current_left);
+    g.current_right = reinterpret_cast<cplx*>(y.current_right);
+    g.sr_iterations = y.sr_iterations;
+    plan.items += x.num_energies;
+    plan.max_nb = std::max(plan.max_nb, x.num_blocks);
+    if (x.num_energies > 0) plan.problems.push_back(g);
+  }
+  return plan;
+}
+
+size_t grouped_bytes(const GroupedPlan& plan, int grid) {
+  const size_t desc = (sizeof(GroupedProblem) * plan.problems.size() + 255) / 256 * 256;
+  return desc + 256 + sizeof(cplx) * (size_t)grid * (size_t)grouped_ws_elems(plan.max_nb, plan.b);
+}
+
+// Returns the device flags (bit 1: a lead did not converge); throws on a zero pivot.
+int transport_grouped_impl(qtx_ctx* ctx, int32_t count, const qtx_transport_problem* p,
+                           const qtx_transport_outputs* o, cudaStream_t s) {
+  GroupedPlan plan = grouped_plan(count, p, o);
+  if (plan.items == 0) return 0;
+  const int grid = grouped_grid(plan.b, plan.items);
+  DevBuf mem(grouped_bytes(plan, grid), s);
+  char* base = mem.as<char>();
+  const size_t desc = (sizeof(GroupedProblem) * plan.problems.size() + 255) / 256 * 256;
+  GroupedProblem* d_problems = reinterpret_cast<GroupedProblem*>(base);
+  unsigned long long* counter = reinterpret_cast<unsigned long long*>(base + desc);
+  int* flags = reinterpret_cast<int*>(base + desc + 64);
+  cplx* ws = reinterpret_cast<cplx*>(base + desc + 256);
+  QTX_CUDA_TRY(cudaMemcpyAsync(d_problems, plan.problems.data(), sizeof(GroupedProblem) * plan.problems.size(),
+                               cudaMemcpyHostToDevice, s));
+  QTX_CUDA_TRY(cudaMemsetAsync(base + desc, 0, 256, s));
+  launch_transport_grouped(plan.b, d_problems, (int)plan.problems.size(), plan.items, counter, flags, ws,
+                           grouped_ws_elems(plan.max_nb, plan.b), plan.max_nb, grid, s);
+  QTX_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+  QTX_CUDA_TRY(cudaStreamSynchronize(s));
+  const int fl = ctx->h_pinned[0];
+  if (fl & 1) throw QtxError(QTX_E_SINGULAR, "qtx_transport_solve_grouped: exactly singular diagonal block");
+  return fl;
+}
+
+// ---------------------------------------------------------------------------
 // host-buffer streaming for qtx_selected_inv / qtx_selected_solve
 // (QTX_FLAG_HOST_BUFFERS)
 // ---------------------------------------------------------------------------
@@ -1812,6 +1905,41 @@ qtx_status qtx_obc_assemble(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
                                 MutView{reinterpret_cast<cplx*>(sigma_l), n, bb},
                                 MutView{reinterpret_cast<cplx*>(sigma_g), n, bb}, MutView{}, s);
   });
+}
+
+qtx_status qtx_transport_solve_grouped(qtx_ctx* ctx, int32_t count, const qtx_transport_problem* problems,
+                                       const qtx_transport_outputs* outputs, int32_t precision, uint32_t flags,
+                                       qtx_stream stream) {
+  int fl = 0;
+  qtx_status st = guarded(ctx, [&] {
+    if (count < 1 || !problems || !outputs) throw QtxError(QTX_E_INVAL, "qtx_transport_solve_grouped: no problems");
+    if (precision != QTX_PREC_FP64)
+      throw QtxError(QTX_E_UNSUPPORTED, "qtx_transport_solve_grouped: FP64 products only");
+    (void)flags;
+    fl = transport_grouped_impl(ctx, count, problems, outputs, reinterpret_cast<cudaStream_t>(stream));
+  });
+  if (st == QTX_OK && (fl & 2)) {
+    ctx->last_error = "Surface Green's function did not converge.";
+    return QTX_E_NOT_CONVERGED;
+  }
+  return st;
+}
+
+size_t qtx_transport_grouped_footprint(int32_t count, const int32_t* num_blocks, const int64_t* num_energies,
+                                       int32_t block_size) {
+  if (count < 1 || !num_blocks || !num_energies || block_size < 1 || block_size > GROUPED_MAX_B) return 0;
+  int max_nb = 0;
+  int64_t items = 0;
+  for (int q = 0; q < count; ++q) {
+    max_nb = std::max(max_nb, num_blocks[q]);
+    items += std::max<int64_t>(num_energies[q], 0);
+  }
+  if (items == 0) return 0;
+  GroupedPlan plan;
+  plan.b = block_size;
+  plan.max_nb = max_nb;
+  plan.problems.resize(count);
+  return grouped_bytes(plan, grouped_grid(block_size, items));
 }
 
 qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,

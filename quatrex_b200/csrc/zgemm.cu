@@ -168,17 +168,22 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_dmma_kernel(Params p) {
         }
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) bf[ni] = frag_b<OPB>(sb, kk + t, wn0 + ni * 8 + g);
+        // first product of every accumulator, then the second (the order
+        // within each accumulator is unchanged: Ar Br, -Ai Bi / Ar Bi, Ai Br)
 #pragma unroll
-        for (int mi = 0; mi < 2; ++mi) {
-          const double nai0 = -af[mi][0].y, nai1 = -af[mi][1].y;
+        for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
           for (int ni = 0; ni < 4; ++ni) {
             dmma(acc_re[mi][ni], af[mi][0].x, af[mi][1].x, bf[ni].x);
-            dmma(acc_re[mi][ni], nai0, nai1, bf[ni].y);
             dmma(acc_im[mi][ni], af[mi][0].x, af[mi][1].x, bf[ni].y);
+          }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) {
+            dmma(acc_re[mi][ni], -af[mi][0].y, -af[mi][1].y, bf[ni].y);
             dmma(acc_im[mi][ni], af[mi][0].y, af[mi][1].y, bf[ni].x);
           }
-        }
       }
     }
     cp_async_wait<0>();

@@ -93,19 +93,6 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-// 1 / z by Smith's scaled division (R. L. Smith, CACM 5(8), 1962) with one
-// reciprocal and one quotient.
-__device__ __forceinline__ cplx crecip_pivot(cplx z) {
-  if (fabs(z.x) >= fabs(z.y)) {
-    const double r = z.y / z.x;
-    const double t = 1.0 / (z.x + z.y * r);
-    return cmk(t, -r * t);
-  }
-  const double r = z.x / z.y;
-  const double t = 1.0 / (z.x * r + z.y);
-  return cmk(r * t, -t);
-}
-
 __device__ __forceinline__ void argmax_combine(double& v, int& i, double v2, int i2) {
   if (v2 > v || (v2 == v && i2 < i)) {
     v = v2;

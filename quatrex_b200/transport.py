@@ -131,3 +131,62 @@ class TransportSolver:
         st = lib.qtx_transport_solve(ctx, ctypes.byref(p), ctypes.byref(o), _PRECISIONS[self.precision], flags, s)
         _lib.check(st, ctx, "transport_solve")
         return outputs
+
+
+GROUPED_MAX_BLOCK_SIZE = 64
+
+
+def grouped_footprint_bytes(num_blocks, num_energies, block_size: int) -> int:
+    """Device bytes of one qtx_transport_solve_grouped call (descriptors and
+    the per-CTA work spaces; H and outputs not included)."""
+    nbs = (ctypes.c_int32 * len(num_blocks))(*[int(x) for x in num_blocks])
+    nes = (ctypes.c_int64 * len(num_energies))(*[int(x) for x in num_energies])
+    return int(_lib.load().qtx_transport_grouped_footprint(len(nbs), nbs, nes, int(block_size)))
+
+
+def solve_grouped(devices: list[TransportDevice], energies: list, keys=OUTPUT_KEYS, cuda_device: int | None = None,
+                  hamiltonians: list | None = None, ctx: int | None = None, stream=None) -> list[dict]:
+    """Solve every energy of several devices that share one block size
+    (<= 64) in one persistent launch (qtx_transport_solve_grouped).
+
+    ``energies[q]`` is the energy grid of ``devices[q]``; ``hamiltonians[q]``
+    may hand in its (h_diag, h_upper) already on the device.  Returns one
+    output dict (device tensors) per device, in input order."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("quatrex_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
+    if len(devices) != len(energies) or not devices:
+        raise ValueError("solve_grouped: one energy grid per device")
+    cuda = torch.cuda.current_device() if cuda_device is None else cuda_device
+    dev = f"cuda:{cuda}"
+    b = devices[0].block_size
+    if any(d.block_size != b for d in devices):
+        raise ValueError("solve_grouped: every device must have the same block size")
+    keep, probs, outs, results = [], [], [], []
+    for q, d in enumerate(devices):
+        if hamiltonians is not None:
+            h_diag, h_upper = hamiltonians[q]
+        else:
+            h_diag = torch.from_numpy(d.h_diag).to(dev)
+            h_upper = torch.from_numpy(d.h_upper).to(dev)
+        e = energies[q]
+        e = e if isinstance(e, torch.Tensor) else torch.as_tensor(np.asarray(e, dtype=np.float64))
+        e = e.to(device=dev, dtype=torch.float64).contiguous()
+        out = allocate_outputs(d.num_blocks, b, int(e.shape[0]), keys, cuda)
+        keep.append((h_diag, h_upper, e))
+        results.append(out)
+        probs.append(_lib.TransportProblem(
+            num_blocks=d.num_blocks, block_size=b, num_energies=int(e.shape[0]), h_diag=h_diag.data_ptr(),
+            h_upper=h_upper.data_ptr(), energies=e.data_ptr(), eta=d.eta, mu_left=d.mu_left, mu_right=d.mu_right,
+            kt=d.kt, sr_tol=d.sr_tol, sr_max_iterations=d.sr_max_iter, max_batch_size=0))
+        outs.append(_lib.TransportOutputs(**{k: (out[k].data_ptr() if k in out else None) for k in OUTPUT_KEYS}))
+    p_arr = (_lib.TransportProblem * len(probs))(*probs)
+    o_arr = (_lib.TransportOutputs * len(outs))(*outs)
+    lib = _lib.load()
+    ctx = ctx if ctx is not None else _lib.context(cuda)
+    if stream is None:
+        s = torch.cuda.current_stream(cuda).cuda_stream
+    else:
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+    st = lib.qtx_transport_solve_grouped(ctx, len(probs), p_arr, o_arr, _lib.QTX_PREC_FP64, 0, s)
+    _lib.check(st, ctx, "transport_solve_grouped")
+    return results

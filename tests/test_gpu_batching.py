@@ -16,7 +16,7 @@ from quatrex_b200 import _lib
 from quatrex_b200.autotune import Autotuner
 from quatrex_b200.batching import BatchedTransport, Instance, OBSERVABLE_KEYS
 from quatrex_b200.serving import TransportServer, poisson_arrivals
-from quatrex_b200.transport import TransportSolver
+from quatrex_b200.transport import TransportSolver, solve_grouped
 from quatrex_b200.workloads import make_device
 
 pytestmark = pytest.mark.gpu
@@ -52,20 +52,33 @@ def test_graph_replay_matches_eager():
     assert lib.qtx_graph_replays(ctx) - r0 == 3
 
 
-def test_uneven_instances_concurrent_streams():
+@pytest.mark.parametrize("group", [False, True])
+def test_uneven_instances_concurrent_streams(group):
+    """With grouping, the b <= 64 instances of each block size share one
+    persistent launch and equal the grouped solve of the instance alone bit for
+    bit (a CTA's energy does not depend on the other pairs of the launch);
+    larger instances, and every instance without grouping, equal the layered
+    solve alone."""
     tuner = Autotuner(candidates_ne=(8,), repeats=1)
     insts = [Instance(make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=10 + i), None)
-             for i, (nb, b, ne) in enumerate([(4, 16, 12), (7, 32, 9), (5, 64, 8), (3, 48, 17), (9, 16, 20)])]
+             for i, (nb, b, ne) in enumerate([(4, 16, 12), (7, 32, 9), (5, 64, 8), (3, 48, 17), (9, 16, 20),
+                                              (3, 128, 6), (6, 64, 5)])]
     for x in insts:
         x.energies = x.device.energies
-    bt = BatchedTransport(precision="fp64", streams=3, tuner=tuner)
+    bt = BatchedTransport(precision="fp64", streams=3, tuner=tuner, group_small=group)
     try:
         res = bt.run(insts)
     finally:
         bt.close()
     for x, r in zip(insts, res):
-        ne_call = tuner.best(x.device.block_size, len(x.energies), "fp64")["energies_per_call"]
-        _close(r, _alone(x.device, x.energies, ne_call))
+        assert r["grouped"] == (group and x.device.block_size <= 64)
+        if r["grouped"]:
+            alone = solve_grouped([x.device], [x.energies], keys=OBSERVABLE_KEYS)[0]
+            for k in OBSERVABLE_KEYS:
+                assert np.array_equal(r[k], alone[k].cpu().numpy()), k
+        else:
+            ne_call = tuner.best(x.device.block_size, len(x.energies), "fp64")["energies_per_call"]
+            _close(r, _alone(x.device, x.energies, ne_call))
 
 
 def test_server_results_same_alone_and_in_mix():
