@@ -5,7 +5,12 @@ runs the batched complex GEMM of one RGF block product (b x b x b, ``batch``
 energies) ``launches`` times after one warm-up launch and prints the mean
 device time and TFLOP/s (8 b^3 flops per complex product).  ``inv`` does the
 same for the batched block inverse (8 b^3 flops per block), ``sr`` for one
-Sancho-Rubio solve.  The same invocations are the targets of the ncu captures
+Sancho-Rubio solve.  ``grouped --b 32 --instances 6`` times the grouped
+transport solve (one persistent launch for every energy of several seeded
+devices of one block size, nb uniform in [8, 128], 64-512 energies; with
+``--instances 1`` the single device nb=22 / 467 energies or, at b = 32,
+nb=12 / 456 energies) against the layered solve of the same devices one after
+the other, each after one warm-up call, with device-resident inputs.  The same invocations are the targets of the ncu captures
 summarised under profiles/.  Inputs are seeded, in HBM, and larger than L2 for
 the default shapes (3 x 128 MiB operands at b = 256).
 """
@@ -108,6 +113,44 @@ def bench_sr(b: int, batch: int, launches: int) -> dict:
             "tflops": 8.0 * b ** 3 * batch * (7 * it + 1) / ms / 1e9}
 
 
+def bench_grouped(b: int, instances: int) -> dict:
+    import time
+
+    from quatrex_b200.batching import OBSERVABLE_KEYS
+    from quatrex_b200.transport import TransportSolver, solve_grouped
+    from quatrex_b200.workloads import make_device
+
+    if instances == 1:
+        specs = [(22, 467)] if b > 32 else [(12, 456)]
+    else:
+        rng = np.random.default_rng(0 if b == 32 else 1)
+        specs = [(int(rng.integers(8, 129)), int(rng.integers(64, 513))) for _ in range(instances)]
+    devs = [make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=900 + q) for q, (nb, ne) in enumerate(specs)]
+    hs = [(torch.from_numpy(d.h_diag).cuda(), torch.from_numpy(d.h_upper).cuda()) for d in devs]
+    es = [torch.from_numpy(d.energies).cuda() for d in devs]
+    solves = sum(ne for _, ne in specs)
+
+    def grouped():
+        return solve_grouped(devs, es, keys=OBSERVABLE_KEYS, hamiltonians=hs)
+
+    sols = [TransportSolver(d, max_batch_size=256, h_diag=h[0], h_upper=h[1]) for d, h in zip(devs, hs)]
+
+    def layered():
+        return [s.solve(e, keys=OBSERVABLE_KEYS) for s, e in zip(sols, es)]
+
+    out = {}
+    for name, fn in (("grouped", grouped), ("layered", layered)):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        out[name] = time.perf_counter() - t0
+    return {"kernel": "transport_grouped", "b": b, "instances": [list(x) for x in specs], "solves": solves,
+            "grouped_s": out["grouped"], "layered_s": out["layered"],
+            "grouped_solves_per_s": solves / out["grouped"], "layered_solves_per_s": solves / out["layered"]}
+
+
 def probe_fp64_peak() -> dict:
     lib = _lib.load()
     out = {}
@@ -123,7 +166,8 @@ def probe_fp64_peak() -> dict:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="fixed-shape kernel timing")
-    ap.add_argument("kernel", choices=["gemm", "gemm_h", "inv", "sr", "fp64peak"])
+    ap.add_argument("kernel", choices=["gemm", "gemm_h", "inv", "sr", "fp64peak", "grouped"])
+    ap.add_argument("--instances", type=int, default=6)
     ap.add_argument("--b", type=int, default=256)
     ap.add_argument("--batch", type=int, default=128)
     ap.add_argument("--launches", type=int, default=5)
@@ -138,6 +182,8 @@ def main(argv=None) -> int:
         r = bench_gemm(args.b, args.batch, args.launches, 1, prec)
     elif args.kernel == "inv":
         r = bench_inv(args.b, args.batch, args.launches)
+    elif args.kernel == "grouped":
+        r = bench_grouped(args.b, args.instances)
     else:
         r = bench_sr(args.b, args.batch, args.launches)
     print(json.dumps(r), flush=True)
