@@ -451,7 +451,7 @@ def run_serve(args):
     arrivals = poisson_arrivals(len(reqs), rate_hz=args.rate, seed=7)
     for prec in ("fp64", "mixed"):
         tuner = Autotuner(cache_path=os.path.join(ROOT, "_build", "autotune.json"))
-        server = TransportServer(slots=args.streams, precision=prec, tuner=tuner)
+        server = TransportServer(slots=args.streams, precision=prec, tuner=tuner, group_small=not args.no_group)
         try:
             # warm-up outside the timed region: tune every (b, batch, precision)
             # key the requests use, and run one request of each block size alone
@@ -482,7 +482,9 @@ def run_serve(args):
                           "requests": len(results), "p50_latency_s": float(np.percentile(lat, 50)),
                           "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
                           "peak_concurrency": st["peak_concurrency"], "arrival_rate_hz": args.rate,
-                          "slots": args.streams, "server": "native qtx_server (C++ workers, one stream each)"}),
+                          "slots": args.streams, "server": "native qtx_server (C++ workers, one stream each)",
+                          "grouped_small": not args.no_group,
+                          "grouped_launches": st["grouped_launches"], "grouped_requests": st["grouped_requests"]}),
               flush=True)
     return 0
 
@@ -566,7 +568,7 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serve workload: Poisson arrival rate (1/s)")
     ap.add_argument("--uneven-precision", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--no-group", action="store_true",
-                    help="uneven: solve b <= 64 instances one by one instead of one grouped launch per block size")
+                    help="uneven/serve: solve b <= 64 instances (requests) one by one instead of grouped launches")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--energies-per-step", type=int, default=0,
                     help="energies per step (0: one per SM of the device)")

@@ -241,11 +241,16 @@ qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, con
  * sweeps, observables); pairs are handed out longest problem first.
  * max_batch_size is ignored.  precision must be QTX_PREC_FP64 (the INT8
  * split products only pay off at b >= 512).  Synchronous (returns when the
- * outputs are written); QTX_E_NOT_CONVERGED as for qtx_transport_solve;
- * QTX_E_UNSUPPORTED for b > 64, QTX_E_INVAL for mixed block sizes. */
+ * outputs are written).  statuses (host, count entries, may be NULL) receives
+ * each problem's own status: QTX_OK, QTX_E_NOT_CONVERGED (a lead's
+ * Sancho-Rubio iteration hit sr_max_iterations; outputs written) or
+ * QTX_E_SINGULAR (an exactly singular diagonal block; that problem's outputs
+ * hold inf/NaN).  The return value is the worst of them (QTX_E_SINGULAR before
+ * QTX_E_NOT_CONVERGED), or QTX_E_UNSUPPORTED for b > 64, QTX_E_INVAL for mixed
+ * block sizes or a bad problem. */
 qtx_status qtx_transport_solve_grouped(qtx_ctx* ctx, int32_t count, const qtx_transport_problem* problems,
                                        const qtx_transport_outputs* outputs, int32_t precision, uint32_t flags,
-                                       qtx_stream stream);
+                                       qtx_status* statuses, qtx_stream stream);
 
 /* Device bytes one qtx_transport_solve_grouped call allocates (descriptors
  * and one work space per resident CTA); H and the outputs are the caller's.
@@ -293,7 +298,11 @@ size_t qtx_transport_footprint(int32_t num_blocks, int32_t block_size, int64_t e
  * requests in arrival order.  The oldest waiting request is admitted as soon
  * as a slot is free and its footprint (qtx_transport_footprint) fits in
  * `memory_budget` next to the running requests, so requests that arrive while
- * others run overlap with them on the device.  A request whose footprint
+ * others run overlap with them on the device.  With group_max_block_size > 0,
+ * a worker that admits an FP64 request of block size b <= group_max_block_size
+ * (<= 64) also takes every waiting FP64 request of the same b that fits the
+ * budget, and solves them together in one qtx_transport_solve_grouped launch;
+ * each still completes with its own status.  A request whose footprint
  * exceeds the whole budget is refused at submission (QTX_E_NOMEM).  The
  * problem's device arrays (H, energies) and the outputs belong to the caller
  * and must stay valid until the request has completed.
@@ -304,6 +313,7 @@ typedef struct qtx_server_config {
   int32_t device;
   int32_t slots;          /* concurrent requests (>= 1) */
   size_t memory_budget;   /* device bytes the running requests may hold; 0 = half of the free memory */
+  int32_t group_max_block_size;  /* 0: every request alone; else group requests of b <= this (max 64) */
 } qtx_server_config;
 
 typedef struct qtx_server_stats {
@@ -311,6 +321,8 @@ typedef struct qtx_server_stats {
   int64_t solves;             /* energies of the completed requests */
   size_t memory_in_use;       /* footprint of the running requests */
   double p50_latency_s, p99_latency_s, mean_latency_s;  /* completion - submission */
+  int64_t grouped_launches;   /* qtx_transport_solve_grouped launches */
+  int64_t grouped_requests;   /* requests solved in them */
 } qtx_server_stats;
 
 qtx_status qtx_server_create(const qtx_server_config* cfg, qtx_server** out);

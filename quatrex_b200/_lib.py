@@ -100,7 +100,8 @@ class TransportOutputs(ctypes.Structure):
 
 
 class ServerConfig(ctypes.Structure):
-    _fields_ = [("device", c_int32), ("slots", c_int32), ("memory_budget", ctypes.c_size_t)]
+    _fields_ = [("device", c_int32), ("slots", c_int32), ("memory_budget", ctypes.c_size_t),
+                ("group_max_block_size", c_int32)]
 
 
 class ServerStats(ctypes.Structure):
@@ -108,6 +109,7 @@ class ServerStats(ctypes.Structure):
         ("submitted", c_int64), ("completed", c_int64), ("failed", c_int64), ("queued", c_int64),
         ("running", c_int64), ("peak_running", c_int64), ("solves", c_int64), ("memory_in_use", ctypes.c_size_t),
         ("p50_latency_s", c_double), ("p99_latency_s", c_double), ("mean_latency_s", c_double),
+        ("grouped_launches", c_int64), ("grouped_requests", c_int64),
     ]
 
 
@@ -172,7 +174,7 @@ SIGNATURES = {
     "qtx_transport_solve_grouped": (
         c_int32,
         [c_void_p, c_int32, ctypes.POINTER(TransportProblem), ctypes.POINTER(TransportOutputs), c_int32, c_uint32,
-         c_void_p],
+         ctypes.POINTER(c_int32), c_void_p],
     ),
     "qtx_transport_grouped_footprint": (
         ctypes.c_size_t, [c_int32, ctypes.POINTER(c_int32), ctypes.POINTER(c_int64), c_int32]),

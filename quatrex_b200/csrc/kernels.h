@@ -126,8 +126,9 @@ constexpr int GROUPED_MAX_B = 64;
 // than fit on the device at once), and the work-space elements of one CTA.
 int grouped_grid(int b, int64_t items);
 int64_t grouped_ws_elems(int max_nb, int b);
-// flags (device int, zeroed by the caller): bit 0 a zero pivot in a sweep
-// inverse, bit 1 a Sancho-Rubio iteration that did not converge.
+// flags (device ints [1 + count], zeroed by the caller): bit 0 a zero pivot in
+// a sweep inverse, bit 1 a Sancho-Rubio iteration that did not converge;
+// flags[0] for the whole launch, flags[1 + q] for problem q.
 void launch_transport_grouped(int b, const GroupedProblem* problems, int count, int64_t items,
                               unsigned long long* counter, int* flags, cplx* ws, int64_t ws_elems, int max_nb, int grid,
                               cudaStream_t stream);

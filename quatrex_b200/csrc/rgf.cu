@@ -1140,6 +1140,7 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
 // ---------------------------------------------------------------------------
 struct GroupedPlan {
   std::vector<GroupedProblem> problems;  // longest first
+  std::vector<int> source;               // index of each in the caller's array
   int64_t items = 0;
   int max_nb = 0, b = 0;
 };
@@ -1192,39 +1193,51 @@ GroupedPlan grouped_plan(int32_t count, const qtx_transport_problem* p, const qt
     g.sr_iterations = y.sr_iterations;
     plan.items += x.num_energies;
     plan.max_nb = std::max(plan.max_nb, x.num_blocks);
-    if (x.num_energies > 0) plan.problems.push_back(g);
+    if (x.num_energies > 0) {
+      plan.problems.push_back(g);
+      plan.source.push_back(q);
+    }
   }
   return plan;
 }
 
+// descriptors | work counter and flags | per-CTA work spaces
+size_t grouped_desc_bytes(const GroupedPlan& plan) {
+  return (sizeof(GroupedProblem) * plan.problems.size() + 255) / 256 * 256;
+}
+size_t grouped_flag_bytes(const GroupedPlan& plan) {
+  return (64 + sizeof(int) * (1 + plan.problems.size()) + 255) / 256 * 256;
+}
 size_t grouped_bytes(const GroupedPlan& plan, int grid) {
-  const size_t desc = (sizeof(GroupedProblem) * plan.problems.size() + 255) / 256 * 256;
-  return desc + 256 + sizeof(cplx) * (size_t)grid * (size_t)grouped_ws_elems(plan.max_nb, plan.b);
+  return grouped_desc_bytes(plan) + grouped_flag_bytes(plan) +
+         sizeof(cplx) * (size_t)grid * (size_t)grouped_ws_elems(plan.max_nb, plan.b);
 }
 
-// Returns the device flags (bit 1: a lead did not converge); throws on a zero pivot.
-int transport_grouped_impl(qtx_ctx* ctx, int32_t count, const qtx_transport_problem* p,
-                           const qtx_transport_outputs* o, cudaStream_t s) {
+// Returns the flags of the caller's problems (count entries; bit 0 a zero
+// pivot, bit 1 a lead that did not converge).
+std::vector<int> transport_grouped_impl(int32_t count, const qtx_transport_problem* p,
+                                        const qtx_transport_outputs* o, cudaStream_t s) {
   GroupedPlan plan = grouped_plan(count, p, o);
-  if (plan.items == 0) return 0;
+  std::vector<int> out(count, 0);
+  if (plan.items == 0) return out;
   const int grid = grouped_grid(plan.b, plan.items);
   DevBuf mem(grouped_bytes(plan, grid), s);
   char* base = mem.as<char>();
-  const size_t desc = (sizeof(GroupedProblem) * plan.problems.size() + 255) / 256 * 256;
+  const size_t desc = grouped_desc_bytes(plan);
   GroupedProblem* d_problems = reinterpret_cast<GroupedProblem*>(base);
   unsigned long long* counter = reinterpret_cast<unsigned long long*>(base + desc);
   int* flags = reinterpret_cast<int*>(base + desc + 64);
-  cplx* ws = reinterpret_cast<cplx*>(base + desc + 256);
+  cplx* ws = reinterpret_cast<cplx*>(base + desc + grouped_flag_bytes(plan));
   QTX_CUDA_TRY(cudaMemcpyAsync(d_problems, plan.problems.data(), sizeof(GroupedProblem) * plan.problems.size(),
                                cudaMemcpyHostToDevice, s));
-  QTX_CUDA_TRY(cudaMemsetAsync(base + desc, 0, 256, s));
+  QTX_CUDA_TRY(cudaMemsetAsync(base + desc, 0, grouped_flag_bytes(plan), s));
   launch_transport_grouped(plan.b, d_problems, (int)plan.problems.size(), plan.items, counter, flags, ws,
                            grouped_ws_elems(plan.max_nb, plan.b), plan.max_nb, grid, s);
-  QTX_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+  std::vector<int> h_flags(1 + plan.problems.size());
+  QTX_CUDA_TRY(cudaMemcpyAsync(h_flags.data(), flags, sizeof(int) * h_flags.size(), cudaMemcpyDeviceToHost, s));
   QTX_CUDA_TRY(cudaStreamSynchronize(s));
-  const int fl = ctx->h_pinned[0];
-  if (fl & 1) throw QtxError(QTX_E_SINGULAR, "qtx_transport_solve_grouped: exactly singular diagonal block");
-  return fl;
+  for (size_t k = 0; k < plan.problems.size(); ++k) out[plan.source[k]] = h_flags[1 + k];
+  return out;
 }
 
 // ---------------------------------------------------------------------------
@@ -1909,20 +1922,36 @@ qtx_status qtx_obc_assemble(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
 
 qtx_status qtx_transport_solve_grouped(qtx_ctx* ctx, int32_t count, const qtx_transport_problem* problems,
                                        const qtx_transport_outputs* outputs, int32_t precision, uint32_t flags,
-                                       qtx_stream stream) {
-  int fl = 0;
+                                       qtx_status* statuses, qtx_stream stream) {
+  std::vector<int> fl;
   qtx_status st = guarded(ctx, [&] {
     if (count < 1 || !problems || !outputs) throw QtxError(QTX_E_INVAL, "qtx_transport_solve_grouped: no problems");
     if (precision != QTX_PREC_FP64)
       throw QtxError(QTX_E_UNSUPPORTED, "qtx_transport_solve_grouped: FP64 products only");
     (void)flags;
-    fl = transport_grouped_impl(ctx, count, problems, outputs, reinterpret_cast<cudaStream_t>(stream));
+    fl = transport_grouped_impl(count, problems, outputs, reinterpret_cast<cudaStream_t>(stream));
   });
-  if (st == QTX_OK && (fl & 2)) {
+  if (st != QTX_OK) {
+    if (statuses)
+      for (int q = 0; q < count; ++q) statuses[q] = st;
+    return st;
+  }
+  bool singular = false, unconverged = false;
+  for (int q = 0; q < count; ++q) {
+    const qtx_status s = (fl[q] & 1) ? QTX_E_SINGULAR : ((fl[q] & 2) ? QTX_E_NOT_CONVERGED : QTX_OK);
+    if (statuses) statuses[q] = s;
+    singular = singular || s == QTX_E_SINGULAR;
+    unconverged = unconverged || s == QTX_E_NOT_CONVERGED;
+  }
+  if (singular) {
+    ctx->last_error = "qtx_transport_solve_grouped: exactly singular diagonal block";
+    return QTX_E_SINGULAR;
+  }
+  if (unconverged) {
     ctx->last_error = "Surface Green's function did not converge.";
     return QTX_E_NOT_CONVERGED;
   }
-  return st;
+  return QTX_OK;
 }
 
 size_t qtx_transport_grouped_footprint(int32_t count, const int32_t* num_blocks, const int64_t* num_energies,

@@ -550,7 +550,8 @@ __device__ __noinline__ int cta_sancho_rubio(int n, double energy, double eta, c
 // The whole transport solve of energy e of problem P (transport_contacts and
 // transport_sweep of rgf.cu for one energy).
 template <int BT>
-__device__ __noinline__ void solve_energy(const GroupedProblem* P, int64_t e, cplx* ws, int max_nb, int* flags) {
+__device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int64_t e, cplx* ws, int max_nb,
+                                          int* flags) {
   const int nb = P->nb, n = P->b;
   const int64_t bb = (int64_t)n * n;
   auto XR = [&](int i) { return ws + i * bb; };
@@ -583,7 +584,10 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int64_t e, cp
       P->sr_iterations[2 * e] = its_l < 0 ? -its_l : its_l;
       P->sr_iterations[2 * e + 1] = its_r < 0 ? -its_r : its_r;
     }
-    if (its_l < 0 || its_r < 0) atomicOr(flags, 2);
+    if (its_l < 0 || its_r < 0) {
+      atomicOr(flags, 2);
+      atomicOr(flags + 1 + pidx, 2);
+    }
   }
   GArgs a = g0;  // Sigma^R_L = A_10 g_L A_01 = (-U_0^H) g_L (-U_0)
   a.a = uu(0); a.opa = OP_C; a.b = Cb[0]; a.d = T[1]; a.alpha = MONE;
@@ -769,7 +773,10 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int64_t e, cp
     const cplx tr = cta_sum<BT>(acc);
     if (threadIdx.x == 0) P->transmission[e] = tr.x;
   }
-  if (zero && threadIdx.x == 0) atomicOr(flags, 1);
+  if (zero && threadIdx.x == 0) {
+    atomicOr(flags, 1);
+    atomicOr(flags + 1 + pidx, 1);
+  }
 }
 
 template <int BT>
@@ -791,7 +798,7 @@ __global__ void __launch_bounds__(GCfg<BT>::THREADS, GCfg<BT>::MIN_BLOCKS)
       if (problems[mid].item0 <= item) lo = mid;
       else hi = mid;
     }
-    solve_energy<BT>(problems + lo, item - problems[lo].item0, my_ws, max_nb, flags);
+    solve_energy<BT>(problems + lo, lo, item - problems[lo].item0, my_ws, max_nb, flags);
   }
 }
 

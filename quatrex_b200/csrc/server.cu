@@ -7,9 +7,13 @@
 // soon as its footprint (qtx_transport_footprint at the request's energies per
 // call) fits in the memory budget next to the requests already running, runs
 // qtx_transport_solve on its stream and synchronises that stream only.
-// Requests admitted while others run overlap with them on the device.  Nothing
-// here synchronises the whole device.  Latency = completion - submission
-// (steady clock); every completed request's latency is kept for p50/p99.
+// Requests admitted while others run overlap with them on the device.  With
+// grouping on, a worker that admits an FP64 request of a small block size
+// also takes the waiting FP64 requests of the same block size that fit the
+// budget (arrival order) and solves them in one qtx_transport_solve_grouped
+// launch (one persistent kernel for all their energies).  Nothing here
+// synchronises the whole device.  Latency = completion - submission (steady
+// clock); every completed request's latency is kept for p50/p99.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -27,6 +31,8 @@
 #include "../../include/qtx_rgf.h"
 
 namespace {
+
+constexpr int kMaxGroup = 256;  // requests per grouped launch
 
 using Clock = std::chrono::steady_clock;
 
@@ -59,12 +65,46 @@ struct qtx_server {
   std::vector<double> latencies;
   int64_t next_id = 1;
   int64_t submitted = 0, completed = 0, failed = 0, running = 0, peak_running = 0, solves = 0;
+  int64_t grouped_launches = 0, grouped_requests = 0;
   size_t in_use = 0;
   bool closing = false;
   int start_errors = 0;
 };
 
 namespace {
+
+bool groupable(const qtx_server* srv, const Request& r) {
+  const int gmax = std::min(srv->cfg.group_max_block_size, 64);
+  return gmax > 0 && r.precision == QTX_PREC_FP64 && r.p.block_size <= gmax;
+}
+
+size_t group_footprint(const std::vector<std::shared_ptr<Request>>& g) {
+  std::vector<int32_t> nbs;
+  std::vector<int64_t> nes;
+  for (const auto& r : g) {
+    nbs.push_back(r->p.num_blocks);
+    nes.push_back(r->p.num_energies);
+  }
+  return qtx_transport_grouped_footprint((int32_t)g.size(), nbs.data(), nes.data(), g[0]->p.block_size);
+}
+
+// Complete one request (lock held).
+void finish(qtx_server* srv, const std::shared_ptr<Request>& req, qtx_status st, const std::string& err,
+            double lat) {
+  req->done = true;
+  req->status = st;
+  req->latency_s = lat;
+  if (st != QTX_OK && st != QTX_E_NOT_CONVERGED) {
+    req->error = err;
+    ++srv->failed;
+  } else {
+    if (st == QTX_E_NOT_CONVERGED) req->error = err;
+    ++srv->completed;
+    srv->solves += req->p.num_energies;
+    srv->latencies.push_back(lat);
+  }
+  srv->completed_uncollected.push_back(req->id);
+}
 
 void worker_main(qtx_server* srv) {
   qtx_ctx* ctx = nullptr;
@@ -77,7 +117,9 @@ void worker_main(qtx_server* srv) {
     ++srv->start_errors;
   }
   for (;;) {
-    std::shared_ptr<Request> req;
+    std::vector<std::shared_ptr<Request>> group;
+    size_t fp = 0;
+    bool grouped = false;
     {
       std::unique_lock<std::mutex> lk(srv->m);
       srv->cv_work.wait(lk, [&] {
@@ -86,40 +128,66 @@ void worker_main(qtx_server* srv) {
         return srv->running == 0 || srv->in_use + head->footprint <= srv->budget;
       });
       if (srv->queue.empty()) break;  // closing and drained
-      req = srv->queue.front();
+      std::shared_ptr<Request> head = srv->queue.front();
       srv->queue.pop_front();
-      srv->in_use += req->footprint;
-      ++srv->running;
+      group.push_back(head);
+      fp = head->footprint;
+      if (groupable(srv, *head)) {
+        grouped = true;
+        // the waiting requests of the same block size, in arrival order, while
+        // the group's work space fits next to the running requests
+        for (auto it = srv->queue.begin(); it != srv->queue.end() && (int)group.size() < kMaxGroup;) {
+          const auto& r = *it;
+          if (!groupable(srv, *r) || r->p.block_size != head->p.block_size) {
+            ++it;
+            continue;
+          }
+          group.push_back(r);
+          const size_t need = std::max(fp, group_footprint(group));
+          if (srv->in_use + need > srv->budget) {
+            group.pop_back();
+            break;
+          }
+          fp = need;
+          it = srv->queue.erase(it);
+        }
+      }
+      srv->in_use += fp;
+      srv->running += (int64_t)group.size();
       srv->peak_running = std::max(srv->peak_running, srv->running);
     }
-    qtx_status st = QTX_E_CUDA;
+    std::vector<qtx_status> st(group.size(), QTX_E_CUDA);
     std::string err = "server worker could not create its context or stream";
-    if (ok) {
-      st = qtx_transport_solve(ctx, &req->p, &req->o, req->precision, req->flags, stream);
-      if (st != QTX_OK) err = qtx_last_error(ctx);
-      if (cudaStreamSynchronize(stream) != cudaSuccess && st == QTX_OK) {
-        st = QTX_E_CUDA;
-        err = cudaGetErrorString(cudaGetLastError());
+    if (ok && grouped) {
+      std::vector<qtx_transport_problem> ps;
+      std::vector<qtx_transport_outputs> os;
+      for (const auto& r : group) {
+        ps.push_back(r->p);
+        os.push_back(r->o);
       }
+      const qtx_status s = qtx_transport_solve_grouped(ctx, (int32_t)group.size(), ps.data(), os.data(),
+                                                       QTX_PREC_FP64, 0, st.data(), stream);
+      if (s != QTX_OK) err = qtx_last_error(ctx);
+    } else if (ok) {
+      st[0] = qtx_transport_solve(ctx, &group[0]->p, &group[0]->o, group[0]->precision, group[0]->flags, stream);
+      if (st[0] != QTX_OK) err = qtx_last_error(ctx);
     }
-    const double lat = std::chrono::duration<double>(Clock::now() - req->submitted).count();
+    if (ok && cudaStreamSynchronize(stream) != cudaSuccess) {
+      err = cudaGetErrorString(cudaGetLastError());
+      for (auto& s : st)
+        if (s == QTX_OK) s = QTX_E_CUDA;
+    }
+    const auto now = Clock::now();
     {
       std::lock_guard<std::mutex> lk(srv->m);
-      req->done = true;
-      req->status = st;
-      req->latency_s = lat;
-      if (st != QTX_OK && st != QTX_E_NOT_CONVERGED) {
-        req->error = err;
-        ++srv->failed;
-      } else {
-        if (st == QTX_E_NOT_CONVERGED) req->error = err;
-        ++srv->completed;
-        srv->solves += req->p.num_energies;
-        srv->latencies.push_back(lat);
+      for (size_t i = 0; i < group.size(); ++i)
+        finish(srv, group[i], st[i], err, std::chrono::duration<double>(now - group[i]->submitted).count());
+      if (grouped && ok) {
+        ++srv->grouped_launches;
+        srv->grouped_requests += (int64_t)group.size();
       }
-      srv->in_use -= req->footprint;
-      --srv->running;
-      srv->completed_uncollected.push_back(req->id);
+      srv->in_use -= fp;
+      srv->running -= (int64_t)group.size();
     }
     srv->cv_work.notify_all();
     srv->cv_done.notify_all();
@@ -213,6 +281,12 @@ qtx_status qtx_server_submit(qtx_server* srv, const qtx_transport_problem* p, co
   req->flags = flags & ~QTX_FLAG_GRAPH;
   const int64_t ne_call = p->max_batch_size > 0 ? std::min(p->max_batch_size, p->num_energies) : p->num_energies;
   req->footprint = qtx_transport_footprint(p->num_blocks, p->block_size, ne_call, precision);
+  if (groupable(srv, *req)) {
+    // solved in a grouped launch: its work space when it runs alone
+    const int32_t nb = p->num_blocks;
+    const int64_t ne = p->num_energies;
+    req->footprint = std::max(req->footprint, qtx_transport_grouped_footprint(1, &nb, &ne, p->block_size));
+  }
   std::lock_guard<std::mutex> lk(srv->m);
   if (srv->closing) return QTX_E_INVAL;
   if (req->footprint > srv->budget) return QTX_E_NOMEM;
@@ -277,6 +351,8 @@ qtx_status qtx_server_get_stats(qtx_server* srv, qtx_server_stats* st) {
   double sum = 0;
   for (double x : srv->latencies) sum += x;
   st->mean_latency_s = srv->latencies.empty() ? 0.0 : sum / (double)srv->latencies.size();
+  st->grouped_launches = srv->grouped_launches;
+  st->grouped_requests = srv->grouped_requests;
   return QTX_OK;
 }
 

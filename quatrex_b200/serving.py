@@ -6,7 +6,9 @@ Requests (one device, its own energy grid and contacts) arrive at any time.
 native server, whose worker threads (one CUDA stream and library context per
 slot) admit the oldest waiting request as soon as a slot is free and its
 device footprint fits in the budget next to the running ones; admitted
-requests overlap on the GPU while new ones keep arriving.  A request's state
+requests overlap on the GPU while new ones keep arriving.  Waiting FP64
+requests of one block size <= 64 are taken together and solved in one
+persistent launch (every energy of every request one work item).  A request's state
 (H, the energy-call work space, outputs) stays on the device until it
 completes; only its observables come back.  Latency = completion time -
 submission time, measured by the native server.
@@ -41,10 +43,13 @@ class TransportServer:
         together (default: half of the free memory at start).
     precision : "fp64" or "mixed" (for "mixed" the autotuner may still pick
         the FP64 products for a block size where they are faster).
+    group_small : waiting FP64 requests of one block size <= 64 are solved
+        together in one persistent launch (qtx_transport_solve_grouped).
     """
 
     def __init__(self, slots: int = 4, memory_budget: int | None = None, precision: str = "fp64",
-                 tuner: Autotuner | None = None, cuda_device: int | None = None, keys=OBSERVABLE_KEYS):
+                 tuner: Autotuner | None = None, cuda_device: int | None = None, keys=OBSERVABLE_KEYS,
+                 group_small: bool = True):
         if not torch.cuda.is_available():
             raise RuntimeError("quatrex_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
         self.cuda = torch.cuda.current_device() if cuda_device is None else cuda_device
@@ -56,7 +61,8 @@ class TransportServer:
         self.tuner = tuner if tuner is not None else Autotuner()
         self.keys = tuple(keys)
         self._lib = _lib.load()
-        cfg = _lib.ServerConfig(device=self.cuda, slots=max(1, int(slots)), memory_budget=self.budget)
+        cfg = _lib.ServerConfig(device=self.cuda, slots=max(1, int(slots)), memory_budget=self.budget,
+                                group_max_block_size=64 if group_small else 0)
         h = ctypes.c_void_p()
         st = self._lib.qtx_server_create(ctypes.byref(cfg), ctypes.byref(h))
         if st != _lib.QTX_OK:
@@ -125,7 +131,8 @@ class TransportServer:
         return {"submitted": st.submitted, "completed": st.completed, "failed": st.failed, "queued": st.queued,
                 "running": st.running, "solves": st.solves, "p50_s": st.p50_latency_s, "p99_s": st.p99_latency_s,
                 "mean_s": st.mean_latency_s, "peak_concurrency": st.peak_running,
-                "memory_in_use": st.memory_in_use}
+                "memory_in_use": st.memory_in_use, "grouped_launches": st.grouped_launches,
+                "grouped_requests": st.grouped_requests}
 
     # -- completions -----------------------------------------------------------
     def _collect(self):

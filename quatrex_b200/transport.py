@@ -187,6 +187,6 @@ def solve_grouped(devices: list[TransportDevice], energies: list, keys=OUTPUT_KE
         s = torch.cuda.current_stream(cuda).cuda_stream
     else:
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
-    st = lib.qtx_transport_solve_grouped(ctx, len(probs), p_arr, o_arr, _lib.QTX_PREC_FP64, 0, s)
+    st = lib.qtx_transport_solve_grouped(ctx, len(probs), p_arr, o_arr, _lib.QTX_PREC_FP64, 0, None, s)
     _lib.check(st, ctx, "transport_solve_grouped")
     return results

@@ -81,12 +81,13 @@ def test_uneven_instances_concurrent_streams(group):
             _close(r, _alone(x.device, x.energies, ne_call))
 
 
-def test_server_results_same_alone_and_in_mix():
+@pytest.mark.parametrize("group", [False, True])
+def test_server_results_same_alone_and_in_mix(group):
     tuner = Autotuner(candidates_ne=(8,), repeats=1)
     rng = np.random.default_rng(1)
     devs = [make_device(num_blocks=int(rng.integers(3, 8)), block_size=int(rng.choice([16, 32, 64])),
                         num_energies=int(rng.integers(5, 20)), seed=100 + i) for i in range(8)]
-    server = TransportServer(slots=3, precision="fp64", tuner=tuner)
+    server = TransportServer(slots=3, precision="fp64", tuner=tuner, group_small=group)
     try:
         arrivals = poisson_arrivals(len(devs), rate_hz=200.0, seed=2)
         t0 = time.perf_counter()
@@ -101,9 +102,16 @@ def test_server_results_same_alone_and_in_mix():
         server.close()
     assert st["completed"] == len(devs)
     assert st["p99_s"] >= st["p50_s"] > 0
+    assert (st["grouped_requests"] == len(devs)) == group and st["grouped_launches"] <= st["grouped_requests"]
     for d, r in zip(devs, results):
-        ne_call = tuner.best(d.block_size, len(d.energies), "fp64")["energies_per_call"]
-        _close(r, _alone(d, d.energies, ne_call))
+        if group:
+            # a grouped launch computes each energy on its own: the mix changes nothing
+            alone = solve_grouped([d], [d.energies], keys=OBSERVABLE_KEYS)[0]
+            for k in OBSERVABLE_KEYS:
+                assert np.array_equal(r[k], alone[k].cpu().numpy()), k
+        else:
+            ne_call = tuner.best(d.block_size, len(d.energies), "fp64")["energies_per_call"]
+            _close(r, _alone(d, d.energies, ne_call))
 
 
 def test_server_rejects_request_above_budget():

@@ -161,6 +161,6 @@ def test_grouped_not_converged_and_refusals():
                               sr_tol=a.sr_tol, sr_max_iterations=a.sr_max_iter, max_batch_size=0)
     o = _lib.TransportOutputs()
     assert lib.qtx_transport_solve_grouped(ctx, 1, ctypes.byref(p), ctypes.byref(o), _lib.QTX_PREC_MIXED, 0,
-                                           None) == _lib.QTX_E_UNSUPPORTED
+                                           None, None) == _lib.QTX_E_UNSUPPORTED
     assert grouped_footprint_bytes([3, 9], [4, 100], 64) > grouped_footprint_bytes([3, 9], [4, 100], 32) > 0
     assert grouped_footprint_bytes([3], [4], 65) == 0

@@ -3,16 +3,18 @@ results equal a direct qtx_transport_solve of the same request, requests are
 collected by id or in completion order, statistics add up, and requests over
 the budget or malformed are refused at submission."""
 
+import contextlib
 import ctypes
 
 import pytest
 import torch
 
 from quatrex_b200 import _lib
-from quatrex_b200.transport import TransportSolver, allocate_outputs
+from quatrex_b200.transport import TransportSolver, allocate_outputs, solve_grouped
 from quatrex_b200.workloads import make_device
 
 pytestmark = pytest.mark.gpu
+_nullcontext = contextlib.nullcontext
 
 KEYS = ("density", "transmission", "current_left", "sr_iterations")
 
@@ -30,9 +32,10 @@ def _outputs(out):
                                     for name, _ in _lib.TransportOutputs._fields_})
 
 
-def _server(slots=3, budget=0):
+def _server(slots=3, budget=0, group=0):
     lib = _lib.load()
-    cfg = _lib.ServerConfig(device=torch.cuda.current_device(), slots=slots, memory_budget=budget)
+    cfg = _lib.ServerConfig(device=torch.cuda.current_device(), slots=slots, memory_budget=budget,
+                            group_max_block_size=group)
     h = ctypes.c_void_p()
     assert lib.qtx_server_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.QTX_OK
     return lib, h.value
@@ -107,3 +110,52 @@ def test_native_server_refuses_over_budget_and_bad_requests():
     finally:
         assert lib.qtx_server_destroy(srv) == 0
 
+
+
+def test_native_server_groups_waiting_small_requests():
+    """One slot, busy with a b=128 request while five small ones arrive: the
+    three b=32 requests then run in one grouped launch, the b=16 one in
+    another, each with its own status (one of the b=32 requests cannot
+    converge in one Sancho-Rubio iteration) and results equal to the grouped
+    solve of the request alone."""
+    lib, srv = _server(slots=1, group=64)
+    specs = [(24, 128, 48, 200), (5, 32, 9, 200), (7, 32, 6, 1), (3, 16, 5, 200), (4, 32, 11, 200),
+             (6, 16, 4, 200)]
+    keep, ids = [], []
+    try:
+        for i, (nb, b, ne, max_it) in enumerate(specs):
+            d = make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=60 + i)
+            d.sr_max_iter = max_it
+            h_diag = torch.from_numpy(d.h_diag).cuda()
+            h_upper = torch.from_numpy(d.h_upper).cuda()
+            e = torch.from_numpy(d.energies).cuda()
+            out = allocate_outputs(nb, b, ne, KEYS, torch.cuda.current_device())
+            keep.append((d, out, h_diag, h_upper, e))
+        torch.cuda.synchronize()
+        for d, out, h_diag, h_upper, e in keep:
+            p, o = _problem(d, h_diag, h_upper, e, 64), _outputs(out)
+            keep[len(ids)] += (p, o)
+            rid = ctypes.c_int64()
+            assert lib.qtx_server_submit(srv, ctypes.byref(p), ctypes.byref(o), _lib.QTX_PREC_FP64, 0,
+                                         ctypes.byref(rid)) == _lib.QTX_OK
+            ids.append(rid.value)
+        statuses = []
+        for rid in ids:
+            status, lat = ctypes.c_int32(), ctypes.c_double()
+            assert lib.qtx_server_wait(srv, rid, -1, ctypes.byref(status), ctypes.byref(lat), None, 0) == 0
+            statuses.append(status.value)
+        stats = _lib.ServerStats()
+        assert lib.qtx_server_get_stats(srv, ctypes.byref(stats)) == 0
+    finally:
+        assert lib.qtx_server_destroy(srv) == 0
+    assert statuses == [_lib.QTX_OK, _lib.QTX_OK, _lib.QTX_E_NOT_CONVERGED, _lib.QTX_OK, _lib.QTX_OK, _lib.QTX_OK]
+    assert stats.grouped_launches == 2 and stats.grouped_requests == 5
+    assert stats.completed == 6 and stats.failed == 0
+    for (d, out, *_), (nb, b, ne, max_it) in zip(keep, specs):
+        if b > 64:
+            ref = TransportSolver(d, max_batch_size=64).solve(d.energies, keys=KEYS)
+        else:
+            with pytest.warns(RuntimeWarning) if max_it == 1 else _nullcontext():
+                ref = solve_grouped([d], [d.energies], keys=KEYS)[0]
+        for k in KEYS:
+            assert torch.equal(out[k], ref[k]), (b, k)
