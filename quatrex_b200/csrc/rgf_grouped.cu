@@ -55,7 +55,9 @@ template <int BT>
 struct Misc {
   double red_v[2][GCfg<BT>::NWARPS];
   int red_i[2][GCfg<BT>::NWARPS];
-  int pos2row[BT], row2pos[BT], perm[BT], colsrc[BT], colinv[BT];
+  cplx red_piv[2][GCfg<BT>::NWARPS];  // column-k entry of each warp's candidate
+  int pivs[BT];  // pivot row of each step
+  int pos[BT];   // step at which each row was the pivot
   double sum[2 * GCfg<BT>::NWARPS];
   unsigned long long item;
 };
@@ -254,12 +256,25 @@ __device__ __forceinline__ void argmax_combine(double& v, int& i, double v2, int
 
 // X = A^-1 (n x n, n <= BT; X must not alias A).  Returns 0, or 1 + the first
 // column whose pivot is exactly zero (the result then holds inf/NaN).
+//
+// Rows stay where they are (implicit pivoting): step k picks pivot row p_k
+// among the rows not used yet and stores the elimination in place.  The
+// row-swapping form would hold row p_k at position k, so with pos(r) the step
+// at which row r was the pivot, X[pos(r)][p_c] = M[r][c]: every thread writes
+// its own elements once, through the pivot list and its inverse.
+//
+// The in-place step is x_rc <- x_rc - (x_rk / piv) p_c for c != k and
+// -x_rk / piv at c = k.  The staged pivot row carries 1 at column k and every
+// row clears its own column-k entry when it reads it, so one branch-free
+// x - fd p covers both (the pivot row's own entries p_c / piv likewise); the
+// pivot value itself travels through shared memory.
 template <int BT>
 __device__ __noinline__ int cta_inverse(const cplx* A, cplx* X, int n) {
   using C = GCfg<BT>;
   cplx* cand = smem_region<BT>();
   Misc<BT>* ms = smem_misc<BT>();
   constexpr int TPR = C::TPR, CPT = C::CPT;
+  constexpr int ROWS_PER_WARP = 32 / TPR;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r_own = tid / TPR, c_own = tid % TPR;
   const int grp0 = lane - c_own;  // first lane of this row's group
@@ -269,111 +284,92 @@ __device__ __noinline__ int cta_inverse(const cplx* A, cplx* X, int n) {
     const int c = c_own + j * TPR;
     reg[j] = (r_own < n && c < n) ? A[(int64_t)r_own * n + c] : cmk(0, 0);
   }
-  for (int r = tid; r < n; r += C::THREADS) {
-    ms->pos2row[r] = r;
-    ms->row2pos[r] = r;
-  }
+  // staged rows are written at columns < n only: the rest stays zero, so the
+  // padding columns of every register row stay zero too
+  for (int q = tid; q < C::CAND_ELEMS; q += C::THREADS) cand[q] = cmk(0, 0);
+  __syncthreads();
   bool used = r_own >= n;
   int zero = 0;
 #pragma unroll 1
   for (int kk = 0; kk < n; ++kk) {
+    const int kc = kk % TPR;  // lanes c_own == kc hold column kk
     cplx colv = cmk(0, 0);
 #pragma unroll
     for (int j = 0; j < CPT; ++j)
-      if (c_own + j * TPR == kk) colv = reg[j];
+      if (c_own + j * TPR == kk) {
+        colv = reg[j];
+        reg[j] = cmk(0, 0);
+      }
     double bv = -1.0;
     int bi = n;
-    if (c_own == kk % TPR && !used) {
+    if (c_own == kc && !used) {
       bv = cabs1(colv);
       bi = r_own;
     }
+    // the warp's best row among the lanes holding column kk (lanes that share
+    // c_own differ in the bits above log2(TPR)); then lane kc tells the rest
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
+    for (int off = 16; off >= TPR; off >>= 1) {
       const double v2 = __shfl_xor_sync(0xffffffffu, bv, off);
       const int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
       argmax_combine(bv, bi, v2, i2);
     }
-    const int src = grp0 + kk % TPR;
+    bi = __shfl_sync(0xffffffffu, bi, kc);
+    const int src = grp0 + kc;
     const cplx f = cmk(__shfl_sync(0xffffffffu, colv.x, src), __shfl_sync(0xffffffffu, colv.y, src));
     const int par = kk & 1;
-    cplx* my_cand = cand + (par * C::NWARPS + warp) * BT;
     if (bi < n && r_own == bi) {
+      cplx* my_cand = cand + (par * C::NWARPS + warp) * BT;
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
         const int c = c_own + j * TPR;
         if (c < n) my_cand[c] = reg[j];
       }
+      if (c_own == kc) {
+        my_cand[kk] = cmk(1, 0);
+        ms->red_piv[par][warp] = colv;
+      }
     }
-    if (lane == 0) {
+    if (lane == kc) {
       ms->red_v[par][warp] = bv;
       ms->red_i[par][warp] = bi;
     }
     __syncthreads();  // every warp's candidate row visible
-    double v = ms->red_v[par][0];
-    int p = ms->red_i[par][0], pw = 0;
+    // best over the warps: every group of NWARPS lanes holds all candidates
+    double v = ms->red_v[par][lane % C::NWARPS];
+    int p = ms->red_i[par][lane % C::NWARPS];
 #pragma unroll
-    for (int q = 1; q < C::NWARPS; ++q) {
-      const double vq = ms->red_v[par][q];
-      const int iq = ms->red_i[par][q];
-      if (vq > v || (vq == v && iq < p)) {
-        v = vq;
-        p = iq;
-        pw = q;
-      }
+    for (int off = C::NWARPS / 2; off > 0; off >>= 1) {
+      const double v2 = __shfl_xor_sync(0xffffffffu, v, off);
+      const int i2 = __shfl_xor_sync(0xffffffffu, p, off);
+      argmax_combine(v, p, v2, i2);
     }
+    // the global best is also the best of its own warp, whose row is staged
+    const int pw = p / ROWS_PER_WARP;
     const cplx* prow = cand + (par * C::NWARPS + pw) * BT;
-    const cplx piv = prow[kk];
+    const cplx piv = ms->red_piv[par][pw];
     if (piv.x == 0.0 && piv.y == 0.0 && !zero) zero = kk + 1;
     const cplx d = crecip_pivot(piv);
-    if (tid == 0) {
-      // classic row-swap bookkeeping: position kk takes row p, the displaced
-      // row goes to p's position (recorded for the column unscrambling)
-      const int qpos = ms->row2pos[p], rk = ms->pos2row[kk];
-      ms->pos2row[kk] = p;
-      ms->row2pos[p] = kk;
-      ms->pos2row[qpos] = rk;
-      ms->row2pos[rk] = qpos;
-      ms->perm[kk] = qpos;
-    }
-    if (r_own < n) {
-      if (r_own == p) {
-        used = true;
+    if (tid == 0) ms->pivs[kk] = p;
+    if (r_own == p) {
+      used = true;
 #pragma unroll
-        for (int j = 0; j < CPT; ++j) {
-          const int c = c_own + j * TPR;
-          if (c < n) reg[j] = (c == kk) ? d : cmul(prow[c], d);
-        }
-      } else {
-        const cplx fd = cmul(f, d);
+      for (int j = 0; j < CPT; ++j) reg[j] = cmul(prow[c_own + j * TPR], d);
+    } else {
+      const cplx fd = cmul(f, d);
 #pragma unroll
-        for (int j = 0; j < CPT; ++j) {
-          const int c = c_own + j * TPR;
-          if (c < n) reg[j] = (c == kk) ? cmk(-fd.x, -fd.y) : cfms(fd, prow[c], reg[j]);
-        }
-      }
+      for (int j = 0; j < CPT; ++j) reg[j] = cfms(fd, prow[c_own + j * TPR], reg[j]);
     }
   }
   __syncthreads();
-  if (tid == 0) {
-    for (int c = 0; c < n; ++c) ms->colsrc[c] = c;
-    for (int k = n - 1; k >= 0; --k) {
-      const int q = ms->perm[k];
-      const int tmp = ms->colsrc[k];
-      ms->colsrc[k] = ms->colsrc[q];
-      ms->colsrc[q] = tmp;
-    }
-  }
+  for (int k = tid; k < n; k += C::THREADS) ms->pos[ms->pivs[k]] = k;
   __syncthreads();
-  for (int c = tid; c < n; c += C::THREADS) ms->colinv[ms->colsrc[c]] = c;
-  __syncthreads();
-  // X[i][c] = M[pos2row[i]][colsrc[c]]: row r of M goes to row row2pos[r],
-  // column c' to column colinv[c']
   if (r_own < n) {
-    const int i = ms->row2pos[r_own];
+    const int i = ms->pos[r_own];
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       const int c = c_own + j * TPR;
-      if (c < n) X[(int64_t)i * n + ms->colinv[c]] = reg[j];
+      if (c < n) X[(int64_t)i * n + ms->pivs[c]] = reg[j];
     }
   }
   __syncthreads();

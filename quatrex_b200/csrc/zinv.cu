@@ -75,7 +75,7 @@ inline size_t inv_smem_bytes(int n) {
   size_t panel = (size_t)n * s.wp * sizeof(cplx);
   size_t slabs = (size_t)slab_elems(n, s) * sizeof(cplx);
   size_t ints = (size_t)(3 * n + 32 + 4) * sizeof(int);
-  size_t red = 2 * NWARPS * (sizeof(double) + sizeof(int));
+  size_t red = 2 * NWARPS * (sizeof(double) + sizeof(int) + sizeof(cplx));
   size_t pivrow = (size_t)2 * NWARPS * s.wp * sizeof(cplx);  // pivot candidates, two column parities
   return panel + slabs + ints + red + pivrow + 256;
 }
@@ -117,7 +117,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   // not a multiple of 8 bytes for odd n)
   int* pivs = perm + n;                          // pivot row of each column of the current panel
   double* red_v = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(pivs + 32) + 15) & ~uintptr_t(15));
-  int* red_i = reinterpret_cast<int*>(red_v + 2 * NWARPS);
+  cplx* red_piv = reinterpret_cast<cplx*>(red_v + 2 * NWARPS);  // column-kk entry of each warp's candidate
+  int* red_i = reinterpret_cast<int*>(red_piv + 2 * NWARPS);
   // per warp and column parity: the panel row of the warp's pivot candidate
   cplx* cand = reinterpret_cast<cplx*>(red_i + 2 * NWARPS + 2);
   cand = reinterpret_cast<cplx*>((reinterpret_cast<uintptr_t>(cand) + 15) & ~uintptr_t(15));
@@ -257,13 +258,19 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll kKUnroll
         for (int kk = 0; kk < w; ++kk) {
           const int k = k0 + kk;
+          // each row reads and clears its column-kk entry: the staged pivot
+          // row carries 1 there, so the update below is one x - fd p for
+          // every entry (-fd at column kk) and p d for the pivot row (d at kk)
           cplx colv[RPT];
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
             cplx v = cmk(0, 0);
 #pragma unroll
             for (int j = 0; j < CPT; ++j)
-              if (c_own + j * TPR == kk) v = reg[q][j];
+              if (c_own + j * TPR == kk) {
+                v = reg[q][j];
+                reg[q][j] = cmk(0, 0);
+              }
             colv[q] = v;
           }
           // pivot search: the owner of (r, kk) looks at row r if it is not a pivot yet
@@ -293,6 +300,7 @@ __global__ void __launch_bounds__(THREADS, 1)
           }
           const int par = kk & 1;
           cplx* my_cand = cand + (size_t)(par * NWARPS + warp) * WP;
+          const int slot = par * NWARPS;
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
             if (r_own + q * rstride == bi) {
@@ -301,27 +309,31 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const int c = c_own + j * TPR;
                 if (c < w) my_cand[c] = reg[q][j];
               }
+              if (c_own == kk % TPR) {
+                my_cand[kk] = cmk(1, 0);
+                red_piv[slot + warp] = colv[q];
+              }
             }
           }
-          const int slot = par * NWARPS;
           if (lane == 0) {
             red_v[slot + warp] = bv;
             red_i[slot + warp] = bi;
           }
           __syncthreads();  // S: candidates of every warp visible
-          double v = red_v[slot];
-          int p = red_i[slot], pw = 0;
-          for (int q = 1; q < NWARPS; ++q) {
-            const double vq = red_v[slot + q];
-            const int iq = red_i[slot + q];
-            if (vq > v || (vq == v && iq < p)) {
-              v = vq;
-              p = iq;
-              pw = q;
-            }
+          // best over the warps, lane-parallel: every group of NWARPS lanes
+          // holds all candidates (same choice as a scan in warp order)
+          double v = red_v[slot + lane % NWARPS];
+          int p = red_i[slot + lane % NWARPS];
+#pragma unroll
+          for (int off = NWARPS / 2; off > 0; off >>= 1) {
+            const double v2 = __shfl_xor_sync(0xffffffffu, v, off);
+            const int i2 = __shfl_xor_sync(0xffffffffu, p, off);
+            argmax_combine(v, p, v2, i2);
           }
+          // the global best is the best of the warp that owns row p
+          const int pw = ((p % rstride) * TPR) >> 5;
           const cplx* prow = cand + (size_t)(par * NWARPS + pw) * WP;
-          const cplx piv = prow[kk];
+          const cplx piv = red_piv[slot + pw];
           if (piv.x == 0.0 && piv.y == 0.0 && !zero_pivot) zero_pivot = k + 1;
           const cplx d = crecip_pivot(piv);
           if (tid == 0) pivs[kk] = p;
@@ -334,14 +346,14 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
               for (int j = 0; j < CPT; ++j) {
                 const int c = c_own + j * TPR;
-                if (c < w) reg[q][j] = (c == kk) ? d : cmul(prow[c], d);
+                if (c < w) reg[q][j] = cmul(prow[c], d);
               }
             } else {
               const cplx fd = cmul(f[q], d);
 #pragma unroll
               for (int j = 0; j < CPT; ++j) {
                 const int c = c_own + j * TPR;
-                if (c < w) reg[q][j] = (c == kk) ? cmk(-fd.x, -fd.y) : cfms(fd, prow[c], reg[q][j]);
+                if (c < w) reg[q][j] = cfms(fd, prow[c], reg[q][j]);
               }
             }
           }
