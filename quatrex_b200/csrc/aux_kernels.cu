@@ -437,3 +437,67 @@ void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t 
   real_part_kernel<<<grid_for(count), TB, 0, stream>>>(count, src, dst);
   qtx_check_launch("real_part_kernel");
 }
+
+namespace {
+__global__ void keldysh_combine_kernel(int n, int64_t batch, const cplx* xl, int64_t ldl, int64_t sl, const cplx* xr,
+                                       int64_t ldr, int64_t sr, const double* occ_l, const double* occ_r,
+                                       double sign_r, int sym, cplx* out_l, int64_t so_l, cplx* out_g, int64_t so_g) {
+  const int64_t per = (int64_t)n * n;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < batch * per; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / per;
+    const int q = (int)(t % per);
+    const int r = q / n, c = q % n;
+    const double fl = occ_l[e], fr = occ_r[e];
+    const cplx a = xl[e * sl + (int64_t)r * ldl + c], b = xr[e * sr + (int64_t)r * ldr + c];
+    const cplx yl = keldysh_mix(fl, a, sign_r * fr, b);
+    const cplx yg = keldysh_mix(fl - 1.0, a, sign_r * (fr - 1.0), b);
+    if (!sym) {
+      if (out_l) out_l[e * so_l + q] = yl;
+      if (out_g) out_g[e * so_g + q] = yg;
+      continue;
+    }
+    const cplx at = xl[e * sl + (int64_t)c * ldl + r], bt = xr[e * sr + (int64_t)c * ldr + r];
+    const cplx ylt = keldysh_mix(fl, at, sign_r * fr, bt);
+    const cplx ygt = keldysh_mix(fl - 1.0, at, sign_r * (fr - 1.0), bt);
+    if (out_l) out_l[e * so_l + q] = cmk(0.5 * (yl.x - ylt.x), 0.5 * (yl.y + ylt.y));
+    if (out_g) out_g[e * so_g + q] = cmk(0.5 * (yg.x - ygt.x), 0.5 * (yg.y + ygt.y));
+  }
+}
+__global__ void keldysh_density_kernel(int n, int64_t batch, const cplx* xl, int64_t ldl, int64_t sl, const cplx* xr,
+                                       int64_t ldr, int64_t sr, const double* occ_l, const double* occ_r,
+                                       double* density, double* hole, int64_t out_stride, int out_col) {
+  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
+    const double fl = occ_l[e], fr = occ_r[e];
+    double dl = 0, dg = 0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+      const cplx a = xl[e * sl + (int64_t)r * ldl + r], b = xr[e * sr + (int64_t)r * ldr + r];
+      dl += keldysh_mix(fl, a, fr, b).y;
+      dg += keldysh_mix(fl - 1.0, a, fr - 1.0, b).y;
+    }
+    const cplx s = block_sum(cmk(dl, dg));
+    if (threadIdx.x == 0) {
+      if (density) density[e * out_stride + out_col] = s.x;
+      if (hole) hole[e * out_stride + out_col] = -s.y;
+    }
+  }
+}
+}  // namespace
+
+void launch_keldysh_combine(int n, int64_t batch, MatView xl, MatView xr, const double* occ_l, const double* occ_r,
+                            double sign_r, bool sym, cplx* out_l, int64_t stride_l, cplx* out_g, int64_t stride_g,
+                            cudaStream_t stream) {
+  if (!out_l && !out_g) return;
+  keldysh_combine_kernel<<<grid_for(batch * (int64_t)n * n), TB, 0, stream>>>(
+      n, batch, xl.ptr, xl.ld, xl.stride, xr.ptr, xr.ld, xr.stride, occ_l, occ_r, sign_r, sym ? 1 : 0, out_l, stride_l,
+      out_g, stride_g);
+  qtx_check_launch("keldysh_combine_kernel");
+}
+
+void launch_keldysh_density(int n, int64_t batch, MatView xl, MatView xr, const double* occ_l, const double* occ_r,
+                            double* density, double* hole, int64_t out_stride, int out_col, cudaStream_t stream) {
+  if (!density && !hole) return;
+  const unsigned g = (unsigned)(batch < 65535 ? batch : 65535);
+  keldysh_density_kernel<<<g, TB, 0, stream>>>(n, batch, xl.ptr, xl.ld, xl.stride, xr.ptr, xr.ld, xr.stride, occ_l,
+                                                occ_r, density, hole, out_stride, out_col);
+  qtx_check_launch("keldysh_density_kernel");
+}

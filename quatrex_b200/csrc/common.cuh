@@ -53,6 +53,13 @@ __host__ __device__ __forceinline__ cplx crecip_pivot(cplx z) {
   return cmk(r * t, -t);
 }
 __host__ __device__ __forceinline__ double cabs1(cplx z) { return fabs(z.x) + fabs(z.y); }
+// a xl + b xr for real a, b: the lesser / greater Green's function block from
+// the responses to the two contact sources (G^< = f_L X_L + f_R X_R,
+// G^> = (f_L - 1) X_L + (f_R - 1) X_R).  Every path that forms these blocks
+// uses this one expression.
+__host__ __device__ __forceinline__ cplx keldysh_mix(double a, cplx xl, double b, cplx xr) {
+  return cmk(fma(a, xl.x, b * xr.x), fma(a, xl.y, b * xr.y));
+}
 
 // Per-context launch counter (host side), incremented by every launch helper.
 extern thread_local int64_t* g_qtx_launch_counter;

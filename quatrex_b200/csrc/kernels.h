@@ -102,6 +102,16 @@ void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream);
 void launch_residual_norm(int n, int64_t batch, MatView x_ref, MatView x, double* abs_res, double* rel_res,
                           cudaStream_t stream);
 void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t stream);
+// Lesser / greater blocks from the two contact-source responses XL, XR
+// (n x n, per batch entry e):  Y< = f_L XL + s f_R XR,  Y> = (f_L - 1) XL + s (f_R - 1) XR
+// with f = occ_l[e], occ_r[e] and s = sign_r; sym: write 0.5 (Y - Y^H), else Y.
+// out_l / out_g (row-major n x n at out + e * stride) may be null.
+void launch_keldysh_combine(int n, int64_t batch, MatView xl, MatView xr, const double* occ_l, const double* occ_r,
+                            double sign_r, bool sym, cplx* out_l, int64_t stride_l, cplx* out_g, int64_t stride_g,
+                            cudaStream_t stream);
+// density[e * out_stride + out_col] = sum_r Im Y<_rr, hole[...] = -sum_r Im Y>_rr (either may be null)
+void launch_keldysh_density(int n, int64_t batch, MatView xl, MatView xr, const double* occ_l, const double* occ_r,
+                            double* density, double* hole, int64_t out_stride, int out_col, cudaStream_t stream);
 
 // One generator-form problem of a grouped transport solve, as the persistent
 // kernel reads it (rgf_grouped.cu).  Pairs item0 .. item0 + num_energies - 1 of

@@ -903,6 +903,16 @@ bool transport_contacts(qtx_ctx* ctx, const TransportWS& w, const qtx_transport_
 // are in `w`.  Only kernel launches and device-to-device copies: it can be
 // captured into a CUDA graph.  `w` is taken by value: the buffer swaps of the
 // recursion permute this copy only, so every call starts from the same layout.
+//
+// Keldysh part.  The contacts are the only sources: Sigma^<_c = i f_c Gamma_c,
+// Sigma^>_c = i (f_c - 1) Gamma_c with scalar occupations f_c, and the
+// recursion for X = G^R Sigma G^A is linear in Sigma.  So it runs for the two
+// contact sources instead of the two Keldysh components:
+//   X_L: source i Gamma_L at block 0,  X_R: source i Gamma_R at block nb - 1,
+//   G^< = f_L X_L + f_R X_R,  G^> = (f_L - 1) X_L + (f_R - 1) X_R
+// (keldysh_mix).  X_R vanishes in the whole forward sweep (its source is the
+// last block), so a forward step takes 7 block products instead of 11 and a
+// backward step 13 instead of 15; the outputs are the same blocks.
 void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_transport_outputs& O, int64_t e0,
                      int64_t ne, int prec, cudaStream_t s) {
   const int nb = w.nb, b = w.b;
@@ -916,34 +926,33 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
   cplx** T = w.T;
   cplx** C = w.C;
   BlockStack& xr = w.xr;
-  BlockStack& xl = w.xl;
-  BlockStack& xg = w.xg;
+  BlockStack& yl = w.xl;  // X_L
+  BlockStack& yr = w.xg;  // X_R
   cplx* shift = w.shift;
   cplx* tr = w.tr;
   cplx* cl = w.cl;
   cplx* cr = w.cr;
   int* info = w.info;
+  const double* fl = w.occ_l;
+  const double* fr = w.occ_r;
+  const cplx I1 = cmk(0, 1);
   auto obc_r = [&](int i) { return i == 0 ? MatView(V(C[2])) : (i == nb - 1 ? MatView(V(C[3])) : MatView{}); };
-  auto obc_x = [&](int comp, int i) {
-    int base = comp == 0 ? 4 : 6;
-    return i == 0 ? MatView(V(C[base])) : (i == nb - 1 ? MatView(V(C[base + 1])) : MatView{});
-  };
   auto tv = [&](int idx) { return V(T[idx]); };
   auto out_at = [&](void* base, int64_t blocks_per_e, int blk) {
     return MutView{reinterpret_cast<cplx*>(base) + (e0 * blocks_per_e + blk) * bb, b, blocks_per_e * bb};
   };
+  auto out_ptr = [&](void* base, int64_t blocks_per_e, int blk) {
+    return base ? reinterpret_cast<cplx*>(base) + (e0 * blocks_per_e + blk) * bb : nullptr;
+  };
+  const bool uppers = O.gl_upper || O.gg_upper;
 
-  // ---- first block: x_0 = inv(A_00 - Sigma^R_L), X_0 = x_0 Sigma_0 x_0^H
+  // ---- first block: x_0 = inv(A_00 - Sigma^R_L), X_L,0 = x_0 (i Gamma_L) x_0^H
   // M_0 = (E + i eta) I - H_00 - Sigma^R_L
   // (a K = 0 product: the epilogue alone forms -H_00 - Sigma^R_L + shift on the diagonal)
   gemm(b, b, 0, ne, ONE, tv(0), OP_N, tv(0), OP_N, tv(1), s, hd(0), MONE, obc_r(0), MONE, nullptr, shift);
   zinv(b, ne, tv(1), xr.view(0), info, nullptr, s);
-  for (int comp = 0; comp < 2; ++comp) {
-    BlockStack& X = comp == 0 ? xl : xg;
-    gemm(b, b, b, ne, ONE, xr.view(0), OP_N, obc_x(comp, 0), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
-         prec);
-    gemm(b, b, b, ne, ONE, tv(2), OP_N, xr.view(0), OP_C, X.view(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-  }
+  gemm(b, b, b, ne, I1, xr.view(0), OP_N, V(C[8]), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+  gemm(b, b, b, ne, ONE, tv(2), OP_N, xr.view(0), OP_C, yl.view(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
   // ---- forward sweep
   for (int i = 0; i + 1 < nb; ++i) {
     const int j = i + 1;
@@ -951,27 +960,24 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     // M = (E + i eta) I - H_jj - Sigma^R_j - U A_ij
     gemm(b, b, b, ne, MONE, tv(0), OP_N, up(i), OP_N, tv(1), s, hd(j), MONE, obc_r(j), MONE, nullptr, shift, prec);
     zinv(b, ne, tv(1), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
-    for (int comp = 0; comp < 2; ++comp) {
-      BlockStack& X = comp == 0 ? xl : xg;
-      // V = X_i A_ji^H ; Q = A_ji V + Sigma_obc,j ; X_j = x_j Q x_j^H   (interior Sigma = 0)
-      gemm(b, b, b, ne, ONE, X.view(i), OP_N, lo(i), OP_C, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      gemm(b, b, b, ne, ONE, lo(i), OP_N, tv(3), OP_N, tv(4), s, obc_x(comp, j), ONE, {}, ZERO, nullptr, nullptr,
-           prec);
-      gemm(b, b, b, ne, ONE, xr.view(j), OP_N, tv(4), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      gemm(b, b, b, ne, ONE, tv(5), OP_N, xr.view(j), OP_C, X.view(j), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    }
+    // V = X_L,i A_ji^H ; Q = A_ji V ; X_L,j = x_j Q x_j^H   (no source past block 0)
+    gemm(b, b, b, ne, ONE, yl.view(i), OP_N, lo(i), OP_C, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, lo(i), OP_N, tv(3), OP_N, tv(4), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, xr.view(j), OP_N, tv(4), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, tv(5), OP_N, xr.view(j), OP_C, yl.view(j), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
   }
-  // ---- last blocks, corner chain start
+  // ---- last block: X_R,n = x_n (i Gamma_R) x_n^H, outputs, corner chain start
   const int n = nb - 1;
-  if (O.gl_diag) launch_block_scatter(b, b, ne, xl.view(n), 1, out_at(O.gl_diag, nb, n).ptr, nb * bb, bb, nullptr, s);
-  if (O.gg_diag) launch_block_scatter(b, b, ne, xg.view(n), 1, out_at(O.gg_diag, nb, n).ptr, nb * bb, bb, nullptr, s);
+  gemm(b, b, b, ne, I1, xr.view(n), OP_N, V(C[9]), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+  gemm(b, b, b, ne, ONE, tv(2), OP_N, xr.view(n), OP_C, yr.view(n), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+  launch_keldysh_combine(b, ne, yl.view(n), yr.view(n), fl, fr, 1.0, true, out_ptr(O.gl_diag, nb, n), nb * bb,
+                         out_ptr(O.gg_diag, nb, n), nb * bb, s);
   if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, out_at(O.gr_diag, nb, n), s);
-  if (O.density) launch_diag_imag_sum(b, ne, xl.view(n), 1.0, O.density + e0 * nb, nb, n, s);
-  if (O.hole_density) launch_diag_imag_sum(b, ne, xg.view(n), -1.0, O.hole_density + e0 * nb, nb, n, s);
+  launch_keldysh_density(b, ne, yl.view(n), yr.view(n), fl, fr, O.density ? O.density + e0 * nb : nullptr,
+                         O.hole_density ? O.hole_density + e0 * nb : nullptr, nb, n, s);
   // contact current at the right contact uses the symmetrised G^<_nn, G^>_nn
   if (O.current_right) {
-    launch_block_scatter(b, b, ne, xl.view(n), 1, T[6], bb, bb, nullptr, s);
-    launch_block_scatter(b, b, ne, xg.view(n), 1, T[7], bb, bb, nullptr, s);
+    launch_keldysh_combine(b, ne, yl.view(n), yr.view(n), fl, fr, 1.0, true, T[6], bb, T[7], bb, s);
     launch_trace_product(b, b, ne, V(C[7]), tv(6), ONE, cr, false, s);
     launch_trace_product(b, b, ne, tv(7), V(C[5]), MONE, cr, true, s);
     QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_right) + e0, cr, sizeof(cplx) * ne,
@@ -997,33 +1003,31 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
            prec);
       std::swap(corner, corner2);
     }
-    for (int comp = 0; comp < 2; ++comp) {
-      BlockStack& X = comp == 0 ? xl : xg;
-      void* od = comp == 0 ? O.gl_diag : O.gg_diag;
-      void* ou = comp == 0 ? O.gl_upper : O.gg_upper;
-      // t1 = P4 X_i - (P4 X_i)^H ; t2 = P1 X_j
-      gemm(b, b, b, ne, ONE, tv(3), OP_N, X.view(i), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      launch_sub_herm_inplace(b, ne, tv(5), s);
-      gemm(b, b, b, ne, ONE, tv(0), OP_N, X.view(j), OP_N, tv(6), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-      // X_ij = -t2 - X_i P2^H
-      if (ou)
-        gemm(b, b, b, ne, MONE, X.view(i), OP_N, tv(1), OP_C, out_at(ou, nb - 1, i), s, tv(6), MONE, {}, ZERO,
-             nullptr, nullptr, prec);
-      // X_i += t2 P1^H + t1
-      gemm(b, b, b, ne, ONE, tv(6), OP_N, tv(0), OP_C, X.view(i), s, X.view(i), ONE, tv(5), ONE, nullptr, nullptr,
-           prec);
-      if (od) launch_block_scatter(b, b, ne, X.view(i), 1, out_at(od, nb, i).ptr, nb * bb, bb, nullptr, s);
-    }
-    if (O.density) launch_diag_imag_sum(b, ne, xl.view(i), 1.0, O.density + e0 * nb, nb, i, s);
-    if (O.hole_density) launch_diag_imag_sum(b, ne, xg.view(i), -1.0, O.hole_density + e0 * nb, nb, i, s);
+    // X_L: t1 = P4 X_i - (P4 X_i)^H ; t2 = P1 X_j ; X_ij = -t2 - X_i P2^H ; X_i += t2 P1^H + t1
+    gemm(b, b, b, ne, ONE, tv(3), OP_N, yl.view(i), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    launch_sub_herm_inplace(b, ne, tv(5), s);
+    gemm(b, b, b, ne, ONE, tv(0), OP_N, yl.view(j), OP_N, tv(6), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    if (uppers)
+      gemm(b, b, b, ne, MONE, yl.view(i), OP_N, tv(1), OP_C, tv(7), s, tv(6), MONE, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, tv(6), OP_N, tv(0), OP_C, yl.view(i), s, yl.view(i), ONE, tv(5), ONE, nullptr, nullptr,
+         prec);
+    // X_R (zero in the forward sweep): t2 = P1 X_j ; X_ij = -t2 ; X_i = t2 P1^H
+    gemm(b, b, b, ne, ONE, tv(0), OP_N, yr.view(j), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, tv(5), OP_N, tv(0), OP_C, yr.view(i), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    if (uppers)
+      launch_keldysh_combine(b, ne, tv(7), tv(5), fl, fr, -1.0, false, out_ptr(O.gl_upper, nb - 1, i),
+                             (nb - 1) * bb, out_ptr(O.gg_upper, nb - 1, i), (nb - 1) * bb, s);
+    launch_keldysh_combine(b, ne, yl.view(i), yr.view(i), fl, fr, 1.0, true, out_ptr(O.gl_diag, nb, i), nb * bb,
+                           out_ptr(O.gg_diag, nb, i), nb * bb, s);
+    launch_keldysh_density(b, ne, yl.view(i), yr.view(i), fl, fr, O.density ? O.density + e0 * nb : nullptr,
+                           O.hole_density ? O.hole_density + e0 * nb : nullptr, nb, i, s);
     gemm(b, b, b, ne, ONE, tv(3), OP_N, xr.view(i), OP_N, tv(4), s, xr.view(i), ONE, {}, ZERO, nullptr, nullptr,
          prec);
     std::swap(xr.ptr[i], T[4]);
     if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(i), ZERO, {}, out_at(O.gr_diag, nb, i), s);
   }
   if (O.current_left) {
-    launch_block_scatter(b, b, ne, xl.view(0), 1, T[6], bb, bb, nullptr, s);
-    launch_block_scatter(b, b, ne, xg.view(0), 1, T[7], bb, bb, nullptr, s);
+    launch_keldysh_combine(b, ne, yl.view(0), yr.view(0), fl, fr, 1.0, true, T[6], bb, T[7], bb, s);
     launch_trace_product(b, b, ne, V(C[6]), tv(6), ONE, cl, false, s);
     launch_trace_product(b, b, ne, tv(7), V(C[4]), MONE, cl, true, s);
     QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_left) + e0, cl, sizeof(cplx) * ne,
@@ -1036,7 +1040,6 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     launch_trace_product_h(b, b, ne, tv(1), V(corner), tr, s);
     launch_real_part(ne, tr, O.transmission + e0, s);
   }
-
 }
 
 void transport_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qtx_transport_outputs& O, int prec,

@@ -412,15 +412,6 @@ __device__ void blk_axpby(int n, cplx alpha, const cplx* x, cplx beta, const cpl
   }
   __syncthreads();
 }
-// d = 0.5 (x - x^H)   (stored diagonal blocks of G^<, G^>)
-__device__ void blk_skew_half(int n, const cplx* x, cplx* d) {
-  for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-    const int r = q / n, c = q % n;
-    const cplx a = x[q], b = x[c * n + r];
-    d[q] = cmk(0.5 * (a.x - b.x), 0.5 * (a.y + b.y));
-  }
-  __syncthreads();
-}
 // x <- x - x^H in place
 __device__ void blk_sub_herm(int n, cplx* x) {
   for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
@@ -450,6 +441,30 @@ __device__ void blk_obc_lesser_greater(int n, const cplx* s, double f, cplx* sl,
   }
   __syncthreads();
 }
+// Y< = f_L xl + s f_R xr, Y> = (f_L - 1) xl + s (f_R - 1) xr  (keldysh_mix);
+// sym: write 0.5 (Y - Y^H).  out_l / out_g may be null.
+__device__ void blk_keldysh_combine(int n, const cplx* xl, const cplx* xr, double fl, double fr, double sign_r,
+                                    bool sym, cplx* out_l, cplx* out_g) {
+  if (out_l || out_g) {
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+      const int r = q / n, c = q % n;
+      const cplx a = xl[q], b = xr[q];
+      const cplx yl = keldysh_mix(fl, a, sign_r * fr, b);
+      const cplx yg = keldysh_mix(fl - 1.0, a, sign_r * (fr - 1.0), b);
+      if (!sym) {
+        if (out_l) out_l[q] = yl;
+        if (out_g) out_g[q] = yg;
+        continue;
+      }
+      const cplx at = xl[c * n + r], bt = xr[c * n + r];
+      const cplx ylt = keldysh_mix(fl, at, sign_r * fr, bt);
+      const cplx ygt = keldysh_mix(fl - 1.0, at, sign_r * (fr - 1.0), bt);
+      if (out_l) out_l[q] = cmk(0.5 * (yl.x - ylt.x), 0.5 * (yl.y + ylt.y));
+      if (out_g) out_g[q] = cmk(0.5 * (yg.x - ygt.x), 0.5 * (yg.y + ygt.y));
+    }
+  }
+  __syncthreads();
+}
 // Tr[x y]
 template <int BT>
 __device__ cplx blk_trace_product(int n, const cplx* x, const cplx* y) {
@@ -460,12 +475,17 @@ __device__ cplx blk_trace_product(int n, const cplx* x, const cplx* y) {
   }
   return cta_sum<BT>(acc);
 }
-// sum_r Im x[r][r]
+// (sum_r Im Y<_rr, -sum_r Im Y>_rr) of the combination above (sign 1)
 template <int BT>
-__device__ double blk_diag_imag_sum(int n, const cplx* x) {
-  double acc = 0;
-  for (int r = threadIdx.x; r < n; r += blockDim.x) acc += x[r * n + r].y;
-  return cta_sum<BT>(cmk(acc, 0)).x;
+__device__ cplx blk_keldysh_density(int n, const cplx* xl, const cplx* xr, double fl, double fr) {
+  double dl = 0, dg = 0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const cplx a = xl[r * n + r], b = xr[r * n + r];
+    dl += keldysh_mix(fl, a, fr, b).y;
+    dg += keldysh_mix(fl - 1.0, a, fr - 1.0, b).y;
+  }
+  const cplx s = cta_sum<BT>(cmk(dl, dg));
+  return cmk(s.x, -s.y);
 }
 
 // Sancho-Rubio decimation of one lead (the loop of sancho_rubio_impl for one
@@ -601,25 +621,22 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
   const double f_r = 1.0 / (1.0 + exp((energy - P->mu_right) / P->kt));
   blk_obc_lesser_greater(n, Cb[2], f_l, Cb[4], Cb[6], Cb[8]);
   blk_obc_lesser_greater(n, Cb[3], f_r, Cb[5], Cb[7], Cb[9]);
-  auto obc_x = [&](int comp, int i) -> const cplx* {
-    const int base = comp == 0 ? 4 : 6;
-    return i == 0 ? Cb[base] : (i == nb - 1 ? Cb[base + 1] : nullptr);
-  };
 
-  // ---- first block: x_0 = inv((E + i eta) I - H_00 - Sigma^R_L), X_0 = x_0 Sigma_0 x_0^H
+  // ---- first block: x_0 = inv((E + i eta) I - H_00 - Sigma^R_L), X_L,0 = x_0 (i Gamma_L) x_0^H
+  // (the Keldysh part runs for the two contact sources, as transport_sweep in
+  // rgf.cu: X_L from i Gamma_L at block 0, X_R from i Gamma_R at block nb - 1,
+  // G^< = f_L X_L + f_R X_R, G^> = (f_L - 1) X_L + (f_R - 1) X_R)
+  const cplx I1 = cmk(0, 1);
   a = g0;
   a.k = 0; a.d = T[1]; a.c = hd(0); a.beta = MONE; a.c2 = Cb[2]; a.gamma = MONE; a.has_shift = 1; a.shift = shift;
   cta_gemm<BT>(a, n);
   zero |= cta_inverse<BT>(T[1], XR(0), n);
-  for (int comp = 0; comp < 2; ++comp) {
-    cplx* X0 = comp == 0 ? XL(0) : XG(0);
-    a = g0;
-    a.a = XR(0); a.b = obc_x(comp, 0); a.d = T[2];
-    cta_gemm<BT>(a, n);
-    a = g0;
-    a.a = T[2]; a.b = XR(0); a.opb = OP_C; a.d = X0;
-    cta_gemm<BT>(a, n);
-  }
+  a = g0;
+  a.a = XR(0); a.b = Cb[8]; a.d = T[2]; a.alpha = I1;
+  cta_gemm<BT>(a, n);
+  a = g0;
+  a.a = T[2]; a.b = XR(0); a.opb = OP_C; a.d = XL(0);
+  cta_gemm<BT>(a, n);
   // ---- forward sweep
   for (int i = 0; i + 1 < nb; ++i) {
     const int j = i + 1;
@@ -634,44 +651,40 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
     }
     cta_gemm<BT>(a, n);
     zero |= cta_inverse<BT>(T[1], XR(j), n);
-    for (int comp = 0; comp < 2; ++comp) {
-      cplx* Xi = comp == 0 ? XL(i) : XG(i);
-      cplx* Xj = comp == 0 ? XL(j) : XG(j);
-      a = g0;  // X_i A_ji^H = -X_i U_i
-      a.a = Xi; a.b = uu(i); a.d = T[3]; a.alpha = MONE;
-      cta_gemm<BT>(a, n);
-      a = g0;  // A_ji (X_i A_ji^H) + Sigma_obc,j
-      a.a = uu(i); a.opa = OP_C; a.b = T[3]; a.d = T[4]; a.alpha = MONE;
-      if (obc_x(comp, j)) {
-        a.c = obc_x(comp, j);
-        a.beta = ONE;
-      }
-      cta_gemm<BT>(a, n);
-      a = g0;
-      a.a = XR(j); a.b = T[4]; a.d = T[5];
-      cta_gemm<BT>(a, n);
-      a = g0;
-      a.a = T[5]; a.b = XR(j); a.opb = OP_C; a.d = Xj;
-      cta_gemm<BT>(a, n);
+    a = g0;  // X_L,i A_ji^H = -X_L,i U_i
+    a.a = XL(i); a.b = uu(i); a.d = T[3]; a.alpha = MONE;
+    cta_gemm<BT>(a, n);
+    a = g0;  // A_ji (X_L,i A_ji^H)   (no source past block 0)
+    a.a = uu(i); a.opa = OP_C; a.b = T[3]; a.d = T[4]; a.alpha = MONE;
+    cta_gemm<BT>(a, n);
+    a = g0;
+    a.a = XR(j); a.b = T[4]; a.d = T[5];
+    cta_gemm<BT>(a, n);
+    a = g0;
+    a.a = T[5]; a.b = XR(j); a.opb = OP_C; a.d = XL(j);
+    cta_gemm<BT>(a, n);
+  }
+  // ---- last block: X_R,n = x_n (i Gamma_R) x_n^H
+  const int nl = nb - 1;
+  a = g0;
+  a.a = XR(nl); a.b = Cb[9]; a.d = T[2]; a.alpha = I1;
+  cta_gemm<BT>(a, n);
+  a = g0;
+  a.a = T[2]; a.b = XR(nl); a.opb = OP_C; a.d = XG(nl);
+  cta_gemm<BT>(a, n);
+  const int64_t o_diag = (e * nb + nl) * bb;
+  blk_keldysh_combine(n, XL(nl), XG(nl), f_l, f_r, 1.0, true, P->gl_diag ? P->gl_diag + o_diag : nullptr,
+                      P->gg_diag ? P->gg_diag + o_diag : nullptr);
+  if (P->gr_diag) blk_axpby(n, ONE, XR(nl), ONE, nullptr, P->gr_diag + o_diag);
+  if (P->density || P->hole_density) {
+    const cplx dh = blk_keldysh_density<BT>(n, XL(nl), XG(nl), f_l, f_r);
+    if (threadIdx.x == 0) {
+      if (P->density) P->density[e * nb + nl] = dh.x;
+      if (P->hole_density) P->hole_density[e * nb + nl] = dh.y;
     }
   }
-  // ---- last block
-  const int nl = nb - 1;
-  const int64_t o_diag = (e * nb + nl) * bb;
-  if (P->gl_diag) blk_skew_half(n, XL(nl), P->gl_diag + o_diag);
-  if (P->gg_diag) blk_skew_half(n, XG(nl), P->gg_diag + o_diag);
-  if (P->gr_diag) blk_axpby(n, ONE, XR(nl), ONE, nullptr, P->gr_diag + o_diag);
-  if (P->density) {
-    const double s = blk_diag_imag_sum<BT>(n, XL(nl));
-    if (threadIdx.x == 0) P->density[e * nb + nl] = s;
-  }
-  if (P->hole_density) {
-    const double s = blk_diag_imag_sum<BT>(n, XG(nl));
-    if (threadIdx.x == 0) P->hole_density[e * nb + nl] = -s;
-  }
   if (P->current_right) {
-    blk_skew_half(n, XL(nl), T[6]);
-    blk_skew_half(n, XG(nl), T[7]);
+    blk_keldysh_combine(n, XL(nl), XG(nl), f_l, f_r, 1.0, true, T[6], T[7]);
     const cplx c1 = blk_trace_product<BT>(n, Cb[7], T[6]);
     const cplx c2 = blk_trace_product<BT>(n, T[7], Cb[5]);
     if (threadIdx.x == 0) P->current_right[e] = cadd(c1, cmul(MONE, c2));
@@ -679,6 +692,7 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
   cplx* corner = T[8];
   cplx* corner2 = T[9];
   if (P->transmission) blk_axpby(n, ONE, XR(nl), ONE, nullptr, corner);
+  const bool uppers = P->gl_upper || P->gg_upper;
   // ---- backward sweep
   cplx* g_next = XR(nl);  // G^R_jj of the block after i
   cplx* spare = T[4];
@@ -711,35 +725,39 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
       corner = corner2;
       corner2 = tmp;
     }
-    for (int comp = 0; comp < 2; ++comp) {
-      cplx* Xi = comp == 0 ? XL(i) : XG(i);
-      cplx* Xj = comp == 0 ? XL(j) : XG(j);
-      cplx* od = comp == 0 ? P->gl_diag : P->gg_diag;
-      cplx* ou = comp == 0 ? P->gl_upper : P->gg_upper;
-      a = g0;  // t1 = P4 X_i - (P4 X_i)^H
-      a.a = T[3]; a.b = Xi; a.d = T[5];
+    a = g0;  // X_L: t1 = P4 X_i - (P4 X_i)^H
+    a.a = T[3]; a.b = XL(i); a.d = T[5];
+    cta_gemm<BT>(a, n);
+    blk_sub_herm(n, T[5]);
+    a = g0;  // t2 = P1 X_j
+    a.a = T[0]; a.b = XL(j); a.d = T[6];
+    cta_gemm<BT>(a, n);
+    if (uppers) {
+      a = g0;  // X_ij = -t2 - X_i P2^H
+      a.a = XL(i); a.b = T[1]; a.opb = OP_C; a.d = T[7]; a.alpha = MONE; a.c = T[6]; a.beta = MONE;
       cta_gemm<BT>(a, n);
-      blk_sub_herm(n, T[5]);
-      a = g0;  // t2 = P1 X_j
-      a.a = T[0]; a.b = Xj; a.d = T[6];
-      cta_gemm<BT>(a, n);
-      if (ou) {
-        a = g0;  // X_ij = -t2 - X_i P2^H
-        a.a = Xi; a.b = T[1]; a.opb = OP_C; a.d = ou + o_up; a.alpha = MONE; a.c = T[6]; a.beta = MONE;
-        cta_gemm<BT>(a, n);
+    }
+    a = g0;  // X_i += t2 P1^H + t1
+    a.a = T[6]; a.b = T[0]; a.opb = OP_C; a.d = XL(i); a.c = XL(i); a.beta = ONE; a.c2 = T[5]; a.gamma = ONE;
+    cta_gemm<BT>(a, n);
+    a = g0;  // X_R (zero in the forward sweep): t2 = P1 X_j, X_ij = -t2, X_i = t2 P1^H
+    a.a = T[0]; a.b = XG(j); a.d = T[5];
+    cta_gemm<BT>(a, n);
+    a = g0;
+    a.a = T[5]; a.b = T[0]; a.opb = OP_C; a.d = XG(i);
+    cta_gemm<BT>(a, n);
+    if (uppers)
+      blk_keldysh_combine(n, T[7], T[5], f_l, f_r, -1.0, false, P->gl_upper ? P->gl_upper + o_up : nullptr,
+                          P->gg_upper ? P->gg_upper + o_up : nullptr);
+    const int64_t o_d = (e * nb + i) * bb;
+    blk_keldysh_combine(n, XL(i), XG(i), f_l, f_r, 1.0, true, P->gl_diag ? P->gl_diag + o_d : nullptr,
+                        P->gg_diag ? P->gg_diag + o_d : nullptr);
+    if (P->density || P->hole_density) {
+      const cplx dh = blk_keldysh_density<BT>(n, XL(i), XG(i), f_l, f_r);
+      if (threadIdx.x == 0) {
+        if (P->density) P->density[e * nb + i] = dh.x;
+        if (P->hole_density) P->hole_density[e * nb + i] = dh.y;
       }
-      a = g0;  // X_i += t2 P1^H + t1
-      a.a = T[6]; a.b = T[0]; a.opb = OP_C; a.d = Xi; a.c = Xi; a.beta = ONE; a.c2 = T[5]; a.gamma = ONE;
-      cta_gemm<BT>(a, n);
-      if (od) blk_skew_half(n, Xi, od + (e * nb + i) * bb);
-    }
-    if (P->density) {
-      const double s = blk_diag_imag_sum<BT>(n, XL(i));
-      if (threadIdx.x == 0) P->density[e * nb + i] = s;
-    }
-    if (P->hole_density) {
-      const double s = blk_diag_imag_sum<BT>(n, XG(i));
-      if (threadIdx.x == 0) P->hole_density[e * nb + i] = -s;
     }
     a = g0;  // G_ii = x_i + P4 x_i
     a.a = T[3]; a.b = XR(i); a.d = spare; a.c = XR(i); a.beta = ONE;
@@ -750,8 +768,7 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
     if (P->gr_diag) blk_axpby(n, ONE, g_next, ONE, nullptr, P->gr_diag + (e * nb + i) * bb);
   }
   if (P->current_left) {
-    blk_skew_half(n, XL(0), T[6]);
-    blk_skew_half(n, XG(0), T[7]);
+    blk_keldysh_combine(n, XL(0), XG(0), f_l, f_r, 1.0, true, T[6], T[7]);
     const cplx c1 = blk_trace_product<BT>(n, Cb[6], T[6]);
     const cplx c2 = blk_trace_product<BT>(n, T[7], Cb[4]);
     if (threadIdx.x == 0) P->current_left[e] = cadd(c1, cmul(MONE, c2));

@@ -84,6 +84,17 @@ def test_grouped_blocks_against_oracle(b):
     assert well >= 4
 
 
+def _obs_err(k, got, want):
+    """Per-energy error of an observable.  A contact current is a small
+    difference of two traces of order one wherever f_L ~ f_R, so its rounding
+    is measured against the device's largest current, not the current itself
+    (as density errors are measured against the largest block of the energy)."""
+    if k.startswith("current"):
+        got = got.cpu().numpy() if isinstance(got, torch.Tensor) else got
+        return np.abs(got - want) / max(np.abs(want).max(), 1e-300)
+    return _per_energy_rel(got, want)
+
+
 def _pair_bound(dev):
     """Per-energy bound for two FP64 evaluations of the same solve: each is
     within max(1e-10, 20 x the oracle's spread) of the exact result."""
@@ -107,7 +118,7 @@ def test_grouped_equals_layered(b):
             err = _per_energy_rel(out[k], ref[k].cpu().numpy())
             assert (err <= bound).all(), (k, err, bound)
         for k in ("density", "hole_density", "transmission", "current_left", "current_right"):
-            err = _per_energy_rel(out[k], ref[k].cpu().numpy())
+            err = _obs_err(k, out[k], ref[k].cpu().numpy())
             assert (err <= 10 * bound).all(), (k, err, bound)
 
 
@@ -131,7 +142,7 @@ def test_grouped_is_one_launch_for_uneven_devices():
         bound = _pair_bound(d)
         assert torch.equal(out["sr_iterations"], ref["sr_iterations"])
         for k in ("density", "hole_density", "transmission", "current_left", "current_right"):
-            err = _per_energy_rel(out[k], ref[k].cpu().numpy())
+            err = _obs_err(k, out[k], ref[k].cpu().numpy())
             assert (err <= 10 * bound).all(), (k, err, bound)
 
 
