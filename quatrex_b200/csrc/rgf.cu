@@ -911,8 +911,9 @@ bool transport_contacts(qtx_ctx* ctx, const TransportWS& w, const qtx_transport_
 //   X_L: source i Gamma_L at block 0,  X_R: source i Gamma_R at block nb - 1,
 //   G^< = f_L X_L + f_R X_R,  G^> = (f_L - 1) X_L + (f_R - 1) X_R
 // (keldysh_mix).  X_R vanishes in the whole forward sweep (its source is the
-// last block), so a forward step takes 7 block products instead of 11 and a
-// backward step 13 instead of 15; the outputs are the same blocks.
+// last block), and the forward X_L step is W X_L,i W^H with W = x_j A_ji, so
+// a forward step takes 6 block products instead of 11 and a backward step 13
+// instead of 15; the outputs are the same blocks.
 void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_transport_outputs& O, int64_t e0,
                      int64_t ne, int prec, cudaStream_t s) {
   const int nb = w.nb, b = w.b;
@@ -960,11 +961,11 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     // M = (E + i eta) I - H_jj - Sigma^R_j - U A_ij
     gemm(b, b, b, ne, MONE, tv(0), OP_N, up(i), OP_N, tv(1), s, hd(j), MONE, obc_r(j), MONE, nullptr, shift, prec);
     zinv(b, ne, tv(1), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
-    // V = X_L,i A_ji^H ; Q = A_ji V ; X_L,j = x_j Q x_j^H   (no source past block 0)
-    gemm(b, b, b, ne, ONE, yl.view(i), OP_N, lo(i), OP_C, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    gemm(b, b, b, ne, ONE, lo(i), OP_N, tv(3), OP_N, tv(4), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    gemm(b, b, b, ne, ONE, xr.view(j), OP_N, tv(4), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    gemm(b, b, b, ne, ONE, tv(5), OP_N, xr.view(j), OP_C, yl.view(j), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    // X_L,j = x_j A_ji X_L,i A_ji^H x_j^H = W X_L,i W^H with W = x_j A_ji
+    // (no source past block 0)
+    gemm(b, b, b, ne, ONE, xr.view(j), OP_N, lo(i), OP_N, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, tv(3), OP_N, yl.view(i), OP_N, tv(4), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    gemm(b, b, b, ne, ONE, tv(4), OP_N, tv(3), OP_C, yl.view(j), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
   }
   // ---- last block: X_R,n = x_n (i Gamma_R) x_n^H, outputs, corner chain start
   const int n = nb - 1;

@@ -651,17 +651,14 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
     }
     cta_gemm<BT>(a, n);
     zero |= cta_inverse<BT>(T[1], XR(j), n);
-    a = g0;  // X_L,i A_ji^H = -X_L,i U_i
-    a.a = XL(i); a.b = uu(i); a.d = T[3]; a.alpha = MONE;
-    cta_gemm<BT>(a, n);
-    a = g0;  // A_ji (X_L,i A_ji^H)   (no source past block 0)
-    a.a = uu(i); a.opa = OP_C; a.b = T[3]; a.d = T[4]; a.alpha = MONE;
+    a = g0;  // W = x_j A_ji = -x_j U_i^H ; X_L,j = W X_L,i W^H  (no source past block 0)
+    a.a = XR(j); a.b = uu(i); a.opb = OP_C; a.d = T[3]; a.alpha = MONE;
     cta_gemm<BT>(a, n);
     a = g0;
-    a.a = XR(j); a.b = T[4]; a.d = T[5];
+    a.a = T[3]; a.b = XL(i); a.d = T[4];
     cta_gemm<BT>(a, n);
     a = g0;
-    a.a = T[5]; a.b = XR(j); a.opb = OP_C; a.d = XL(j);
+    a.a = T[4]; a.b = T[3]; a.opb = OP_C; a.d = XL(j);
     cta_gemm<BT>(a, n);
   }
   // ---- last block: X_R,n = x_n (i Gamma_R) x_n^H
