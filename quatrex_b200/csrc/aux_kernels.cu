@@ -192,16 +192,6 @@ __global__ void trace_product_h_kernel(int rows, int cols, int64_t batch, const 
   }
 }
 
-__global__ void diag_imag_sum_kernel(int n, int64_t batch, const cplx* x, int64_t ldx, int64_t sx, double sign,
-                                     double* out, int64_t out_stride, int out_col) {
-  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
-    double acc = 0;
-    for (int r = threadIdx.x; r < n; r += blockDim.x) acc += x[e * sx + (int64_t)r * ldx + r].y;
-    cplx s = block_sum(cmk(acc, 0));
-    if (threadIdx.x == 0) out[e * out_stride + out_col] = sign * s.x;
-  }
-}
-
 __global__ void sr_norm_kernel(int n, int64_t batch, const cplx* a, int64_t lda, int64_t sa, const cplx* b,
                                int64_t ldb, int64_t sb, double tol, int* active, int* iterations, int* num_active) {
   for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
@@ -385,12 +375,6 @@ void launch_trace_product_h(int rows, int cols, int64_t batch, MatView x, MatVie
   qtx_check_launch("trace_product_h_kernel");
 }
 
-void launch_diag_imag_sum(int n, int64_t batch, MatView x, double sign, double* out, int64_t out_stride, int out_col,
-                          cudaStream_t stream) {
-  unsigned g = (unsigned)(batch < 65535 ? batch : 65535);
-  diag_imag_sum_kernel<<<g, TB, 0, stream>>>(n, batch, x.ptr, x.ld, x.stride, sign, out, out_stride, out_col);
-  qtx_check_launch("diag_imag_sum_kernel");
-}
 
 void launch_sr_norm_update(int n, int64_t batch, MatView alpha, MatView beta, double tol, int* active,
                            int* iterations, int* num_active, cudaStream_t stream) {

@@ -80,9 +80,6 @@ void launch_trace_product(int rows, int cols, int64_t batch, MatView x, MatView 
 // tr[e] = sum_rc x[r][c] * conj(y[r][c])   (Tr[x y^H])
 void launch_trace_product_h(int rows, int cols, int64_t batch, MatView x, MatView y, cplx* tr,
                             cudaStream_t stream);
-// out[e * out_stride + out_col] = sign * sum_r Im x[r][r]
-void launch_diag_imag_sum(int n, int64_t batch, MatView x, double sign, double* out, int64_t out_stride,
-                          int out_col, cudaStream_t stream);
 // Sancho-Rubio convergence: delta[e] = || |alpha| + |beta| ||_F / 2 ; then
 // active[e] = active[e] && delta >= tol; iterations[e] += active-before.
 void launch_sr_norm_update(int n, int64_t batch, MatView alpha, MatView beta, double tol, int* active,
