@@ -227,6 +227,10 @@ typedef struct qtx_transport_outputs {
   void* current_left;    /* (num_energies) complex contact current (observables.py:151-157) */
   void* current_right;   /* (num_energies) complex */
   int32_t* sr_iterations; /* (num_energies, 2) */
+  double* dos;           /* (num_energies, nb): mean over each block of -Im diag G^R, the density of
+                            states ElectronSolver._filter_peaks builds (src/quatrex/electron/solver.py:428-434) */
+  void* layer_current;   /* (num_energies, nb-1) complex: observables.device_current with the Hamiltonian,
+                            sum(H_ij * G^<_ji^T - G^<_ij * H_ji^T) per interface (src/quatrex/core/observables.py:192-237) */
 } qtx_transport_outputs;
 
 qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, const qtx_transport_outputs* o,

@@ -16,6 +16,8 @@ upstream qttools / quatrex code (paths relative to the upstream repository):
   ``src/quatrex/core/statistics.py:7-23``
 * ``get_batches``    -- ``src/qttools/utils/solvers_utils.py:7-32`` with
   ``src/qttools/utils/mpi_utils.py:16-67``
+* ``layer_current``  -- ``src/quatrex/core/observables.py:192-237``
+* ``block_dos``, ``peak_mask`` -- ``src/quatrex/electron/solver.py:412-454``
 
 Parity of this restatement is pinned against the upstream implementation run
 in the build container: ``tests/golden/make_golden.py`` imports the upstream
@@ -355,6 +357,35 @@ def contact_currents(xl_first, xg_first, xl_last, xg_last, obc):
     i_left = np.trace(obc["greater"][0] @ xl_first - xg_first @ obc["lesser"][0], axis1=-2, axis2=-1)
     i_right = np.trace(obc["greater"][1] @ xl_last - xg_last @ obc["lesser"][1], axis1=-2, axis2=-1)
     return i_left, i_right
+
+
+def block_dos(xr_diag):
+    """Per-block mean of -Im diag(G^R_ii): the local density of states that
+    ``ElectronSolver._filter_peaks`` builds (``src/quatrex/electron/solver.py:428-434``);
+    returns (E, nb)."""
+    return np.stack([-np.diagonal(x, axis1=-2, axis2=-1).imag.mean(-1) for x in xr_diag], axis=-1)
+
+
+def layer_current(xl_upper, h_upper):
+    """``observables.device_current`` (``src/quatrex/core/observables.py:192-237``)
+    with the Hamiltonian as the operator: for interface i (j = i + 1),
+    sum(H_ij * (G^<_ji)^T - G^<_ij * (H_ji)^T) over the block, with the stored
+    lower block G^<_ji = -(G^<_ij)^H and H_ji = H_ij^H; returns (E, nb - 1)."""
+    out = []
+    for g, h in zip(xl_upper, h_upper):
+        g_ji = -_h(g)
+        h_ji = _h(h)
+        out.append((h * g_ji.swapaxes(-2, -1) - g * h_ji.swapaxes(-2, -1)).sum(axis=(-1, -2)))
+    return np.stack(out, axis=-1)
+
+
+def peak_mask(dos, energies, dos_peak_limit):
+    """Energies at which ``ElectronSolver._filter_peaks`` zeroes G^<, G^>, G^R
+    (``src/quatrex/electron/solver.py:436-454``): the largest |d dos / dE| over
+    the blocks above ``dos_peak_limit``, or the largest dos above 10.  ``dos``
+    is (E, nb); the derivative is numpy.gradient along the energy grid."""
+    grad = np.abs(np.gradient(dos, energies, axis=0))
+    return (grad.max(axis=1) > dos_peak_limit) | (dos.max(axis=1) > 10)
 
 
 def dense_from_blocks(diag, upper, lower):

@@ -96,6 +96,8 @@ class TransportOutputs(ctypes.Structure):
         ("current_left", c_void_p),
         ("current_right", c_void_p),
         ("sr_iterations", c_void_p),
+        ("dos", c_void_p),
+        ("layer_current", c_void_p),
     ]
 
 

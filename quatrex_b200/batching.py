@@ -34,7 +34,8 @@ from quatrex_b200.transport import (GROUPED_MAX_BLOCK_SIZE, TransportSolver, gro
                                     solve_grouped)
 from quatrex_b200.workloads import TransportDevice
 
-OBSERVABLE_KEYS = ("density", "hole_density", "transmission", "current_left", "current_right", "sr_iterations")
+OBSERVABLE_KEYS = ("density", "hole_density", "transmission", "current_left", "current_right", "sr_iterations", "dos",
+                   "layer_current")
 
 
 def instance_flops(dev: TransportDevice, num_energies: int) -> float:

@@ -485,3 +485,49 @@ void launch_keldysh_density(int n, int64_t batch, MatView xl, MatView xr, const 
                                                 occ_r, density, hole, out_stride, out_col);
   qtx_check_launch("keldysh_density_kernel");
 }
+
+namespace {
+__global__ void block_dos_kernel(int n, int64_t batch, const cplx* g, int64_t ld, int64_t sg, double* out,
+                                 int64_t out_stride, int out_col) {
+  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
+    double acc = 0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) acc += g[e * sg + (int64_t)r * ld + r].y;
+    const cplx s = block_sum(cmk(acc, 0));
+    if (threadIdx.x == 0) out[e * out_stride + out_col] = -s.x / n;
+  }
+}
+__global__ void layer_current_kernel(int n, int64_t batch, const cplx* xl, int64_t ldl, int64_t sl, const cplx* xr,
+                                     int64_t ldr, int64_t sr, const double* occ_l, const double* occ_r,
+                                     double sign_r, const cplx* h, cplx* out, int64_t out_stride, int out_col) {
+  for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
+    const double fl = occ_l[e], fr = occ_r[e];
+    cplx acc = cmk(0, 0);
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+      const int r = q / n, c = q % n;
+      const cplx y = keldysh_mix(fl, xl[e * sl + (int64_t)r * ldl + c], sign_r * fr, xr[e * sr + (int64_t)r * ldr + c]);
+      const cplx hv = h[q];
+      acc = cadd(acc, csub(cmul(hv, cmk(-y.x, y.y)), cmul(y, cconj(hv))));
+    }
+    const cplx s = block_sum(acc);
+    if (threadIdx.x == 0) out[e * out_stride + out_col] = s;
+  }
+}
+}  // namespace
+
+void launch_block_dos(int n, int64_t batch, MatView g, double* out, int64_t out_stride, int out_col,
+                      cudaStream_t stream) {
+  if (!out) return;
+  const unsigned grid = (unsigned)(batch < 65535 ? batch : 65535);
+  block_dos_kernel<<<grid, TB, 0, stream>>>(n, batch, g.ptr, g.ld, g.stride, out, out_stride, out_col);
+  qtx_check_launch("block_dos_kernel");
+}
+
+void launch_layer_current(int n, int64_t batch, MatView xl, MatView xr, const double* occ_l, const double* occ_r,
+                          double sign_r, const cplx* coupling, cplx* out, int64_t out_stride, int out_col,
+                          cudaStream_t stream) {
+  if (!out) return;
+  const unsigned grid = (unsigned)(batch < 65535 ? batch : 65535);
+  layer_current_kernel<<<grid, TB, 0, stream>>>(n, batch, xl.ptr, xl.ld, xl.stride, xr.ptr, xr.ld, xr.stride, occ_l,
+                                                occ_r, sign_r, coupling, out, out_stride, out_col);
+  qtx_check_launch("layer_current_kernel");
+}

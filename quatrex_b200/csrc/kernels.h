@@ -106,6 +106,15 @@ void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t 
 void launch_keldysh_combine(int n, int64_t batch, MatView xl, MatView xr, const double* occ_l, const double* occ_r,
                             double sign_r, bool sym, cplx* out_l, int64_t stride_l, cplx* out_g, int64_t stride_g,
                             cudaStream_t stream);
+// out[e * out_stride + out_col] = -(1/n) sum_r Im g[r][r]   (per-block density of states of G^R)
+void launch_block_dos(int n, int64_t batch, MatView g, double* out, int64_t out_stride, int out_col,
+                      cudaStream_t stream);
+// out[e * out_stride + out_col] = sum_rc H[r][c] (-conj Y[r][c]) - Y[r][c] conj H[r][c] with Y the lesser
+// combination of (xl, xr) as in launch_keldysh_combine: the layer current across the interface whose
+// coupling block is H (one matrix for the whole batch) and whose G^< upper block is Y.
+void launch_layer_current(int n, int64_t batch, MatView xl, MatView xr, const double* occ_l, const double* occ_r,
+                          double sign_r, const cplx* coupling, cplx* out, int64_t out_stride, int out_col,
+                          cudaStream_t stream);
 // density[e * out_stride + out_col] = sum_r Im Y<_rr, hole[...] = -sum_r Im Y>_rr (either may be null)
 void launch_keldysh_density(int n, int64_t batch, MatView xl, MatView xr, const double* occ_l, const double* occ_r,
                             double* density, double* hole, int64_t out_stride, int out_col, cudaStream_t stream);
@@ -126,6 +135,8 @@ struct GroupedProblem {
   double *density = nullptr, *hole_density = nullptr, *transmission = nullptr;
   cplx *current_left = nullptr, *current_right = nullptr;
   int* sr_iterations = nullptr;
+  double* dos = nullptr;
+  cplx* layer_current = nullptr;
 };
 // Largest block size of the grouped solve.
 constexpr int GROUPED_MAX_B = 64;

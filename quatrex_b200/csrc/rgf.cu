@@ -945,7 +945,11 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
   auto out_ptr = [&](void* base, int64_t blocks_per_e, int blk) {
     return base ? reinterpret_cast<cplx*>(base) + (e0 * blocks_per_e + blk) * bb : nullptr;
   };
-  const bool uppers = O.gl_upper || O.gg_upper;
+  // the G^< upper blocks are formed whenever an output needs them
+  const bool uppers = O.gl_upper || O.gg_upper || O.layer_current;
+  const cplx* h_up = reinterpret_cast<const cplx*>(P.h_upper);
+  double* dos = O.dos ? O.dos + e0 * nb : nullptr;
+  cplx* lcur = O.layer_current ? reinterpret_cast<cplx*>(O.layer_current) + e0 * (nb - 1) : nullptr;
 
   // ---- first block: x_0 = inv(A_00 - Sigma^R_L), X_L,0 = x_0 (i Gamma_L) x_0^H
   // M_0 = (E + i eta) I - H_00 - Sigma^R_L
@@ -974,6 +978,7 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
   launch_keldysh_combine(b, ne, yl.view(n), yr.view(n), fl, fr, 1.0, true, out_ptr(O.gl_diag, nb, n), nb * bb,
                          out_ptr(O.gg_diag, nb, n), nb * bb, s);
   if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, out_at(O.gr_diag, nb, n), s);
+  launch_block_dos(b, ne, xr.view(n), dos, nb, n, s);
   launch_keldysh_density(b, ne, yl.view(n), yr.view(n), fl, fr, O.density ? O.density + e0 * nb : nullptr,
                          O.hole_density ? O.hole_density + e0 * nb : nullptr, nb, n, s);
   // contact current at the right contact uses the symmetrised G^<_nn, G^>_nn
@@ -1018,6 +1023,7 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     if (uppers)
       launch_keldysh_combine(b, ne, tv(7), tv(5), fl, fr, -1.0, false, out_ptr(O.gl_upper, nb - 1, i),
                              (nb - 1) * bb, out_ptr(O.gg_upper, nb - 1, i), (nb - 1) * bb, s);
+    launch_layer_current(b, ne, tv(7), tv(5), fl, fr, -1.0, h_up + i * bb, lcur, nb - 1, i, s);
     launch_keldysh_combine(b, ne, yl.view(i), yr.view(i), fl, fr, 1.0, true, out_ptr(O.gl_diag, nb, i), nb * bb,
                            out_ptr(O.gg_diag, nb, i), nb * bb, s);
     launch_keldysh_density(b, ne, yl.view(i), yr.view(i), fl, fr, O.density ? O.density + e0 * nb : nullptr,
@@ -1026,6 +1032,7 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
          prec);
     std::swap(xr.ptr[i], T[4]);
     if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(i), ZERO, {}, out_at(O.gr_diag, nb, i), s);
+    launch_block_dos(b, ne, xr.view(i), dos, nb, i, s);
   }
   if (O.current_left) {
     launch_keldysh_combine(b, ne, yl.view(0), yr.view(0), fl, fr, 1.0, true, T[6], bb, T[7], bb, s);
@@ -1077,7 +1084,7 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
            (uintptr_t)ne, (uintptr_t)prec, (uintptr_t)O.gr_diag, (uintptr_t)O.gr_upper, (uintptr_t)O.gr_lower,
            (uintptr_t)O.gl_diag, (uintptr_t)O.gl_upper, (uintptr_t)O.gg_diag, (uintptr_t)O.gg_upper,
            (uintptr_t)O.density, (uintptr_t)O.hole_density, (uintptr_t)O.transmission, (uintptr_t)O.current_left,
-           (uintptr_t)O.current_right};
+           (uintptr_t)O.current_right, (uintptr_t)O.dos, (uintptr_t)O.layer_current};
   // scalars are baked into the captured launches: they are part of the key
   for (double v : {P.eta, P.mu_left, P.mu_right, P.kt, P.sr_tol}) {
     uint64_t bits;
@@ -1195,6 +1202,8 @@ GroupedPlan grouped_plan(int32_t count, const qtx_transport_problem* p, const qt
     g.current_left = reinterpret_cast<cplx*>(y.current_left);
     g.current_right = reinterpret_cast<cplx*>(y.current_right);
     g.sr_iterations = y.sr_iterations;
+    g.dos = y.dos;
+    g.layer_current = reinterpret_cast<cplx*>(y.layer_current);
     plan.items += x.num_energies;
     plan.max_nb = std::max(plan.max_nb, x.num_blocks);
     if (x.num_energies > 0) {

@@ -475,6 +475,26 @@ __device__ cplx blk_trace_product(int n, const cplx* x, const cplx* y) {
   }
   return cta_sum<BT>(acc);
 }
+// -(1/n) sum_r Im g[r][r]: the block's density of states (G^R)
+template <int BT>
+__device__ double blk_block_dos(int n, const cplx* g) {
+  double acc = 0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) acc += g[r * n + r].y;
+  return -cta_sum<BT>(cmk(acc, 0)).x / n;
+}
+// sum_rc H[r][c] (-conj Y[r][c]) - Y[r][c] conj H[r][c], Y = f_L xl + s f_R xr:
+// the layer current across an interface with coupling H and G^< upper block Y
+template <int BT>
+__device__ cplx blk_layer_current(int n, const cplx* xl, const cplx* xr, double fl, double fr, double sign_r,
+                                  const cplx* h) {
+  cplx acc = cmk(0, 0);
+  for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+    const cplx y = keldysh_mix(fl, xl[q], sign_r * fr, xr[q]);
+    const cplx hv = h[q];
+    acc = cadd(acc, csub(cmul(hv, cmk(-y.x, y.y)), cmul(y, cconj(hv))));
+  }
+  return cta_sum<BT>(acc);
+}
 // (sum_r Im Y<_rr, -sum_r Im Y>_rr) of the combination above (sign 1)
 template <int BT>
 __device__ cplx blk_keldysh_density(int n, const cplx* xl, const cplx* xr, double fl, double fr) {
@@ -673,6 +693,10 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
   blk_keldysh_combine(n, XL(nl), XG(nl), f_l, f_r, 1.0, true, P->gl_diag ? P->gl_diag + o_diag : nullptr,
                       P->gg_diag ? P->gg_diag + o_diag : nullptr);
   if (P->gr_diag) blk_axpby(n, ONE, XR(nl), ONE, nullptr, P->gr_diag + o_diag);
+  if (P->dos) {
+    const double v = blk_block_dos<BT>(n, XR(nl));
+    if (threadIdx.x == 0) P->dos[e * nb + nl] = v;
+  }
   if (P->density || P->hole_density) {
     const cplx dh = blk_keldysh_density<BT>(n, XL(nl), XG(nl), f_l, f_r);
     if (threadIdx.x == 0) {
@@ -689,7 +713,7 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
   cplx* corner = T[8];
   cplx* corner2 = T[9];
   if (P->transmission) blk_axpby(n, ONE, XR(nl), ONE, nullptr, corner);
-  const bool uppers = P->gl_upper || P->gg_upper;
+  const bool uppers = P->gl_upper || P->gg_upper || P->layer_current;
   // ---- backward sweep
   cplx* g_next = XR(nl);  // G^R_jj of the block after i
   cplx* spare = T[4];
@@ -746,6 +770,10 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
     if (uppers)
       blk_keldysh_combine(n, T[7], T[5], f_l, f_r, -1.0, false, P->gl_upper ? P->gl_upper + o_up : nullptr,
                           P->gg_upper ? P->gg_upper + o_up : nullptr);
+    if (P->layer_current) {
+      const cplx v = blk_layer_current<BT>(n, T[7], T[5], f_l, f_r, -1.0, uu(i));
+      if (threadIdx.x == 0) P->layer_current[e * (nb - 1) + i] = v;
+    }
     const int64_t o_d = (e * nb + i) * bb;
     blk_keldysh_combine(n, XL(i), XG(i), f_l, f_r, 1.0, true, P->gl_diag ? P->gl_diag + o_d : nullptr,
                         P->gg_diag ? P->gg_diag + o_d : nullptr);
@@ -763,6 +791,10 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
     g_next = spare;
     spare = freed;
     if (P->gr_diag) blk_axpby(n, ONE, g_next, ONE, nullptr, P->gr_diag + (e * nb + i) * bb);
+    if (P->dos) {
+      const double v = blk_block_dos<BT>(n, g_next);
+      if (threadIdx.x == 0) P->dos[e * nb + i] = v;
+    }
   }
   if (P->current_left) {
     blk_keldysh_combine(n, XL(0), XG(0), f_l, f_r, 1.0, true, T[6], T[7]);

@@ -23,7 +23,8 @@ from quatrex_b200.workloads import TransportDevice
 _PRECISIONS = {"fp64": _lib.QTX_PREC_FP64, "mixed": _lib.QTX_PREC_MIXED}
 
 OUTPUT_KEYS = ("gr_diag", "gr_upper", "gr_lower", "gl_diag", "gl_upper", "gg_diag", "gg_upper", "density",
-               "hole_density", "transmission", "current_left", "current_right", "sr_iterations")
+               "hole_density", "transmission", "current_left", "current_right", "sr_iterations", "dos",
+               "layer_current")
 
 
 def allocate_outputs(num_blocks: int, block_size: int, num_energies: int, keys=OUTPUT_KEYS,
@@ -40,8 +41,10 @@ def allocate_outputs(num_blocks: int, block_size: int, num_energies: int, keys=O
     for k in keys:
         if k in shapes:
             out[k] = torch.empty(shapes[k], dtype=torch.complex128, device=dev)
-        elif k in ("density", "hole_density"):
+        elif k in ("density", "hole_density", "dos"):
             out[k] = torch.empty((ne, nb), dtype=torch.float64, device=dev)
+        elif k == "layer_current":
+            out[k] = torch.empty((ne, nb - 1), dtype=torch.complex128, device=dev)
         elif k == "transmission":
             out[k] = torch.empty((ne,), dtype=torch.float64, device=dev)
         elif k in ("current_left", "current_right"):
@@ -190,3 +193,32 @@ def solve_grouped(devices: list[TransportDevice], energies: list, keys=OUTPUT_KE
     st = lib.qtx_transport_solve_grouped(ctx, len(probs), p_arr, o_arr, _lib.QTX_PREC_FP64, 0, None, s)
     _lib.check(st, ctx, "transport_solve_grouped")
     return results
+
+
+# outputs derived from the Green's functions of an energy (zero when those are)
+_G_DERIVED_KEYS = ("gr_diag", "gr_upper", "gr_lower", "gl_diag", "gl_upper", "gg_diag", "gg_upper", "density",
+                   "hole_density", "transmission", "current_left", "current_right", "layer_current")
+
+
+def peak_mask(dos, energies, dos_peak_limit: float = 100.0):
+    """Energies whose Green's functions ``ElectronSolver._filter_peaks``
+    (``src/quatrex/electron/solver.py:412-454``) sets to zero: the largest
+    slope |d dos / dE| over the blocks above ``dos_peak_limit``, or the largest
+    block DOS above 10.  ``dos`` is the (num_energies, nb) 'dos' output over
+    the whole energy grid (a slope needs the neighbouring energies); the slope
+    is taken as numpy.gradient takes it: second-order central differences
+    inside the grid, one-sided differences at its ends."""
+    e = torch.as_tensor(np.asarray(energies, dtype=np.float64) if not isinstance(energies, torch.Tensor)
+                        else energies, dtype=torch.float64, device=dos.device)
+    slope = torch.gradient(dos, spacing=(e,), dim=0)[0].abs()
+    return (slope.amax(dim=1) > dos_peak_limit) | (dos.amax(dim=1) > 10)
+
+
+def filter_peaks(outputs: dict, mask) -> None:
+    """Zero, in place, the Green's-function blocks of the masked energies and
+    the observables formed from them (upstream filters G before its
+    observables are computed, so they vanish there too); 'dos' and
+    'sr_iterations' are kept."""
+    for k in _G_DERIVED_KEYS:
+        if k in outputs:
+            outputs[k][mask.to(outputs[k].device)] = 0

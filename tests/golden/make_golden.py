@@ -19,6 +19,11 @@ never runs on the GPU machine and nothing imports it.  It imports the upstream
 * ``transport_cfg_small_subset.npz`` -- nb=16, b=64 at 4 of its 32 energies;
   reduced outputs (per-block density, per-block Frobenius norms, contact
   currents, traces) so the file stays small.
+* ``observables_small.npz`` -- nb=5, b=8, 40 energies of the seeded transport
+  generator: upstream ``observables.device_current`` on the upstream G^< with
+  the Hamiltonian as the operator, the per-block density of states of
+  upstream G^R and the energies that upstream ``ElectronSolver._filter_peaks``
+  zeroes for a peak limit set to the median of the largest DOS slopes.
 
 Usage:  python tests/golden/make_golden.py
 """
@@ -32,6 +37,7 @@ import warnings
 
 import numpy as np
 
+sys.dont_write_bytecode = True  # nothing is written next to the upstream sources
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 UPSTREAM = os.environ.get("QTX_UPSTREAM", "/root/reference")
@@ -208,9 +214,45 @@ def transport_cfg_small_subset():
     print("transport_cfg_small_subset written")
 
 
+def observables_small():
+    from quatrex.core.observables import device_current
+    from quatrex.electron.solver import ElectronSolver
+
+    dev = make_device(num_blocks=5, block_size=8, num_energies=40, seed=21)
+    r = transport_reference(dev, dev.energies)
+    nb, b = 5, 8
+    n = nb * b
+    h = np.zeros((n, n), dtype=np.complex128)
+    for i in range(nb):
+        h[i * b:(i + 1) * b, i * b:(i + 1) * b] = dev.h_diag[i]
+        if i + 1 < nb:
+            h[i * b:(i + 1) * b, (i + 1) * b:(i + 2) * b] = dev.h_upper[i]
+            h[(i + 1) * b:(i + 2) * b, i * b:(i + 1) * b] = dev.h_upper[i].conj().T
+    current = device_current(r["xl"], sparse.coo_matrix(h))
+    # per-block DOS of upstream G^R, the quantity _filter_peaks differentiates
+    diag = r["xr"].diagonal()
+    dos = np.stack([-diag[..., i * b:(i + 1) * b].imag.mean(-1) for i in range(nb)], axis=-1)
+    slopes = np.abs(np.gradient(dos, dev.energies, axis=0)).max(axis=1)
+    limit = float(np.median(slopes))
+
+    class _Solver:  # the two attributes _filter_peaks reads
+        energies = dev.energies
+        dos_peak_limit = limit
+
+    xl, xg, xr = r["xl"], r["xg"], r["xr"]
+    before = np.abs(xr.data).sum(axis=-1)
+    ElectronSolver._filter_peaks(_Solver(), (xl, xg, xr))
+    mask = (np.abs(xr.data).sum(axis=-1) == 0) & (before > 0)
+    np.savez_compressed(os.path.join(HERE, "observables_small.npz"), h_diag=dev.h_diag, h_upper=dev.h_upper,
+                        energies=dev.energies, layer_current=np.asarray(current), dos=dos, peak_limit=limit,
+                        peak_mask=mask)
+    print("observables_small written", int(mask.sum()), "of", len(mask), "energies masked")
+
+
 if __name__ == "__main__":
     warnings.simplefilter("ignore", FutureWarning)
     btd_case("constant", [2] * 10, 10, seed=11)
     btd_case("mixed", [2, 2, 2, 4, 4, 2, 2, 2], 10, seed=12)
     transport_small()
     transport_cfg_small_subset()
+    observables_small()

@@ -20,7 +20,7 @@ from oracle import rgf_oracle as orc
 from quatrex_b200 import _lib
 from quatrex_b200.transport import TransportSolver, grouped_footprint_bytes, solve_grouped
 from quatrex_b200.workloads import make_device
-from test_gpu_transport import _oracle, _oracle_h, _per_energy_rel
+from test_gpu_transport import _layer_err, _oracle, _oracle_h, _per_energy_rel
 
 pytestmark = pytest.mark.gpu
 
@@ -67,6 +67,10 @@ def _check_oracle(dev, energies, out):
     i_l, i_r = orc.contact_currents(ref["xl_diag"][0], ref["xg_diag"][0], ref["xl_diag"][-1], ref["xg_diag"][-1], obc)
     check(out["current_left"], i_l, 10)
     check(out["current_right"], i_r, 10)
+    check(out["dos"], orc.block_dos(ref["xr_diag"]), 10)
+    err = _layer_err(out["layer_current"], orc.layer_current(ref["xl_upper"], dev.h_upper), ref["xl_upper"],
+                     dev.h_upper)
+    assert (err <= 10 * bound).all(), (err, bound)
     its = out["sr_iterations"].cpu().numpy()
     assert its.min() >= 1 and its.max() <= max(obc["iterations"]) + 1
     return bound
@@ -117,9 +121,11 @@ def test_grouped_equals_layered(b):
                 assert torch.equal(out[k], ref[k]), k
             err = _per_energy_rel(out[k], ref[k].cpu().numpy())
             assert (err <= bound).all(), (k, err, bound)
-        for k in ("density", "hole_density", "transmission", "current_left", "current_right"):
+        for k in ("density", "hole_density", "transmission", "current_left", "current_right", "dos"):
             err = _obs_err(k, out[k], ref[k].cpu().numpy())
             assert (err <= 10 * bound).all(), (k, err, bound)
+        err = _layer_err(out["layer_current"], ref["layer_current"].cpu().numpy(), ref["gl_upper"], d.h_upper)
+        assert (err <= 10 * bound).all(), ("layer_current", err, bound)
 
 
 def test_grouped_is_one_launch_for_uneven_devices():

@@ -72,6 +72,17 @@ def _oracle_spread(dev, energies, ref, trials=3):
     return spread
 
 
+
+def _layer_err(got, want, gl_upper, h_upper):
+    """Per-energy error of the layer currents (E, nb - 1), each against the size
+    of the terms its trace sums, ||G^<_ij||_F ||H_ij||_F: wherever f_L ~ f_R a
+    layer current is rounding noise of order one of those terms, so neither
+    its own size nor the device's largest current is a scale."""
+    got = got.cpu().numpy() if isinstance(got, torch.Tensor) else got
+    gl = gl_upper.cpu().numpy() if isinstance(gl_upper, torch.Tensor) else np.stack(gl_upper, axis=1)
+    scale = np.linalg.norm(gl, axis=(-2, -1)) * np.linalg.norm(h_upper, axis=(-2, -1))[None, :]
+    return (np.abs(got - want) / np.maximum(scale, 1e-300)).max(axis=1)
+
 @pytest.mark.parametrize("max_batch_size", [2, 100])
 def test_transport_blocks_and_observables(max_batch_size):
     dev = make_device(num_blocks=5, block_size=24, num_energies=6, seed=31)
@@ -100,6 +111,10 @@ def test_transport_blocks_and_observables(max_batch_size):
     i_l, i_r = orc.contact_currents(ref["xl_diag"][0], ref["xg_diag"][0], ref["xl_diag"][-1], ref["xg_diag"][-1], obc)
     check(out["current_left"], i_l, 10)
     check(out["current_right"], i_r, 10)
+    check(out["dos"], orc.block_dos(ref["xr_diag"]), 10)
+    err = _layer_err(out["layer_current"], orc.layer_current(ref["xl_upper"], dev.h_upper), ref["xl_upper"],
+                     dev.h_upper)
+    assert (err <= 10 * bound).all(), (err, bound)
     # the well-conditioned energies meet the plain 1e-10 bar
     assert (bound == 1e-10).sum() >= 4
     its = out["sr_iterations"].cpu().numpy()
@@ -127,3 +142,8 @@ def test_transport_ballistic_transmission_matches_current():
     f_r = orc.fermi_dirac(dev.energies - dev.mu_right, dev.kt)
     t_cur = (-out["current_left"].cpu().numpy() / (f_l - f_r)).real
     assert np.allclose(out["transmission"].cpu().numpy(), t_cur, rtol=1e-6, atol=1e-9)
+    # current conservation: every interface carries the same layer current, up
+    # to the leakage of the eta = 1e-6 broadening (< 1e-2 here, as for the
+    # interface currents of the selected solve in tests/test_oracle.py)
+    lay = out["layer_current"].cpu().numpy()
+    assert np.allclose(lay, lay[:, :1], rtol=1e-2, atol=1e-9 * np.abs(lay).max())

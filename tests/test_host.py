@@ -119,3 +119,26 @@ def test_transport_footprint_is_host_arithmetic():
     # the recursion state alone: 3 nb + 20 block stacks of 16 b^2 bytes per energy
     assert f16 - f8 >= 8 * (3 * 16 + 20) * 16 * 64 * 64
     assert lib.qtx_transport_footprint(1, 64, 8, _lib.QTX_PREC_FP64) == 0
+
+
+def test_peak_mask_matches_upstream_filter():
+    """quatrex_b200.transport.peak_mask (torch) picks the energies that upstream
+    ElectronSolver._filter_peaks zeroes (fixture written by the upstream code)."""
+    import torch
+
+    from oracle import rgf_oracle as orc
+    from quatrex_b200.transport import filter_peaks, peak_mask
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "observables_small.npz"))
+    dos = torch.from_numpy(g["dos"])
+    mask = peak_mask(dos, g["energies"], float(g["peak_limit"]))
+    assert np.array_equal(mask.numpy(), g["peak_mask"])
+    assert np.array_equal(mask.numpy(), orc.peak_mask(g["dos"], g["energies"], float(g["peak_limit"])))
+    # uneven spacing follows numpy.gradient too
+    e = np.sort(np.random.default_rng(0).uniform(-2, 2, 40))
+    got = torch.gradient(dos, spacing=(torch.from_numpy(e),), dim=0)[0].numpy()
+    assert np.allclose(got, np.gradient(g["dos"], e, axis=0), rtol=1e-12, atol=0)
+    out = {"density": torch.ones(40, 5), "dos": dos.clone(), "gl_diag": torch.ones(40, 5, 2, 2)}
+    filter_peaks(out, mask)
+    assert (out["density"][mask] == 0).all() and (out["density"][~mask] == 1).all()
+    assert (out["gl_diag"][mask] == 0).all() and torch.equal(out["dos"], dos)

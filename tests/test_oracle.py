@@ -84,6 +84,30 @@ def test_oracle_transport_small_against_upstream():
     assert nb == len(d)
 
 
+def test_oracle_observables_against_upstream():
+    """Layer current (upstream observables.device_current with the Hamiltonian),
+    per-block DOS and the energies upstream ElectronSolver._filter_peaks zeroes,
+    on the oracle's own solve of the fixture's device."""
+    g = np.load(os.path.join(GOLDEN, "observables_small.npz"))
+    dev = make_device(num_blocks=5, block_size=8, num_energies=40, seed=21)
+    assert np.array_equal(dev.h_diag, g["h_diag"]) and np.array_equal(dev.h_upper, g["h_upper"])
+    d, u, lo = dev.system_blocks()
+    obc = orc.obc_self_energies(d, u, lo, dev.energies, dev.mu_left, dev.mu_right, dev.kt, dev.sr_tol, dev.sr_max_iter)
+    pad = [None] * 3
+    zd = [np.zeros_like(x) for x in d]
+    zu = [np.zeros_like(x) for x in u]
+    res = orc.selected_solve(d, u, lo, zd, zu, zd, zu, [obc["retarded"][0], *pad, obc["retarded"][1]],
+                             [obc["lesser"][0], *pad, obc["lesser"][1]], [obc["greater"][0], *pad, obc["greater"][1]])
+    cur = orc.layer_current(res["xl_upper"], dev.h_upper)
+    assert cur.shape == g["layer_current"].shape == (40, 4)
+    assert np.abs(cur - g["layer_current"]).max() <= 1e-10 * np.abs(g["layer_current"]).max()
+    dos = orc.block_dos(res["xr_diag"])
+    assert _rel(dos, g["dos"]) < 1e-11
+    assert np.array_equal(orc.peak_mask(g["dos"], dev.energies, float(g["peak_limit"])), g["peak_mask"])
+    assert np.array_equal(orc.peak_mask(dos, dev.energies, float(g["peak_limit"])), g["peak_mask"])
+    assert 0 < g["peak_mask"].sum() < len(dev.energies)
+
+
 def test_oracle_transport_cfg_small_subset():
     g = np.load(os.path.join(GOLDEN, "transport_cfg_small_subset.npz"))
     dev = make_device(num_blocks=16, block_size=64, num_energies=32, seed=1234)
