@@ -142,3 +142,26 @@ def test_peak_mask_matches_upstream_filter():
     filter_peaks(out, mask)
     assert (out["density"][mask] == 0).all() and (out["density"][~mask] == 1).all()
     assert (out["gl_diag"][mask] == 0).all() and torch.equal(out["dos"], dos)
+
+
+def test_uneven_batch_job_plan():
+    """BatchedTransport.jobs: one grouped job per block size <= 64, the larger
+    instances one by one, every instance exactly once, longest job first; no
+    grouping when it is switched off."""
+    from types import SimpleNamespace
+
+    from quatrex_b200.batching import BatchedTransport, Instance, instance_flops
+
+    specs = [(6, 16, 8), (9, 32, 20), (4, 32, 5), (7, 64, 12), (5, 128, 9), (3, 512, 4), (8, 16, 3)]
+    insts = []
+    for q, (nb, b, ne) in enumerate(specs):
+        d = SimpleNamespace(num_blocks=nb, block_size=b)
+        insts.append(Instance(d, np.linspace(-1, 1, ne)))
+    jobs = BatchedTransport.jobs(SimpleNamespace(group_small=True), insts)
+    kinds = {tuple(sorted(idx)): kind for kind, idx in jobs}
+    assert kinds == {(0, 6): "group", (1, 2): "group", (3,): "group", (4,): "one", (5,): "one"}
+    assert sorted(i for _, idx in jobs for i in idx) == list(range(len(specs)))
+    cost = [sum(instance_flops(insts[i].device, len(insts[i].energies)) for i in idx) for _, idx in jobs]
+    assert cost == sorted(cost, reverse=True)
+    plain = BatchedTransport.jobs(SimpleNamespace(group_small=False), insts)
+    assert all(kind == "one" and len(idx) == 1 for kind, idx in plain) and len(plain) == len(specs)
