@@ -121,6 +121,25 @@ def test_transport_footprint_is_host_arithmetic():
     assert lib.qtx_transport_footprint(1, 64, 8, _lib.QTX_PREC_FP64) == 0
 
 
+def test_grouped_footprint_is_host_arithmetic():
+    """Work space of a grouped launch: one (3 nb_max + 20)-block work space per
+    resident CTA (never more CTAs than pairs), plus descriptors; block sizes
+    above 64 are not offered (0)."""
+    from quatrex_b200.transport import grouped_footprint_bytes
+
+    one = grouped_footprint_bytes([8], [1], 32)
+    assert one >= (3 * 8 + 20) * 16 * 32 * 32
+    # a longer device raises the per-CTA work space, more energies more CTAs
+    assert grouped_footprint_bytes([16], [1], 32) > one
+    assert grouped_footprint_bytes([8], [4], 32) > one
+    # the work space follows the longest device of the group
+    mixed = grouped_footprint_bytes([8, 16], [2, 2], 32)
+    assert mixed >= 4 * (3 * 16 + 20) * 16 * 32 * 32
+    assert grouped_footprint_bytes([8], [4], 64) > grouped_footprint_bytes([8], [4], 32)
+    assert grouped_footprint_bytes([8], [4], 65) == 0
+    assert grouped_footprint_bytes([8], [0], 32) == 0
+
+
 def test_peak_mask_matches_upstream_filter():
     """quatrex_b200.transport.peak_mask (torch) picks the energies that upstream
     ElectronSolver._filter_peaks zeroes (fixture written by the upstream code)."""
