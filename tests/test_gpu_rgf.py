@@ -260,3 +260,54 @@ def test_host_buffer_streaming_equals_device_path(max_batch_size):
     x_d = solver.selected_inv(Ad, obc_blocks=ob)
     assert isinstance(x_h.data, np.ndarray)
     assert np.array_equal(x_h.data, x_d.data.cpu().numpy())
+
+
+def test_coulomb_screening_call_pattern():
+    """The second upstream caller of the same solver, CoulombScreeningSolver.solve
+    (src/quatrex/coulomb_screening/solver.py:466-489): out=(W^<, W^>) of length
+    two with return_retarded=False, sources L^< and L^> on every block of the
+    pattern, mixed block sizes, and contact blocks (retarded, lesser, greater,
+    different per energy) at both ends.  Reference: the dense
+    W^R = (A - OBC^R)^-1 and W^≶ = W^R (L^≶ + OBC^≶) W^R^H per energy."""
+    rng = np.random.default_rng(77)
+    sizes = np.array([3, 5, 4, 4, 2])
+    ne = 6
+    offs = np.hstack(([0], np.cumsum(sizes)))
+    bt = _bt_dense(rng, sizes)
+    s = _bt_dense(rng, sizes)
+    srcs = {"lesser": s - s.conj().T, "greater": 2.0 * (s.conj().T - s)}
+    A = DSDBCOO.from_sparray(sparse.coo_matrix(bt), sizes, (ne,), device="cuda")
+    L = {k: DSDBCOO.from_sparray(sparse.coo_matrix(v), sizes, (ne,), device="cuda") for k, v in srcs.items()}
+    ob = OBCBlocks(len(sizes))
+
+    def rnd(b):
+        return 0.3 * (rng.standard_normal((ne, b, b)) + 1j * rng.standard_normal((ne, b, b)))
+
+    r0, rn = rnd(sizes[0]), rnd(sizes[-1])
+    ob.retarded[0], ob.retarded[-1] = r0, rn
+    obc_src = {}
+    for k in ("lesser", "greater"):
+        a0, an = rnd(sizes[0]), rnd(sizes[-1])
+        obc_src[k] = (a0 - a0.conj().swapaxes(-1, -2), an - an.conj().swapaxes(-1, -2))
+    ob.lesser[0], ob.lesser[-1] = obc_src["lesser"]
+    ob.greater[0], ob.greater[-1] = obc_src["greater"]
+    out = (DSDBCOO.zeros_like(A), DSDBCOO.zeros_like(A))
+    assert RGF(max_batch_size=4).selected_solve(A, L["lesser"], L["greater"], obc_blocks=ob, out=out,
+                                                return_retarded=False) is None
+    first, last = slice(offs[0], offs[1]), slice(offs[-2], offs[-1])
+    mask = np.broadcast_to(bt != 0, (ne,) + bt.shape)
+    for (k, src), x in zip(srcs.items(), out):
+        ref = np.empty((ne,) + bt.shape, dtype=np.complex128)
+        for e in range(ne):
+            a = bt.copy()
+            a[first, first] -= r0[e]
+            a[last, last] -= rn[e]
+            sig = src.copy()
+            sig[first, first] += obc_src[k][0][e]
+            sig[last, last] += obc_src[k][1][e]
+            wr = np.linalg.inv(a)
+            ref[e] = wr @ sig @ wr.conj().T
+        got = x.to_dense()
+        got = got.cpu().numpy() if isinstance(got, torch.Tensor) else got
+        assert _rel(got[mask], ref[mask]) < TOL, k
+        assert np.allclose(got[mask], ref[mask])
