@@ -63,8 +63,8 @@ def _flops_per_energy(nb, b, sr_iterations):
       forward step: A_ji x_i, Schur update, inverse,
                     3 for X_L (W = x_j A_ji, W X W^H)             =  6 per step
       last block: 2 products for X_R                                =  2
-      backward step: P1..P4, G^R_ji, corner chain, 4 for X_L,
-                     2 for X_R, x_i                                 = 13 per step
+      backward step: P1, P2, P4, G^R_ij, G^R_ji, corner chain,
+                     4 for X_L, 2 for X_R, x_i                      = 13 per step
       contacts: Sigma^R 2 x 2; transmission: 2                      =  6
       Sancho-Rubio: 7 per iteration + final inverse, per contact"""
     units = 3 + 2 + (nb - 1) * (6 + 13) + 6 + sum(7 * it + 1 for it in sr_iterations)

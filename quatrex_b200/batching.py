@@ -39,10 +39,11 @@ OBSERVABLE_KEYS = ("density", "hole_density", "transmission", "current_left", "c
 
 
 def instance_flops(dev: TransportDevice, num_energies: int) -> float:
-    """Algorithmic flops of one instance (8 b^3 per block product, 19 per
-    block step, Sancho-Rubio at ~22 iterations per contact)."""
+    """Algorithmic flops of one instance with observables only (8 b^3 per
+    block product; 17 per block step, the G^R off-diagonal outputs not being
+    formed; Sancho-Rubio at ~22 iterations per contact)."""
     b, nb = dev.block_size, dev.num_blocks
-    return 8.0 * b ** 3 * (19 * (nb - 1) + 11 + 2 * (7 * 22 + 1)) * num_energies
+    return 8.0 * b ** 3 * (17 * (nb - 1) + 11 + 2 * (7 * 22 + 1)) * num_energies
 
 
 class Worker:

@@ -997,9 +997,12 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     const int j = i + 1;
     gemm(b, b, b, ne, ONE, xr.view(i), OP_N, up(i), OP_N, tv(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
     gemm(b, b, b, ne, ONE, xr.view(j), OP_N, lo(i), OP_N, tv(1), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    gemm(b, b, b, ne, ONE, tv(0), OP_N, xr.view(j), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
+    // G^R_ij = -P1 G_jj: only an output, so written there directly (and
+    // skipped when it is not asked for)
+    if (O.gr_upper)
+      gemm(b, b, b, ne, MONE, tv(0), OP_N, xr.view(j), OP_N, out_at(O.gr_upper, nb - 1, i), s, {}, ZERO, {}, ZERO,
+           nullptr, nullptr, prec);
     gemm(b, b, b, ne, ONE, tv(0), OP_N, tv(1), OP_N, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    if (O.gr_upper) launch_axpby(b, b, ne, MONE, tv(2), ZERO, {}, out_at(O.gr_upper, nb - 1, i), s);
     if (O.gr_lower)
       gemm(b, b, b, ne, MONE, tv(1), OP_N, xr.view(i), OP_N, out_at(O.gr_lower, nb - 1, i), s, {}, ZERO, {}, ZERO,
            nullptr, nullptr, prec);

@@ -726,13 +726,14 @@ __device__ __noinline__ void solve_energy(const GroupedProblem* P, int pidx, int
     a = g0;  // P2 = G_jj A_ji = -G_jj U_i^H
     a.a = g_next; a.b = uu(i); a.opb = OP_C; a.d = T[1]; a.alpha = MONE;
     cta_gemm<BT>(a, n);
-    a = g0;  // P3 = P1 G_jj
-    a.a = T[0]; a.b = g_next; a.d = T[2];
-    cta_gemm<BT>(a, n);
+    if (P->gr_upper) {
+      a = g0;  // G^R_ij = -P1 G_jj, only an output
+      a.a = T[0]; a.b = g_next; a.d = P->gr_upper + o_up; a.alpha = MONE;
+      cta_gemm<BT>(a, n);
+    }
     a = g0;  // P4 = P1 P2
     a.a = T[0]; a.b = T[1]; a.d = T[3];
     cta_gemm<BT>(a, n);
-    if (P->gr_upper) blk_axpby(n, MONE, T[2], ONE, nullptr, P->gr_upper + o_up);
     if (P->gr_lower) {
       a = g0;
       a.a = T[1]; a.b = XR(i); a.d = P->gr_lower + o_up; a.alpha = MONE;
