@@ -173,3 +173,39 @@ def test_get_batches_matches_upstream_rule():
     assert orc.get_batches(10, 100)[0] == [10]
     assert orc.get_batches(7, 1)[0] == [1] * 7
     assert list(orc.get_batches(10, 2)[1]) == [0, 2, 4, 6, 8, 10]
+
+
+def test_keldysh_recursion_is_linear_in_the_contact_sources():
+    """The identity the generator-form kernels use: with the contacts as the
+    only sources (Sigma^<_c = i f_c Gamma_c, Sigma^>_c = i (f_c - 1) Gamma_c),
+    the recursion run once per contact source (i Gamma_L at the first block,
+    i Gamma_R at the last) and mixed with the occupations gives the G^< and
+    G^> of the component recursion, block for block."""
+    dev = make_device(num_blocks=5, block_size=8, num_energies=6, seed=17)
+    d, u, lo = dev.system_blocks()
+    obc = orc.obc_self_energies(d, u, lo, dev.energies, dev.mu_left, dev.mu_right, dev.kt, dev.sr_tol,
+                                dev.sr_max_iter)
+    nb = len(d)
+    zd = [np.zeros_like(x) for x in d]
+    zu = [np.zeros_like(x) for x in u]
+    pad = [None] * (nb - 2)
+    obc_r = [obc["retarded"][0], *pad, obc["retarded"][1]]
+
+    def solve(src0, srcn):
+        return orc.selected_solve(d, u, lo, zd, zu, zd, zu, obc_r, [src0, *pad, srcn], [src0, *pad, srcn])
+
+    full = orc.selected_solve(d, u, lo, zd, zu, zd, zu, obc_r, [obc["lesser"][0], *pad, obc["lesser"][1]],
+                              [obc["greater"][0], *pad, obc["greater"][1]])
+    zero_l, zero_r = np.zeros_like(obc["gamma"][0]), np.zeros_like(obc["gamma"][1])
+    x_l = solve(1j * obc["gamma"][0], zero_r)
+    x_r = solve(zero_l, 1j * obc["gamma"][1])
+    f_l = orc.fermi_dirac(dev.energies - dev.mu_left, dev.kt)[:, None, None]
+    f_r = orc.fermi_dirac(dev.energies - dev.mu_right, dev.kt)[:, None, None]
+    for part in ("diag", "upper"):
+        for i in range(len(full[f"xl_{part}"])):
+            want_l = full[f"xl_{part}"][i]
+            want_g = full[f"xg_{part}"][i]
+            got_l = f_l * x_l[f"xl_{part}"][i] + f_r * x_r[f"xl_{part}"][i]
+            got_g = (f_l - 1) * x_l[f"xl_{part}"][i] + (f_r - 1) * x_r[f"xl_{part}"][i]
+            assert _rel(got_l, want_l) < 1e-12, (part, i)
+            assert _rel(got_g, want_g) < 1e-12, (part, i)
