@@ -156,7 +156,8 @@ qtx_status qtx_selected_solve(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const vo
  * iterations (device, [batch], may be NULL) receives the iteration count of
  * each batch entry; converged entries stop iterating (per-entry masks).
  * Returns QTX_E_NOT_CONVERGED (after writing x) when an entry reached
- * max_iterations (sancho_rubio.py:81-82 warns in that case).
+ * max_iterations (sancho_rubio.py:81-82 warns in that case), QTX_E_SINGULAR
+ * when a decimation block was exactly singular.
  * <- SanchoRubio(max_iterations, convergence_tol)(a_ii, a_ij, a_ji, contact). */
 qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
                             const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
@@ -172,10 +173,12 @@ qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
  * work space is one fixed 16 MiB device array inside the library, held by
  * every GPU that loads it until the process exits.  A call needs about
  * 9 * 16 * n^2 * batch bytes of it; larger requests return QTX_E_INVAL with the
- * reason in `err` (optional caller buffer of err_len bytes).  The first call on
- * a device looks up the array's device address; make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race, so
- * serialise them.  The call synchronises `stream` (convergence checks). */
+ * reason in `err` (optional caller buffer of err_len bytes).  An exactly
+ * singular decimation block returns QTX_E_SINGULAR.  Every call looks up the
+ * array's address on the current device.  All calls share the array: calls
+ * that overlap on the GPU race, so serialise them.  The call synchronises
+ * `stream` after every iteration (convergence checks through pageable host
+ * memory), so it cannot run inside a stream capture. */
 qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
                                     const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
                                     double convergence_tol, int32_t max_iterations, void* x, int32_t* iterations,
@@ -355,12 +358,6 @@ int64_t qtx_graph_replays(const qtx_ctx* ctx);
  * synchronisation (safe while other threads capture or run).  No reference
  * counterpart: the reference captures no graphs. */
 qtx_status qtx_ctx_release_graphs(qtx_ctx* ctx, qtx_stream stream);
-
-/* FP64 roofline probe -- no counterpart in the upstream code.  Measures the
- * issue-rate ceiling of the FP64 tensor path (kind 0: DMMA mma.sync m8n8k4)
- * or of scalar DFMA (kind 1) on the current device, in TFLOP/s; the roofline
- * denominator of the FP64 kernels.  Synchronous. */
-qtx_status qtx_probe_fp64_peak(int32_t kind, double* tflops);
 
 /* Number of kernel launches this context has issued (for launch accounting). */
 int64_t qtx_launch_count(const qtx_ctx* ctx);

@@ -129,7 +129,6 @@ SIGNATURES = {
     "qtx_ctx_set_timing": (c_int32, [c_void_p, ctypes.c_int]),
     "qtx_ctx_timing_report": (
         c_int32, [c_void_p, c_int32, ctypes.POINTER(c_double), ctypes.POINTER(c_double), ctypes.POINTER(c_int64)]),
-    "qtx_probe_fp64_peak": (c_int32, [c_int32, ctypes.POINTER(c_double)]),
     "qtx_inv": (c_int32, [c_void_p, c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p]),
     "qtx_zgemm": (
         c_int32,

@@ -15,6 +15,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libqtxrgf.so")
+# the FP64 peak probe of kernel_bench (a measurement tool, kept out of libqtxrgf.so)
+PROBE_SRC = os.path.join(HERE, "probe", "peak_probe.cu")
+PROBE_LIB = os.path.join(HERE, "libqtxprobe.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -34,6 +37,15 @@ def _stale(lib: str, deps: list[str]) -> bool:
         return True
     t = os.path.getmtime(lib)
     return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_probe(force: bool = False) -> str:
+    if force or _stale(PROBE_LIB, [PROBE_SRC]):
+        tmp = PROBE_LIB + ".tmp"
+        subprocess.check_call([nvcc_path(), *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+                               "-cudart", "static", PROBE_SRC, "-o", tmp])
+        os.replace(tmp, PROBE_LIB)
+    return PROBE_LIB
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -71,3 +83,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_probe(force="--force" in sys.argv))

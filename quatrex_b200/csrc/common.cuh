@@ -89,6 +89,12 @@ inline void qtx_check_launch(const char* what) {
 
 inline unsigned ceil_div_u(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
+// Opt kernel `func` in to `bytes` of dynamic shared memory on the CURRENT
+// device.  The attribute is per device, so the library remembers the largest
+// value set for each (kernel, device) pair and sets it again on a device that
+// has not seen it.  Thread safe; throws QTX_E_CUDA when the runtime refuses.
+void qtx_opt_in_smem(const void* func, size_t bytes);
+
 // Stream-ordered allocation from the device's default pool.  The pool keeps
 // freed memory for reuse (release threshold unlimited); when a request does
 // not fit, the memory the pool holds unused is returned to the driver and the

@@ -49,8 +49,10 @@ size_t mixed_workspace_bytes(int m, int n, int k, int64_t a_batch, int64_t b_bat
 void mixed_check_error(cudaStream_t stream);
 
 // Batched in-place-capable Gauss-Jordan inverse with partial pivoting:
-// X = A^-1 for n x n matrices.  info[e] (device, optional) receives 0 or the
-// 1-based column of the first exactly-zero pivot.  X may alias A.
+// X = A^-1 for n x n matrices.  info[e] (device, optional) receives the
+// 1-based column of the first exactly-zero pivot and is left untouched when
+// there is none (callers zero it once and may read it after several
+// launches).  X may alias A.
 void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const int* active,
                  cudaStream_t stream);
 

@@ -16,6 +16,7 @@
 #include <deque>
 #include <exception>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -24,6 +25,18 @@
 #include "kernels.h"
 
 thread_local int64_t* g_qtx_launch_counter = nullptr;
+
+void qtx_opt_in_smem(const void* func, size_t bytes) {
+  static std::mutex m;
+  static std::map<std::pair<const void*, int>, size_t> set_bytes;
+  int dev = 0;
+  QTX_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(m);
+  size_t& have = set_bytes[{func, dev}];
+  if (bytes <= have) return;
+  QTX_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  have = bytes;
+}
 
 // Per-kernel-class CUDA-event timing of the launches a context issues
 // (enabled by qtx_ctx_set_timing): 0 = complex GEMM, 1 = inverse.
@@ -755,7 +768,7 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
 bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView a_ij, MatView a_ji, double tol,
                        int max_iter, MutView x, int* iterations, cudaStream_t s) {
   const size_t mat = (size_t)n * n * batch;
-  DevBuf buf(sizeof(cplx) * 9 * mat + sizeof(int) * (2 * batch + 2), s);
+  DevBuf buf(sizeof(cplx) * 9 * mat + sizeof(int) * (3 * batch + 2), s);
   cplx* p = buf.as<cplx>();
   auto slot = [&](int q) { return MutView{p + q * mat, n, (int64_t)n * n}; };
   MutView eps = slot(0), eps_s = slot(1), alpha = slot(2), beta = slot(3), inv = slot(4), t0 = slot(5),
@@ -763,6 +776,8 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
   int* active = reinterpret_cast<int*>(p + 9 * mat);
   int* its = active + batch;
   int* num_active = its + batch;
+  int* info = num_active + 2;  // zero pivots of the decimation inverses (sticky over the iterations)
+  QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
   launch_axpby(n, n, batch, ONE, a_ii, ZERO, {}, eps, s);
   launch_axpby(n, n, batch, ONE, a_ii, ZERO, {}, eps_s, s);
   launch_axpby(n, n, batch, ONE, a_ji, ZERO, {}, alpha, s);
@@ -771,7 +786,7 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
   QTX_CUDA_TRY(cudaMemsetAsync(its, 0, sizeof(int) * batch, s));
   bool converged = false;
   for (int it = 0; it < max_iter; ++it) {
-    zinv(n, batch, eps, inv, nullptr, active, s);
+    zinv(n, batch, eps, inv, info, active, s);
     gemm(n, n, n, batch, ONE, alpha, OP_N, inv, OP_N, t0, s, {}, ZERO, {}, ZERO, active);   // a inv
     gemm(n, n, n, batch, ONE, beta, OP_N, inv, OP_N, t1, s, {}, ZERO, {}, ZERO, active);    // b inv
     gemm(n, n, n, batch, ONE, t0, OP_N, beta, OP_N, t2, s, {}, ZERO, {}, ZERO, active);     // a inv b
@@ -791,8 +806,9 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
       break;
     }
   }
-  zinv(n, batch, eps_s, x, nullptr, nullptr, s);
+  zinv(n, batch, eps_s, x, info, nullptr, s);
   if (iterations) QTX_CUDA_TRY(cudaMemcpyAsync(iterations, its, sizeof(int) * batch, cudaMemcpyDeviceToDevice, s));
+  read_info_or_throw(ctx, info, batch, s, "sancho_rubio (decimation block)");
   return converged;
 }
 

@@ -845,20 +845,23 @@ __global__ void __launch_bounds__(GCfg<BT>::THREADS, GCfg<BT>::MIN_BLOCKS)
   }
 }
 
+// Resident CTAs of the persistent launch on the current device (host
+// arithmetic callers such as the footprint query may run without a device:
+// then one CTA per SM of a B200 is assumed).
 template <int BT>
 int resident_ctas() {
-  static const int per_sm = [] {
-    cudaFuncSetAttribute(transport_grouped_kernel<BT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem_bytes<BT>());
-    int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, transport_grouped_kernel<BT>, GCfg<BT>::THREADS,
-                                                    smem_bytes<BT>()) !=
-        cudaSuccess) {
-      cudaGetLastError();
-      blocks = 1;
-    }
-    return blocks < 1 ? 1 : blocks;
-  }();
+  try {
+    qtx_opt_in_smem((const void*)transport_grouped_kernel<BT>, smem_bytes<BT>());
+  } catch (const QtxError&) {
+    cudaGetLastError();
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, transport_grouped_kernel<BT>, GCfg<BT>::THREADS,
+                                                    smem_bytes<BT>()) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  if (per_sm < 1) per_sm = 1;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
     cudaGetLastError();
@@ -882,11 +885,11 @@ void launch_transport_grouped(int b, const GroupedProblem* problems, int count, 
   if (items <= 0 || grid <= 0) return;
   if (b < 1 || b > GROUPED_MAX_B) throw QtxError(QTX_E_UNSUPPORTED, "grouped transport: block size above 64");
   if (b <= 32) {
-    resident_ctas<32>();  // shared-memory opt-in
+    qtx_opt_in_smem((const void*)transport_grouped_kernel<32>, smem_bytes<32>());
     transport_grouped_kernel<32><<<grid, GCfg<32>::THREADS, smem_bytes<32>(), stream>>>(problems, count, items, counter, flags, ws,
                                                                          ws_elems, max_nb);
   } else {
-    resident_ctas<64>();
+    qtx_opt_in_smem((const void*)transport_grouped_kernel<64>, smem_bytes<64>());
     transport_grouped_kernel<64><<<grid, GCfg<64>::THREADS, smem_bytes<64>(), stream>>>(problems, count, items, counter, flags, ws,
                                                                          ws_elems, max_nb);
   }

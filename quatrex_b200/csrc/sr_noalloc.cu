@@ -15,9 +15,12 @@
 // cudaFree or any allocating routine.
 //
 // Use:
-//  - the first call on a device looks up the device address of the array
-//    (cudaGetSymbolAddress, once per device, with that device current); make
-//    that first call before any stream capture;
+//  - every call looks up the device address of the array on the current
+//    device (cudaGetSymbolAddress with that device current; cheap once the
+//    module is loaded, and never stale after a context teardown such as
+//    cudaDeviceReset);
+//  - a call cannot run inside a stream capture: each iteration copies the
+//    convergence count to pageable host memory and synchronises the stream;
 //  - all calls share the one array: calls that overlap on the GPU (different
 //    streams, or different host threads on the same device) race; serialise
 //    them on one stream;
@@ -25,22 +28,18 @@
 //    that must start at zero is cleared at the start of each call.
 #include <cstdio>
 #include <cstring>
-#include <mutex>
+#include <string>
+#include <vector>
 
 #include "kernels.h"
 
 namespace {
 
 constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(16) << 20;
-constexpr int MAX_DEVICES = 64;
 
+// The name g_sr_scratch in host code is only a host-side stand-in, never a
+// device address: kernels receive the address cudaGetSymbolAddress returns.
 static __device__ __align__(256) unsigned char g_sr_scratch[NOALLOC_SCRATCH_BYTES];
-
-// Host-side cache of the array's device address, per device.  The name
-// g_sr_scratch in host code is only a host-side stand-in, never a device
-// address, so kernels receive this looked-up address instead.
-void* g_scratch_addr[MAX_DEVICES] = {nullptr};
-std::mutex g_scratch_mutex;
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -63,7 +62,7 @@ extern "C" qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const v
     return QTX_E_INVAL;
   }
   const size_t mat_bytes = align_up(sizeof(cplx) * (size_t)n * n * batch, 256);
-  const size_t need = 9 * mat_bytes + align_up(sizeof(int) * (2 * (size_t)batch + 1), 256);
+  const size_t need = 9 * mat_bytes + align_up(sizeof(int) * (3 * (size_t)batch + 2), 256);
   if (need > NOALLOC_SCRATCH_BYTES) {
     char msg[256];
     std::snprintf(msg, sizeof(msg),
@@ -74,26 +73,17 @@ extern "C" qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const v
     set_err(err, err_len, msg);
     return QTX_E_INVAL;
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
-    cudaGetLastError();
-    set_err(err, err_len, "qtx_sancho_rubio_noalloc: no current CUDA device");
-    return QTX_E_CUDA;
-  }
+  // the array's address on the current device, looked up on every call
   unsigned char* base = nullptr;
   {
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
-      void* p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_sr_scratch);
-      if (e != cudaSuccess || !p) {
-        cudaGetLastError();
-        set_err(err, err_len, "qtx_sancho_rubio_noalloc: cudaGetSymbolAddress failed");
-        return QTX_E_CUDA;
-      }
-      g_scratch_addr[dev] = p;
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sr_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      set_err(err, err_len, "qtx_sancho_rubio_noalloc: cudaGetSymbolAddress failed (no usable current device?)");
+      return QTX_E_CUDA;
     }
-    base = static_cast<unsigned char*>(g_scratch_addr[dev]);
+    base = static_cast<unsigned char*>(p);
   }
 
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -104,6 +94,7 @@ extern "C" qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const v
   int* active = reinterpret_cast<int*>(base + 9 * mat_bytes);
   int* its = active + batch;
   int* num_active = its + batch;
+  int* info = num_active + 2;  // zero pivots of the decimation inverses (sticky over the iterations)
   MatView aii{reinterpret_cast<const cplx*>(a_ii), n, stride_ii};
   MatView aij{reinterpret_cast<const cplx*>(a_ij), n, stride_ij};
   MatView aji{reinterpret_cast<const cplx*>(a_ji), n, stride_ji};
@@ -125,10 +116,11 @@ extern "C" qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const v
     launch_axpby(n, n, batch, ONE, aji, ZERO, MatView{}, alpha, s);
     launch_axpby(n, n, batch, ONE, aij, ZERO, MatView{}, beta, s);
     launch_fill_int(active, batch, 1, s);
-    if (cudaMemsetAsync(its, 0, sizeof(int) * (size_t)batch, s) != cudaSuccess)
+    if (cudaMemsetAsync(its, 0, sizeof(int) * (size_t)batch, s) != cudaSuccess ||
+        cudaMemsetAsync(info, 0, sizeof(int) * (size_t)batch, s) != cudaSuccess)
       throw QtxError(QTX_E_CUDA, "cudaMemsetAsync failed");
     for (int it = 0; it < max_iterations; ++it) {
-      launch_zinv(n, batch, eps, inv, nullptr, active, s);
+      launch_zinv(n, batch, eps, inv, info, active, s);
       mm(ONE, alpha, inv, t0);                               // a inv
       mm(ONE, beta, inv, t1);                                // b inv
       mm(ONE, t0, beta, t2);                                 // a inv b
@@ -150,11 +142,19 @@ extern "C" qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const v
         break;
       }
     }
-    launch_zinv(n, batch, eps_s, MutView{reinterpret_cast<cplx*>(x), n, (int64_t)n * n}, nullptr, nullptr, s);
+    launch_zinv(n, batch, eps_s, MutView{reinterpret_cast<cplx*>(x), n, (int64_t)n * n}, info, nullptr, s);
     if (iterations &&
         cudaMemcpyAsync(iterations, its, sizeof(int) * (size_t)batch, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
       throw QtxError(QTX_E_CUDA, "iteration count copy failed");
-    if (cudaStreamSynchronize(s) != cudaSuccess) throw QtxError(QTX_E_CUDA, "stream synchronisation failed");
+    // pivot status of every batch entry, into pageable host memory
+    std::vector<int> h_info((size_t)batch);
+    if (cudaMemcpyAsync(h_info.data(), info, sizeof(int) * (size_t)batch, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      throw QtxError(QTX_E_CUDA, "pivot status readback failed");
+    for (int64_t e = 0; e < batch; ++e)
+      if (h_info[(size_t)e])
+        throw QtxError(QTX_E_SINGULAR, "qtx_sancho_rubio_noalloc: exactly singular decimation block (batch entry " +
+                                           std::to_string(e) + ", pivot " + std::to_string(h_info[(size_t)e]) + ")");
   } catch (const QtxError& e) {
     set_err(err, err_len, e.msg.c_str());
     return e.code;

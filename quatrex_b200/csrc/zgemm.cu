@@ -216,12 +216,8 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_dmma_kernel(Params p) {
 
 template <int OPA, int OPB>
 void launch_t(const Params& p, cudaStream_t stream) {
-  // thread-safe one-time opt-in to the large shared-memory carve-out
-  static const bool configured = [] {
-    cudaFuncSetAttribute(zgemm_dmma_kernel<OPA, OPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    return true;
-  }();
-  (void)configured;
+  // opt-in to the large shared-memory carve-out (per device)
+  qtx_opt_in_smem((const void*)zgemm_dmma_kernel<OPA, OPB>, SMEM_BYTES);
   dim3 grid(ceil_div_u(p.n, BN), ceil_div_u(p.m, BM), (unsigned)(p.batch < 65535 ? p.batch : 65535));
   zgemm_dmma_kernel<OPA, OPB><<<grid, THREADS, SMEM_BYTES, stream>>>(p);
 }

@@ -732,15 +732,7 @@ void launch_zgemm_mixed(const GemmCall& g, cudaStream_t stream) {
   // as many stages as fit next to the barrier words (S = 7: 2, S <= 6: 3)
   p.nst = std::min<int>(MAX_STAGES, (MAX_SMEM - BAR_BYTES) / stage_bytes);
   const size_t smem = (size_t)p.nst * stage_bytes + BAR_BYTES;
-  {
-    static std::mutex m;
-    static size_t configured = 0;
-    std::lock_guard<std::mutex> lk(m);
-    if (smem > configured) {
-      QTX_CUDA_TRY(cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      configured = smem;
-    }
-  }
+  qtx_opt_in_smem((const void*)ozaki_gemm_kernel, smem);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

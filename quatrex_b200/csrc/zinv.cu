@@ -26,8 +26,6 @@
 // matrices); shared memory holds the panel (n x Wp, XOR-swizzled so that both
 // row-per-thread access and DMMA fragment loads are conflict-free), two slabs
 // of pivot rows and the permutation arrays.
-#include <mutex>
-
 #include "kernels.h"
 
 namespace {
@@ -537,7 +535,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         __syncthreads();
       }
     }
-    if (info && tid == 0) info[e] = zero_pivot;
+    // sticky: callers zero info once and read it after several launches
+    if (info && tid == 0 && zero_pivot) info[e] = zero_pivot;
     __syncthreads();
   }
 }
@@ -549,15 +548,7 @@ namespace {
 template <int TPR, int RPT, int CPT>
 void launch_inv_t(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, size_t smem,
                   cudaStream_t stream) {
-  {
-    static std::mutex m;
-    static size_t configured = 0;
-    std::lock_guard<std::mutex> lk(m);
-    if (smem > configured) {
-      cudaFuncSetAttribute(zinv_gj_kernel<TPR, RPT, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      configured = smem;
-    }
-  }
+  qtx_opt_in_smem((const void*)zinv_gj_kernel<TPR, RPT, CPT>, smem);
   int grid = (int)(batch < 65535 ? batch : 65535);
   zinv_gj_kernel<TPR, RPT, CPT><<<grid, THREADS, smem, stream>>>(n, batch, a.ptr, a.ld, a.stride, x.ptr, x.ld,
                                                                   x.stride, info, active);

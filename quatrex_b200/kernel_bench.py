@@ -152,13 +152,17 @@ def bench_grouped(b: int, instances: int) -> dict:
 
 
 def probe_fp64_peak() -> dict:
-    lib = _lib.load()
+    from quatrex_b200.build import PROBE_LIB
+
+    lib = ctypes.CDLL(PROBE_LIB)
+    lib.qtx_probe_fp64_peak.restype = ctypes.c_int32
+    lib.qtx_probe_fp64_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
     out = {}
     for kind, name in ((0, "dmma_m8n8k4_tflops"), (1, "dfma_tflops")):
         v = ctypes.c_double()
         torch.cuda.init()
         st = lib.qtx_probe_fp64_peak(kind, ctypes.byref(v))
-        if st != _lib.QTX_OK:
+        if st != 0:
             raise RuntimeError(f"qtx_probe_fp64_peak failed with status {st}")
         out[name] = v.value
     return {"kernel": "fp64_peak_probe", **out}

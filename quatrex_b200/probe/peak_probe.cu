@@ -1,9 +1,18 @@
-// FP64 peak probe: the issue-rate ceiling of the FP64 tensor path (DMMA,
-// mma.sync m8n8k4 f64) and of scalar DFMA on this GPU, used as the roofline
-// denominator of the FP64 kernels (the driver-measured peaks cover HBM and bf16
-// only).  Each warp issues independent accumulator chains with no memory
-// traffic; the result is flops / elapsed time over the whole grid.
-#include "kernels.h"
+// FP64 peak probe (measurement tool, not part of libqtxrgf.so): the
+// issue-rate ceiling of the FP64 tensor path (DMMA, mma.sync m8n8k4 f64) and of
+// scalar DFMA on this GPU, used as the roofline denominator of the FP64
+// kernels (the measured peaks of the GPU pool cover HBM and bf16 only).  Each
+// warp issues independent accumulator chains with no memory traffic; the
+// result is flops / elapsed time over the whole grid.  Built into its own
+// libqtxprobe.so by quatrex_b200/build.py and called only by
+// `python -m quatrex_b200.kernel_bench fp64peak`.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define QTX_OK 0
+#define QTX_E_INVAL 1
+#define QTX_E_CUDA 6
+typedef int qtx_status;
 
 namespace {
 

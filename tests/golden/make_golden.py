@@ -1,7 +1,7 @@
 """Generate the golden fixtures under tests/golden/ by running the UPSTREAM code.
 
 This script is run by hand in a container where the upstream repository is
-checked out (default ``/root/reference``, override with ``QTX_UPSTREAM``); it
+checked out (its root given by the required ``QTX_UPSTREAM`` variable); it
 never runs on the GPU machine and nothing imports it.  It imports the upstream
 ``qttools`` package (NumPy backend) through a single-rank ``mpi4py`` stand-in
 (``tests/golden/_mpi_shim``) and records, for seeded inputs:
@@ -25,7 +25,7 @@ never runs on the GPU machine and nothing imports it.  It imports the upstream
   upstream G^R and the energies that upstream ``ElectronSolver._filter_peaks``
   zeroes for a peak limit set to the median of the largest DOS slopes.
 
-Usage:  python tests/golden/make_golden.py
+Usage:  QTX_UPSTREAM=<upstream checkout> python tests/golden/make_golden.py
 """
 
 from __future__ import annotations
@@ -40,7 +40,10 @@ import numpy as np
 sys.dont_write_bytecode = True  # nothing is written next to the upstream sources
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-UPSTREAM = os.environ.get("QTX_UPSTREAM", "/root/reference")
+UPSTREAM = os.environ.get("QTX_UPSTREAM")
+if not UPSTREAM or not os.path.isdir(os.path.join(UPSTREAM, "src", "qttools")):
+    sys.exit("make_golden.py: set QTX_UPSTREAM to the root of an upstream quatrex checkout "
+             "(the directory that holds src/qttools)")
 
 os.environ["QTX_ARRAY_MODULE"] = "numpy"
 os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "qtx_numba_cache"))

@@ -138,6 +138,27 @@ def test_sancho_rubio_not_converged_warns():
         SanchoRubio(max_iterations=1, convergence_tol=1e-12)(d[0], u[0], lo[0], "left")
 
 
+def test_sancho_rubio_singular_decimation_block():
+    """An exactly singular decimation block is reported (QTX_E_SINGULAR ->
+    LinAlgError), not passed on as silent NaN; the context stays usable."""
+    n, ne = 8, 2
+    a_ii = torch.zeros(ne, n, n, dtype=torch.complex128, device="cuda")
+    a_ij = torch.eye(n, dtype=torch.complex128, device="cuda").repeat(ne, 1, 1)
+    x = torch.empty_like(a_ii)
+    lib = _lib.load()
+    ctx = _lib.context(0)
+    st = lib.qtx_sancho_rubio(ctx, n, ne, a_ii.data_ptr(), n * n, a_ij.data_ptr(), n * n, a_ij.data_ptr(), n * n,
+                              1e-12, 3, x.data_ptr(), None, 0)
+    assert st == _lib.QTX_E_SINGULAR
+    with pytest.raises(np.linalg.LinAlgError):
+        SanchoRubio(max_iterations=3, convergence_tol=1e-12)(a_ii, a_ij, a_ij, "left")
+    dev = make_device(num_blocks=2, block_size=8, num_energies=2, seed=3)
+    d, u, lo = dev.system_blocks()
+    x_ok = SanchoRubio(max_iterations=200, convergence_tol=1e-12)(d[0], u[0], lo[0], "left")
+    x_ref, _ = orc.sancho_rubio(d[0], u[0], lo[0], 200, 1e-12)
+    assert _rel(x_ok, x_ref) < 1e-10
+
+
 def test_contact_self_energies_match_oracle():
     dev = make_device(num_blocks=3, block_size=16, num_energies=5, seed=2)
     d, u, lo = dev.system_blocks()
