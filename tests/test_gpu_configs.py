@@ -17,7 +17,10 @@ Green's function, and through it every block, by up to 6e-9.  So
 1. the CUDA path is compared with the oracle's selected solve fed with the
    surface Green's functions that the CUDA Sancho-Rubio produced (the contact
    self-energies, Fermi functions and every RGF product are still the
-   oracle's): 1e-10 per block at EVERY energy;
+   oracle's): 1e-10 per block at EVERY energy of the nb=16, b=64 device; at
+   nb=64, b=256 the selected solve's own sensitivity reaches 6e-10 in the G^<
+   blocks at one energy, so G^< and G^> are held there to 20 x that measured
+   spread and G^R to the plain bar;
 2. it is compared with the oracle end to end (the oracle's own Sancho-Rubio)
    with the per-energy bound max(1e-10, 20 x the oracle's spread under two
    1e-16 perturbations of H), and the plain 1e-10 bar holds at every energy
@@ -108,19 +111,47 @@ def _oracle_spread(dev, energies, ref, trials=2):
     return spread
 
 
-def _check_transport_blocks(out, ref, nb, bound):
-    """Every returned block of the generator form against an oracle result."""
-    worst = np.zeros_like(bound)
-    for i in range(nb):
-        for got, want in ((out["gr_diag"][:, i], ref["xr_diag"][i]), (out["gl_diag"][:, i], ref["xl_diag"][i]),
-                          (out["gg_diag"][:, i], ref["xg_diag"][i])):
-            worst = np.maximum(worst, _block_rel(got, want))
-    for i in range(nb - 1):
-        for got, want in ((out["gr_upper"][:, i], ref["xr_upper"][i]), (out["gr_lower"][:, i], ref["xr_lower"][i]),
-                          (out["gl_upper"][:, i], ref["xl_upper"][i]), (out["gg_upper"][:, i], ref["xg_upper"][i])):
-            worst = np.maximum(worst, _block_rel(got, want))
-    assert (worst <= bound).all(), (worst, bound)
+# returned blocks of the generator form: (output key, oracle key, block class)
+_BLOCKS = (("gr_diag", "xr_diag", "r"), ("gr_upper", "xr_upper", "r"), ("gr_lower", "xr_lower", "r"),
+           ("gl_diag", "xl_diag", "l"), ("gl_upper", "xl_upper", "l"), ("gg_diag", "xg_diag", "g"),
+           ("gg_upper", "xg_upper", "g"))
+
+
+def _worst_per_class(out, ref):
+    """Per energy and block class (G^R, G^<, G^>), the worst relative error
+    over every returned block of that class."""
+    ne = len(ref["xr_diag"][0])
+    worst = {c: np.zeros(ne) for c in "rlg"}
+    for key, rkey, cls in _BLOCKS:
+        for i in range(len(ref[rkey])):
+            worst[cls] = np.maximum(worst[cls], _block_rel(out[key][:, i], ref[rkey][i]))
     return worst
+
+
+def _check_transport_blocks(out, ref, nb, bound):
+    """Every returned block of the generator form against an oracle result;
+    `bound` is one per-energy array for every block, or one per block class."""
+    worst = _worst_per_class(out, ref)
+    bounds = bound if isinstance(bound, dict) else {c: bound for c in "rlg"}
+    for c in "rlg":
+        assert (worst[c] <= bounds[c]).all(), (c, worst[c], bounds[c])
+    return np.maximum(np.maximum(worst["r"], worst["l"]), worst["g"])
+
+
+def _rgf_spread(d, u, lo, obc, ref, trials=1):
+    """Per energy and block class, the relative change of the oracle's own
+    selected solve under a 1e-16 relative perturbation of the diagonal blocks
+    of A, with the contact blocks held fixed."""
+    rng = np.random.default_rng(7)
+    spread = {c: np.zeros(len(d[0])) for c in "rlg"}
+    for _ in range(trials):
+        d2 = [x * (1 + 1e-16 * rng.standard_normal(x.shape)) for x in d]
+        r2 = _oracle_solve(d2, u, lo, obc)
+        out2 = {key: np.stack(r2[rkey], axis=1) for key, rkey, _ in _BLOCKS}
+        w = _worst_per_class(out2, ref)
+        for c in "rlg":
+            spread[c] = np.maximum(spread[c], w[c])
+    return spread
 
 
 def _check_observables(out, ref, obc, bound):
@@ -215,18 +246,26 @@ def test_config_small_dropin_every_block_every_energy():
 
 
 def test_config_large_three_energies_every_block():
-    """nb=64, b=256 at energies 100, 500 and 900 of its 1024-point grid: every
-    returned block at 1e-10 against the oracle's selected solve on the CUDA
-    surface Green's functions, and against the oracle end to end within the
-    conditioning bound."""
+    """nb=64, b=256 at energies 100, 500 and 900 of its 1024-point grid,
+    against the oracle's selected solve on the CUDA surface Green's functions:
+    every G^R block (diagonal, upper, lower) at 1e-10; every G^< and G^> block
+    at max(1e-10, 20 x the oracle's own spread).  At this size the oracle's
+    selected solve is itself stable only to ~6e-10 in the G^< blocks at the
+    energy where G^< is a small difference of nearly equal terms (index 900,
+    f_L ~ f_R ~ 0), and to ~2e-11 in G^R.  Then against the oracle end to end
+    within the Sancho-Rubio conditioning bound."""
     dev, e, d, u, lo, out, obc_gpu, ref_gpu = _config_run(CONFIG_LARGE, CFG2_ENERGY_INDEX)
-    bound = np.full(len(e), BAR)
-    _check_transport_blocks(out, ref_gpu, dev.num_blocks, bound)
-    _check_observables(out, ref_gpu, obc_gpu, bound)
+    spread = _rgf_spread(d, u, lo, obc_gpu, ref_gpu)
+    assert (spread["r"] < 5e-11).all(), spread["r"]
+    bounds = {"r": np.full(len(e), BAR), "l": np.maximum(BAR, 20 * spread["l"]),
+              "g": np.maximum(BAR, 20 * spread["g"])}
+    _check_transport_blocks(out, ref_gpu, dev.num_blocks, bounds)
+    _check_observables(out, ref_gpu, obc_gpu, np.maximum(BAR, 20 * spread["l"]))
     obc_ref = orc.obc_self_energies(d, u, lo, e, dev.mu_left, dev.mu_right, dev.kt, dev.sr_tol, dev.sr_max_iter)
     ref = _oracle_solve(d, u, lo, obc_ref)
-    spread = _oracle_spread(dev, e, ref, trials=1)
-    _check_transport_blocks(out, ref, dev.num_blocks, np.maximum(BAR, 20 * spread))
+    spread_e2e = _oracle_spread(dev, e, ref, trials=1)
+    worst_rgf = np.maximum(np.maximum(spread["r"], spread["l"]), spread["g"])
+    _check_transport_blocks(out, ref, dev.num_blocks, np.maximum(BAR, 20 * np.maximum(spread_e2e, worst_rgf)))
 
 
 def test_config_mixed_precision_on_small_inputs():

@@ -226,3 +226,18 @@ def test_assemble_system_matches_formula(with_overlap):
         full = (e[k] + 1e-3j) * sm - np.diag(v) - hm
         want = full[H.rows, H.cols] - sig[k]
         assert np.allclose(got[k], want, rtol=0, atol=1e-13)
+
+
+@pytest.mark.skipif(not torch.cuda.is_available() or torch.cuda.device_count() < 2,
+                    reason="needs two visible CUDA devices")
+def test_two_devices_in_one_process():
+    """The large shared-memory opt-in of the GEMM and inverse kernels is a
+    per-device attribute: a solve on a second device after the first has used
+    the library must still launch (and agree with the oracle)."""
+    dev = make_device(num_blocks=3, block_size=64, num_energies=4, seed=7)
+    d, u, lo = dev.system_blocks()
+    x_ref, _ = orc.sancho_rubio(d[0], u[0], lo[0], 200, 1e-12)
+    for k in (0, 1):
+        with torch.cuda.device(k):
+            x = SanchoRubio(max_iterations=200, convergence_tol=1e-12)(d[0], u[0], lo[0], "left")
+            assert _rel(x, x_ref) < 1e-10
