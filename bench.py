@@ -137,6 +137,7 @@ def cpu_baseline(cfg, sample_energies: int, threads_note: dict):
     dev = make_device(**cfg)
     idx = np.linspace(0, cfg["num_energies"] - 1, sample_energies).round().astype(int)
     e = dev.energies[idx]
+    results = []
     t0 = time.perf_counter()
     for k in range(len(e)):
         ek = e[k:k + 1]
@@ -149,10 +150,32 @@ def cpu_baseline(cfg, sample_energies: int, threads_note: dict):
         ref = orc.selected_solve(d, u, lo, z, zu, z, zu, [obc["retarded"][0], *pad, obc["retarded"][1]],
                                  [obc["lesser"][0], *pad, obc["lesser"][1]],
                                  [obc["greater"][0], *pad, obc["greater"][1]], return_extras=True)
-        orc.caroli_transmission(ref["xr_corner"], obc["gamma"][0], obc["gamma"][1])
-        orc.block_density(ref["xl_diag"])
+        trans = orc.caroli_transmission(ref["xr_corner"], obc["gamma"][0], obc["gamma"][1])
+        dens = orc.block_density(ref["xl_diag"])
+        results.append({"gr_diag": np.stack(ref["xr_diag"], axis=1)[0], "gl_diag": np.stack(ref["xl_diag"], axis=1)[0],
+                        "density": dens[0], "transmission": float(trans[0])})
     dt = time.perf_counter() - t0
-    return len(e) / dt, dt, idx
+    return len(e) / dt, dt, idx, results
+
+
+def accuracy_against_oracle(gpu: dict, oracle_results: list) -> dict:
+    """Largest error over the sampled energies of one GPU form against the
+    oracle (end to end: the oracle's own Sancho-Rubio): G^R and G^< diagonal
+    blocks (relative Frobenius per block), per-block density (relative to the
+    energy's largest block), transmission (relative)."""
+    err = {"gr_diag_block_rel_max": 0.0, "gl_diag_block_rel_max": 0.0, "density_rel_max": 0.0,
+           "transmission_rel_max": 0.0}
+    for k, ref in enumerate(oracle_results):
+        for key, name in (("gr_diag", "gr_diag_block_rel_max"), ("gl_diag", "gl_diag_block_rel_max")):
+            got = gpu[key][k]
+            num = np.linalg.norm(got - ref[key], axis=(-2, -1))
+            den = np.maximum(np.linalg.norm(ref[key], axis=(-2, -1)), 1e-300)
+            err[name] = max(err[name], float((num / den).max()))
+        err["density_rel_max"] = max(err["density_rel_max"], float(
+            np.abs(gpu["density"][k] - ref["density"]).max() / max(np.abs(ref["density"]).max(), 1e-300)))
+        err["transmission_rel_max"] = max(err["transmission_rel_max"], float(
+            abs(gpu["transmission"][k] - ref["transmission"]) / max(abs(ref["transmission"]), 1e-12)))
+    return err
 
 
 def blas_threads() -> dict:
@@ -180,7 +203,7 @@ def run_reference(args):
     for _ in range(args.warmup):
         cpu_baseline(cfg, 1, bt)
     for _ in range(args.steps):
-        rate, dt, _ = cpu_baseline(cfg, args.ref_energies_per_step, bt)
+        rate, dt, _, _ = cpu_baseline(cfg, args.ref_energies_per_step, bt)
         total += dt
         solves += args.ref_energies_per_step
     value = solves / total
@@ -269,38 +292,19 @@ def run_ours(args):
     elapsed_ms = max_over_ranks(elapsed_ms, device=f"cuda:{local}")
     value = world * args.steps * E / (elapsed_ms / 1000.0)
 
-    # ---- end to end through the public API: H and energies from pinned host memory,
-    # observables back to pinned host memory, every step
+    # ---- end to end through the public API (TransportSolver.solve over
+    # qtx_transport_solve): every step copies H and its energies in from
+    # pinned host memory and copies back to pinned host memory every diagonal
+    # block of G^R, G^< and G^> (the blocks the density, the DOS and the
+    # carrier statistics are read from) plus the observables.  The outputs are
+    # double buffered on the device so that the download of step k runs on a
+    # copy stream while step k + 1 solves; the timed region ends when the
+    # last download has landed.
+    del out
+    torch.cuda.empty_cache()
     e2e = None
     if not args.no_e2e:
-        h_diag_host = torch.from_numpy(dev.h_diag).pin_memory()
-        h_upper_host = torch.from_numpy(dev.h_upper).pin_memory()
-        e_host = [step_energies(k).cpu().pin_memory() for k in range(args.steps)]
-        obs_keys = ("density", "hole_density", "transmission", "current_left", "current_right", "sr_iterations")
-        host_obs = {k: torch.empty(out[k].shape, dtype=out[k].dtype).pin_memory() for k in obs_keys}
-        h_diag_dev = torch.empty_like(solver.h_diag)
-        h_upper_dev = torch.empty_like(solver.h_upper)
-        e_dev = torch.empty(E, dtype=torch.float64, device=f"cuda:{local}")
-        s2 = TransportSolver(dev, max_batch_size=E, precision=args.precision, cuda_device=local,
-                             h_diag=h_diag_dev, h_upper=h_upper_dev)
-        h2d = h_diag_host.numel() * 16 + h_upper_host.numel() * 16 + E * 8
-        d2h = sum(v.numel() * v.element_size() for v in host_obs.values())
-        barrier()
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for k in range(args.steps):
-            h_diag_dev.copy_(h_diag_host, non_blocking=True)
-            h_upper_dev.copy_(h_upper_host, non_blocking=True)
-            e_dev.copy_(e_host[k], non_blocking=True)
-            s2.solve(e_dev, out)
-            for key in obs_keys:
-                host_obs[key].copy_(out[key], non_blocking=True)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), device=f"cuda:{local}")
-        e2e = {"value": world * args.steps * E / (e2e_ms / 1000.0), "unit": "solves/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+        e2e = _e2e_generator(args, dev, E, step_energies, stream, barrier, local, world)
 
     # ---- roofline of the dominant kernel (batched complex FP64 GEMM on DMMA)
     gemm_tflops = gemm["flops"] / (gemm["ms"] / 1000.0) / 1e12 if gemm["ms"] > 0 else 0.0
@@ -316,6 +320,8 @@ def run_ours(args):
         "gemm_share_of_step": round(gemm["ms"] / elapsed_ms, 4) if elapsed_ms > 0 else None,
         "inverse_ms": round(inv["ms"], 3), "inverse_launches": inv["launches"],
         "inverse_tflops": round(inv["flops"] / (inv["ms"] / 1000.0) / 1e12, 3) if inv["ms"] > 0 else None,
+        "inverse_frac": (round(inv["flops"] / (inv["ms"] / 1000.0) / 1e12 / FP64_DMMA_PEAK_TFLOPS, 4)
+                         if inv["ms"] > 0 else None),
     }
     alg = _flops_per_energy(nb, b, [float(np.mean(sr_its[:, 0])), float(np.mean(sr_its[:, 1]))])
     whole_tflops = alg * args.steps * E / (elapsed_ms / 1000.0) / 1e12
@@ -326,35 +332,36 @@ def run_ours(args):
         roofline["traffic"] = OZAKI_TRAFFIC_BYTES
         roofline["traffic_source"] = "ncu capture of ozaki_gemm_kernel, profiles/ozaki_gemm_b256_batch128.md"
 
-    # ---- accuracy of the mixed form against the FP64 form (itself within 1e-10
-    # of the oracle) on the first energies of the first step
-    accuracy = None
-    if args.precision == "mixed" and rank == 0:
-        n_chk = min(32, E)
-        e_chk = step_e[0][:n_chk].contiguous()
-        keys = ("gr_diag", "gl_diag", "density", "transmission")
-        mix = TransportSolver(dev, max_batch_size=n_chk, precision="mixed", cuda_device=local).solve(e_chk, keys=keys)
-        ref = TransportSolver(dev, max_batch_size=n_chk, precision="fp64", cuda_device=local).solve(e_chk, keys=keys)
+    # ---- the precision form on the same workload, same box, same run (rank 0
+    # alone, device resident): its rate and its ratio to this line's form
+    mixed = None
+    if args.precision == "fp64" and world == 1 and not args.no_mixed:
+        mixed = _mixed_line(args, dev, E, step_energies, stream, local, value)
 
-        def block_rel(a, r):
-            return float((torch.linalg.norm(a - r, dim=(-2, -1)) / torch.linalg.norm(r, dim=(-2, -1))).max())
-
-        dens = (torch.abs(mix["density"] - ref["density"]) / torch.abs(ref["density"]).amax(dim=1, keepdim=True))
-        tr = torch.abs(mix["transmission"] - ref["transmission"]) / torch.clamp(torch.abs(ref["transmission"]),
-                                                                                   min=1e-12)
-        accuracy = {"against": "fp64 form, same energies", "energies": n_chk,
-                    "gr_diag_block_rel_max": block_rel(mix["gr_diag"], ref["gr_diag"]),
-                    "gl_diag_block_rel_max": block_rel(mix["gl_diag"], ref["gl_diag"]),
-                    "density_rel_max": float(dens.max()), "transmission_rel_max": float(tr.max())}
-        del mix, ref
-
+    # ---- CPU baseline (the oracle on a bounded sample) and the accuracy of
+    # the FP64 and mixed forms against it at the same energies
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         bt = blas_threads()
-        rate, dt, idx = cpu_baseline(cfg, args.cpu_energies, bt)
+        rate, dt, idx, oracle_results = cpu_baseline(cfg, args.cpu_energies, bt)
         cpu = {"value": rate, "unit": "solves/s", "cores": bt["threads"], "kind": "port",
                "sample": f"{args.cpu_energies} energies of the same workload ({dt:.1f} s, oracle NumPy path)",
                "blas": bt["library"]}
+        e_chk = torch.from_numpy(dev.energies[idx]).to(f"cuda:{local}")
+        keys = ("gr_diag", "gl_diag", "density", "transmission")
+        acc = {}
+        for prec in ("fp64", "mixed"):
+            if prec == "mixed" and mixed is None:
+                continue
+            res = TransportSolver(dev, max_batch_size=len(idx), precision=prec, cuda_device=local).solve(
+                e_chk, keys=keys)
+            acc[prec] = accuracy_against_oracle({k: v.cpu().numpy() for k, v in res.items()}, oracle_results)
+            del res
+        cpu["accuracy_fp64"] = acc["fp64"]
+        if mixed is not None:
+            mixed["accuracy"] = acc["mixed"]
+            mixed["accuracy"]["against"] = (f"oracle (NumPy, end to end incl. its Sancho-Rubio) at energy "
+                                            f"indices {idx.tolist()}")
 
     if rank == 0:
         line = {
@@ -371,12 +378,167 @@ def run_ours(args):
             "whole_step_tflops_fp64_equiv": round(whole_tflops, 3),
             "sr_iterations_mean": [float(np.mean(sr_its[:, 0])), float(np.mean(sr_its[:, 1]))],
         }
-        if accuracy is not None:
-            line["accuracy"] = accuracy
+        if mixed is not None:
+            line["mixed"] = mixed
+        if world == 1 and not args.no_dropin_e2e:
+            line["e2e_dropin"] = _e2e_dropin(args)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+E2E_KEYS = ("gr_diag", "gl_diag", "gg_diag", "density", "hole_density", "transmission", "current_left",
+            "current_right", "dos", "sr_iterations")
+
+
+def _e2e_generator(args, dev, E, step_energies, stream, barrier, local, world):
+    import torch
+
+    from quatrex_b200.energy_shards import max_over_ranks
+    from quatrex_b200.transport import TransportSolver
+
+    cuda = f"cuda:{local}"
+    h_diag_host = torch.from_numpy(dev.h_diag).pin_memory()
+    h_upper_host = torch.from_numpy(dev.h_upper).pin_memory()
+    e_host = [step_energies(k).cpu().pin_memory() for k in range(args.steps)]
+    h_diag_dev = torch.empty(h_diag_host.shape, dtype=h_diag_host.dtype, device=cuda)
+    h_upper_dev = torch.empty(h_upper_host.shape, dtype=h_upper_host.dtype, device=cuda)
+    e_dev = torch.empty(E, dtype=torch.float64, device=cuda)
+    solver = TransportSolver(dev, max_batch_size=E, precision=args.precision, cuda_device=local,
+                             h_diag=h_diag_dev, h_upper=h_upper_dev)
+    bufs = [solver.allocate_outputs(E, keys=E2E_KEYS) for _ in range(2)]
+    # one flat page-locked host buffer holds every returned array of a step
+    sizes = {k: v.numel() * v.element_size() for k, v in bufs[0].items()}
+    total = sum((n + 255) // 256 * 256 for n in sizes.values())
+    flat = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+    host, off = {}, 0
+    for k, v in bufs[0].items():
+        host[k] = flat[off:off + sizes[k]].view(v.dtype).view(v.shape)
+        off += (sizes[k] + 255) // 256 * 256
+    copy_stream = torch.cuda.Stream(device=cuda)
+    h2d = h_diag_host.numel() * 16 + h_upper_host.numel() * 16 + E * 8
+    d2h = sum(sizes.values())
+
+    def one_step(k, timed_events):
+        kb = k % 2
+        stream.wait_event(timed_events["copied"][kb])  # buffer kb's previous download has landed
+        h_diag_dev.copy_(h_diag_host, non_blocking=True)
+        h_upper_dev.copy_(h_upper_host, non_blocking=True)
+        e_dev.copy_(e_host[k % len(e_host)], non_blocking=True)
+        solver.solve(e_dev, bufs[kb])
+        timed_events["solved"][kb].record(stream)
+        copy_stream.wait_event(timed_events["solved"][kb])
+        with torch.cuda.stream(copy_stream):
+            for key, t in bufs[kb].items():
+                host[key].copy_(t, non_blocking=True)
+        timed_events["copied"][kb].record(copy_stream)
+
+    ev = {"solved": [torch.cuda.Event() for _ in range(2)], "copied": [torch.cuda.Event() for _ in range(2)]}
+    for e in ev["copied"]:
+        e.record(copy_stream)
+    for k in range(args.warmup):
+        one_step(k, ev)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(args.steps):
+        one_step(k, ev)
+    stream.wait_stream(copy_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), device=cuda)
+    # the host copy of the last step is the solve's result: spot-check it is there
+    assert torch.isfinite(host["density"]).all()
+    del bufs, flat, host
+    torch.cuda.empty_cache()
+    return {"value": world * args.steps * E / (e2e_ms / 1000.0), "unit": "solves/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": round(e2e_ms / args.steps, 3),
+            "returned": "every diagonal block of G^R, G^<, G^> + density, hole density, DOS, transmission, "
+                        "contact currents (double-buffered on the device, downloads overlap the next solve)",
+            "path": "TransportSolver.solve -> qtx_transport_solve, H and energies from pinned host memory"}
+
+
+def _mixed_line(args, dev, E, step_energies, stream, local, fp64_value):
+    import torch
+
+    from quatrex_b200.transport import TransportSolver
+
+    solver = TransportSolver(dev, max_batch_size=E, precision="mixed", cuda_device=local)
+    keys = ("gr_diag", "gr_upper", "gr_lower", "gl_diag", "gl_upper", "gg_diag", "gg_upper", "density",
+            "hole_density", "transmission", "current_left", "current_right", "sr_iterations", "dos", "layer_current")
+    out = solver.allocate_outputs(E, keys)
+    step_e = [step_energies(k) for k in range(args.steps)]
+    for k in range(args.warmup):
+        solver.solve(step_energies(k), out)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(args.steps):
+        solver.solve(step_e[k], out)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    del out
+    torch.cuda.empty_cache()
+    v = args.steps * E / (ms / 1000.0)
+    return {"value": round(v, 3), "unit": "solves/s", "ms_per_step": round(ms / args.steps, 3),
+            "ratio_vs_fp64": round(v / fp64_value, 4), "steps": args.steps, "warmup": args.warmup,
+            "form": "bulk sweep products as INT8 split products (tcgen05 kind::i8, 8 slices), inverses and "
+                    "Sancho-Rubio in FP64; same outputs as the FP64 line"}
+
+
+def _e2e_dropin(args):
+    """The plugin call RGF.selected_solve(return_retarded) on NumPy DSDBCOO
+    matrices of the nb=64, b=256 device (32 energies, batches of 16): every
+    operand streamed host -> device and every output block back inside the
+    timed region (QTX_FLAG_HOST_BUFFERS)."""
+    import torch
+
+    from quatrex_b200.datastructures import DSDBCOO
+    from quatrex_b200.greens_function_solver import RGF, OBCBlocks
+    from quatrex_b200.obc import SanchoRubio, contact_self_energies
+    from quatrex_b200.workloads import make_device
+
+    nb, b, ne, batch = 64, 256, 32, 16
+    dev = make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=1234)
+    d, u, lo = dev.system_blocks()
+    A = DSDBCOO.from_blocks(d, u, lo)
+    Z = DSDBCOO.zeros_like(A)
+    e = dev.energies
+    sr = SanchoRubio(dev.sr_max_iter, dev.sr_tol)
+    g_left = sr(d[0], u[0], lo[0])
+    g_right = sr(d[-1], lo[-1], u[-1])
+    f_left = 1.0 / (1.0 + np.exp((e - dev.mu_left) / dev.kt))
+    f_right = 1.0 / (1.0 + np.exp((e - dev.mu_right) / dev.kt))
+    ob = OBCBlocks(nb)
+    ob.retarded[0], ob.lesser[0], ob.greater[0] = contact_self_energies(g_left, lo[0], u[0], f_left)
+    ob.retarded[-1], ob.lesser[-1], ob.greater[-1] = contact_self_energies(g_right, u[-1], lo[-1], f_right)
+    del d, u, lo
+    outs = [DSDBCOO.zeros_like(A) for _ in range(3)]
+    solver = RGF(max_batch_size=batch)
+    for _ in range(2):
+        solver.selected_solve(A, Z, Z, obc_blocks=ob, out=outs, return_retarded=True)
+    torch.cuda.synchronize()
+    steps = 2
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        solver.selected_solve(A, Z, Z, obc_blocks=ob, out=outs, return_retarded=True)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    row_bytes = A.data.shape[-1] * 16
+    return {"value": round(ne * steps / dt, 3), "unit": "solves/s", "h2d_bytes_per_step": int(3 * ne * row_bytes),
+            "d2h_bytes_per_step": int(3 * ne * row_bytes), "steps": steps, "warmup": 2,
+            "path": "RGF.selected_solve(a, sigma_lesser, sigma_greater, obc_blocks, out=[xl, xg, xr], "
+                    "return_retarded=True) on NumPy DSDBCOO -> qtx_selected_solve with QTX_FLAG_HOST_BUFFERS",
+            "config": {"num_blocks": nb, "block_size": b, "energies": ne, "max_batch_size": batch,
+                       "outputs": "G^<, G^> (every BTD block), G^R diagonal; Sigma^<, Sigma^> zero in the interior"}}
 
 
 def run_uneven(args):
@@ -580,6 +742,8 @@ def main():
     ap.add_argument("--cpu-energies", type=int, default=3)
     ap.add_argument("--ref-energies-per-step", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the precision-form sub-line")
+    ap.add_argument("--no-dropin-e2e", action="store_true", help="skip the plugin-call end-to-end key")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

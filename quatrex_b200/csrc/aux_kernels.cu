@@ -4,6 +4,8 @@
 // contact self-energy assembly and Fermi occupancies.  All are grid-stride
 // loops over (batch, element) with coalesced row-major access; the transposed
 // operands go through 32x32 shared-memory tiles.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace {
@@ -274,6 +276,30 @@ __global__ void fill_int_kernel(int* p, int64_t count, int value) {
     p[t] = value;
 }
 
+// One CTA column per block slice (blockIdx.y), CTAs stride over the data rows:
+// flags[k] = 1 once any entry of slice k is nonzero (NaN counts as nonzero).
+// Slice k is entries [slices[2k], slices[2k] + slices[2k + 1]) of every row.
+__global__ void block_nonzero_kernel(const int64_t* slices, const cplx* data, int64_t stride, int64_t rows,
+                                     int* flags) {
+  const int k = blockIdx.y;
+  const int64_t off = slices[2 * k], nnz = slices[2 * k + 1];
+  if (off < 0 || nnz <= 0) return;
+  volatile int* f = flags + k;
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    if (*f) return;
+    const double2* row = reinterpret_cast<const double2*>(data + r * stride + off);
+    bool any = false;
+    for (int64_t q = threadIdx.x; q < nnz; q += blockDim.x) {
+      const double2 v = row[q];
+      any |= (v.x != 0.0) || (v.y != 0.0) || (v.x != v.x) || (v.y != v.y);
+    }
+    if (__syncthreads_or(any)) {
+      if (threadIdx.x == 0) *f = 1;
+      return;
+    }
+  }
+}
+
 __global__ void real_part_kernel(int64_t count, const cplx* src, double* dst) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
     dst[t] = src[t].x;
@@ -414,6 +440,14 @@ void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream) {
   if (count <= 0) return;
   fill_int_kernel<<<grid_for(count), TB, 0, stream>>>(p, count, value);
   qtx_check_launch("fill_int_kernel");
+}
+
+void launch_block_nonzero(int num_slices, const int64_t* slices, const cplx* data, int64_t stride, int64_t rows,
+                          int* flags, cudaStream_t stream) {
+  if (num_slices <= 0 || rows <= 0) return;
+  const unsigned gx = (unsigned)std::min<int64_t>(rows, 256);
+  block_nonzero_kernel<<<dim3(gx, (unsigned)num_slices), TB, 0, stream>>>(slices, data, stride, rows, flags);
+  qtx_check_launch("block_nonzero_kernel");
 }
 
 void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t stream) {

@@ -101,6 +101,12 @@ void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream);
 void launch_residual_norm(int n, int64_t batch, MatView x_ref, MatView x, double* abs_res, double* rel_res,
                           cudaStream_t stream);
 void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t stream);
+// flags[k] = 1 if block slice k of a DSDBSparse data stack holds any nonzero
+// entry in any of `rows` data rows (flags zeroed by the caller).  slices
+// (device int64 [2 * num_slices]): (offset, nnz) of each slice in a row;
+// num_slices <= 65535.
+void launch_block_nonzero(int num_slices, const int64_t* slices, const cplx* data, int64_t stride, int64_t rows,
+                          int* flags, cudaStream_t stream);
 // Lesser / greater blocks from the two contact-source responses XL, XR
 // (n x n, per batch entry e):  Y< = f_L XL + s f_R XR,  Y> = (f_L - 1) XL + s (f_R - 1) XR
 // with f = occ_l[e], occ_r[e] and s = sign_r; sym: write 0.5 (Y - Y^H), else Y.

@@ -560,6 +560,34 @@ struct SolveArgs {
   int precision = QTX_PREC_FP64;
 };
 
+// Per block k of a Sigma operand: 1 if block k holds a nonzero entry anywhere
+// in the stack (one pass over the operand's data and one small read-back).
+std::vector<char> sigma_nonzero_blocks(const Btd& m, cudaStream_t s) {
+  const int nb = m.nb(), nk = 3 * nb - 2;
+  std::vector<char> out(nk, 0);
+  if (!m.data || m.d->stack_size <= 0) return out;
+  std::vector<int64_t> slices(2 * (size_t)nk, -1);
+  for (int i = 0; i < nb; ++i)
+    for (int j = std::max(0, i - 1); j <= std::min(nb - 1, i + 1); ++j) {
+      const int k = bidx(i, j);
+      slices[2 * k] = m.empty(k) ? -1 : m.off(k);
+      slices[2 * k + 1] = m.empty(k) ? 0 : m.nnz(k);
+    }
+  DevBuf buf(sizeof(int64_t) * slices.size() + sizeof(int) * nk, s);
+  int64_t* d_slices = buf.as<int64_t>();
+  int* d_flags = reinterpret_cast<int*>(d_slices + slices.size());
+  QTX_CUDA_TRY(cudaMemcpyAsync(d_slices, slices.data(), sizeof(int64_t) * slices.size(), cudaMemcpyHostToDevice, s));
+  QTX_CUDA_TRY(cudaMemsetAsync(d_flags, 0, sizeof(int) * nk, s));
+  for (int k0 = 0; k0 < nk; k0 += 65535)
+    launch_block_nonzero(std::min(nk - k0, 65535), d_slices + 2 * k0, m.data, m.d->stack_stride, m.d->stack_size,
+                         d_flags + k0, s);
+  std::vector<int> h(nk);
+  QTX_CUDA_TRY(cudaMemcpyAsync(h.data(), d_flags, sizeof(int) * nk, cudaMemcpyDeviceToHost, s));
+  QTX_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int k = 0; k < nk; ++k) out[k] = h[k] != 0;
+  return out;
+}
+
 void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
   const Btd& a = A.a;
   const int nb = a.nb();
@@ -602,6 +630,14 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
   const void* const* obc_r = A.obc ? A.obc->retarded : nullptr;
   const void* const* obc_l = A.obc ? A.obc->lesser : nullptr;
   const void* const* obc_g = A.obc ? A.obc->greater : nullptr;
+
+  // Which blocks of Sigma^< and Sigma^> hold a nonzero entry anywhere in the
+  // stack.  ElectronSolver passes interior self-energies that are zero in the
+  // ballistic case (only the OBC blocks inject); every product with a zero
+  // block is then skipped, and the forward step of both components shares
+  // W = x_j A_ji (X_j = W X_i W^H when nothing is injected at block j).
+  const std::vector<char> nz_l = sigma_nonzero_blocks(A.sl, s), nz_g = sigma_nonzero_blocks(A.sg, s);
+  auto nz = [&](int comp, int i, int j) { return (comp == 0 ? nz_l : nz_g)[bidx(i, j)] != 0; };
 
   for (size_t q = 0; q + 1 < offs.size(); ++q) {
     const int64_t e0 = offs[q], ne = offs[q + 1] - offs[q];
@@ -649,15 +685,35 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
              obc_view(obc_r, j, bj, e0), MONE, nullptr, nullptr, prec);
         zinv(bj, ne, tv(1, bj), xr.view(j), info + (int64_t)j * ne_max, nullptr, s);
       }
+      // W = x_j A_ji, shared by both components when neither injects at
+      // (i, j) or (j, j): X_j = W X_i W^H (3 products for two components
+      // instead of 8)
+      bool shared_w = !want_cur;
+      for (int comp = 0; comp < 2; ++comp)
+        shared_w = shared_w && !nz(comp, i, j) && !nz(comp, j, j) && !obc_view(comp == 0 ? obc_l : obc_g, j, bj, e0).ptr;
+      if (shared_w) {
+        gemm(bj, bi, bj, ne, ONE, xr.view(j), OP_N, a_ji, OP_N, tv(2, bi), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+             prec);
+        for (int comp = 0; comp < 2; ++comp) {
+          BlockStack& X = comp == 0 ? xl : xg;
+          gemm(bj, bi, bi, ne, ONE, tv(2, bi), OP_N, X.view(i), OP_N, tv(5, bi), s, {}, ZERO, {}, ZERO, nullptr,
+               nullptr, prec);
+          gemm(bj, bj, bi, ne, ONE, tv(5, bi), OP_N, tv(2, bi), OP_C, X.view(j), s, {}, ZERO, {}, ZERO, nullptr,
+               nullptr, prec);
+        }
+        continue;
+      }
       for (int comp = 0; comp < 2; ++comp) {
         const Btd& S = comp == 0 ? A.sl : A.sg;
         const void* const* ob = comp == 0 ? obc_l : obc_g;
         BlockStack& X = comp == 0 ? xl : xg;
-        MatView s_ij = in_block(S, i, j, e0, ne, T[10], ws);
-        MatView s_jj = in_block(S, j, j, e0, ne, T[11], ws);
-        // W = U S_ij
-        gemm(bj, bj, bi, ne, ONE, tv(0, bi), OP_N, s_ij, OP_N, tv(2, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
-             prec);
+        const bool inj_ij = nz(comp, i, j);
+        MatView s_ij = inj_ij ? in_block(S, i, j, e0, ne, T[10], ws) : MatView{};
+        MatView s_jj = nz(comp, j, j) ? in_block(S, j, j, e0, ne, T[11], ws) : MatView{};
+        // W = U S_ij (zero when S_ij is)
+        if (inj_ij)
+          gemm(bj, bj, bi, ne, ONE, tv(0, bi), OP_N, s_ij, OP_N, tv(2, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+               prec);
         // V = X_i A_ji^H
         gemm(bi, bj, bi, ne, ONE, X.view(i), OP_N, a_ji, OP_C, tv(3, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
              prec);
@@ -666,15 +722,15 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
           // Sigma~ = A_ji V + W^H - W  (kept for the layer current)
           gemm(bj, bj, bi, ne, ONE, a_ji, OP_N, tv(3, bj), OP_N, ST.view(i), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
                prec);
-          launch_skew_combine(bj, ne, ST.view(i), tv(2, bj), ST.view(i), s);
-          launch_axpby(bj, bj, ne, ONE, ST.view(i), ONE, s_jj, tv(4, bj), s);
+          if (inj_ij) launch_skew_combine(bj, ne, ST.view(i), tv(2, bj), ST.view(i), s);
+          launch_axpby(bj, bj, ne, ONE, ST.view(i), ONE, s_jj.ptr ? s_jj : MatView{ws.zero, bj, 0}, tv(4, bj), s);
           MatView o2 = obc_view(ob, j, bj, e0);
           if (o2.ptr) launch_axpby(bj, bj, ne, ONE, tv(4, bj), ONE, o2, tv(4, bj), s);
         } else {
           // Q = A_ji V + S_jj + Sigma^<_obc,j ; Q += W^H - W
           gemm(bj, bj, bi, ne, ONE, a_ji, OP_N, tv(3, bj), OP_N, tv(4, bj), s, s_jj, ONE, obc_view(ob, j, bj, e0),
                ONE, nullptr, nullptr, prec);
-          launch_skew_combine(bj, ne, tv(4, bj), tv(2, bj), tv(4, bj), s);
+          if (inj_ij) launch_skew_combine(bj, ne, tv(4, bj), tv(2, bj), tv(4, bj), s);
         }
         // X_j = x_j Q x_j^H
         gemm(bj, bj, bj, ne, ONE, xr.view(j), OP_N, tv(4, bj), OP_N, tv(5, bj), s, {}, ZERO, {}, ZERO, nullptr,
@@ -716,24 +772,32 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
         const Btd& S = comp == 0 ? A.sl : A.sg;
         const Btd& OUT = comp == 0 ? A.xl : A.xg;
         BlockStack& X = comp == 0 ? xl : xg;
-        MatView s_ij = in_block(S, i, j, e0, ne, T[10], ws);
-        // Y = x_i S_ij
-        gemm(bi, bj, bi, ne, ONE, xr.view(i), OP_N, s_ij, OP_N, tv(4, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
-             prec);
+        const bool inj_ij = nz(comp, i, j);
+        MatView s_ij = inj_ij ? in_block(S, i, j, e0, ne, T[10], ws) : MatView{};
+        // Y = x_i S_ij (zero when S_ij is)
+        if (inj_ij)
+          gemm(bi, bj, bi, ne, ONE, xr.view(i), OP_N, s_ij, OP_N, tv(4, bj), s, {}, ZERO, {}, ZERO, nullptr, nullptr,
+               prec);
         // t1 = P4 X_i - Y P3^H ; t1 -= t1^H
         gemm(bi, bi, bi, ne, ONE, tv(3, bi), OP_N, X.view(i), OP_N, tv(5, bi), s, {}, ZERO, {}, ZERO, nullptr,
              nullptr, prec);
-        gemm(bi, bi, bj, ne, MONE, tv(4, bj), OP_N, tv(2, bj), OP_C, tv(5, bi), s, tv(5, bi), ONE, {}, ZERO, nullptr,
-             nullptr, prec);
+        if (inj_ij)
+          gemm(bi, bi, bj, ne, MONE, tv(4, bj), OP_N, tv(2, bj), OP_C, tv(5, bi), s, tv(5, bi), ONE, {}, ZERO,
+               nullptr, nullptr, prec);
         launch_sub_herm_inplace(bi, ne, tv(5, bi), s);
         // t2 = P1 X_j
         gemm(bi, bj, bj, ne, ONE, tv(0, bj), OP_N, X.view(j), OP_N, tv(6, bj), s, {}, ZERO, {}, ZERO, nullptr,
              nullptr, prec);
         // X_ij = Y X_jj^H - t2 - X_i P2^H
-        gemm(bi, bj, bj, ne, ONE, tv(4, bj), OP_N, xr.view(j), OP_C, tv(7, bj), s, tv(6, bj), MONE, {}, ZERO,
-             nullptr, nullptr, prec);
-        gemm(bi, bj, bi, ne, MONE, X.view(i), OP_N, tv(1, bi), OP_C, tv(7, bj), s, tv(7, bj), ONE, {}, ZERO, nullptr,
-             nullptr, prec);
+        if (inj_ij) {
+          gemm(bi, bj, bj, ne, ONE, tv(4, bj), OP_N, xr.view(j), OP_C, tv(7, bj), s, tv(6, bj), MONE, {}, ZERO,
+               nullptr, nullptr, prec);
+          gemm(bi, bj, bi, ne, MONE, X.view(i), OP_N, tv(1, bi), OP_C, tv(7, bj), s, tv(7, bj), ONE, {}, ZERO,
+               nullptr, nullptr, prec);
+        } else {
+          gemm(bi, bj, bi, ne, MONE, X.view(i), OP_N, tv(1, bi), OP_C, tv(7, bj), s, tv(6, bj), MONE, {}, ZERO,
+               nullptr, nullptr, prec);
+        }
         out_block(OUT, i, j, e0, ne, tv(7, bj), 0, ws);
         if (!symmetric) out_block(OUT, j, i, e0, ne, tv(7, bj), 2, ws);
         // X_i += t2 P1^H + t1
