@@ -15,9 +15,24 @@ host (``numpy``); the solvers move host data to the device and back.  Only the
 single-rank stack/block distribution is modelled (one GPU holds the whole
 stack slice it is given).
 
-``btd_layout`` also accepts any object with ``rows``, ``cols``,
-``block_sizes`` and ``data`` attributes of that layout (an upstream qttools
-DSDBCOO included).
+``DSDBCSR`` keeps qttools' DSDBCSR layout
+(``src/qttools/datastructures/dsdbcsr.py:23-869``): the same block-sorted data
+order (``compute_rowptr_map``,
+``src/qttools/kernels/datastructure/numba/dsdbcsr.py:229-305``, block rows in
+order, blocks of a block row in order, canonical COO order inside a block),
+described by a row-pointer map ``{(i, j): rowptr}`` of absolute positions and
+the column indices instead of row and column indices.
+
+``layout_of`` accepts any object with ``rows``, ``cols``, ``block_sizes`` and
+``data`` attributes (an upstream DSDBCOO) or with ``rowptr_map``, ``cols``,
+``block_sizes`` and ``data`` (an upstream DSDBCSR).
+
+Symmetric storage (``symmetry=True``, ``dsdbcoo.py:483-492``,
+``dsdbcsr.py:262-339``) keeps the upper block triangle and the upper triangle
+of each diagonal block; block (j, i) is ``symmetry_op(X_ij^T)`` and a diagonal
+block is completed as ``U + symmetry_op(U^T)`` with its diagonal halved.  The
+solvers expand symmetric-storage INPUTS on the device to full storage
+(``expand_symmetric``) and write symmetric-storage OUTPUTS upper blocks only.
 """
 
 from __future__ import annotations
@@ -114,6 +129,62 @@ def btd_layout_from_coords(rows: np.ndarray, cols: np.ndarray, block_sizes) -> B
             if not (cn == bi * bj and np.array_equal(lin, np.arange(cn))):
                 local_index[kk] = lin.astype(np.int32)
     return BtdLayout(bsz.astype(np.int32), block_offset, block_nnz, local_index, int(rows.size))
+
+
+def rows_from_rowptr(rowptr_map: dict, nnz: int, block_sizes) -> np.ndarray:
+    """Global row index of every stored entry of a DSDBCSR pattern."""
+    offs = np.concatenate(([0], np.cumsum(np.asarray(block_sizes, dtype=np.int64))))
+    rows = np.full(int(nnz), -1, dtype=np.int64)
+    for (i, _j), rp in rowptr_map.items():
+        rp = np.asarray(rp, dtype=np.int64)
+        counts = np.diff(rp)
+        rows[rp[0]:rp[-1]] = np.repeat(offs[int(i)] + np.arange(len(counts), dtype=np.int64), counts)
+    if (rows < 0).any():
+        raise ValueError("rowptr map does not cover every stored entry")
+    return rows
+
+
+def rowptr_map_from_coords(rows: np.ndarray, cols: np.ndarray, block_sizes) -> dict:
+    """Row-pointer map of block-sorted coordinates (``compute_rowptr_map``,
+    ``src/qttools/kernels/datastructure/numba/dsdbcsr.py:229-305``)."""
+    bsz = np.asarray(block_sizes, dtype=np.int64)
+    offs = np.concatenate(([0], np.cumsum(bsz)))
+    br = np.searchsorted(offs, rows, side="right") - 1
+    bc = np.searchsorted(offs, cols, side="right") - 1
+    out = {}
+    if rows.size == 0:
+        return out
+    key = br * len(bsz) + bc
+    uk, start, count = np.unique(key, return_index=True, return_counts=True)
+    for kk, st, cn in zip(uk, start, count):
+        i, j = int(kk) // len(bsz), int(kk) % len(bsz)
+        local = rows[st:st + cn] - offs[i]
+        hist = np.bincount(local, minlength=int(bsz[i]))
+        out[(i, j)] = np.concatenate(([0], np.cumsum(hist))).astype(np.int64) + st
+    return out
+
+
+def symmetry_kind(op) -> str:
+    """Classify a qttools ``symmetry_op``: 'conj' (Hermitian storage, the
+    default), 'neg_conj' (skew-Hermitian: G^<, G^>, Sigma^<, Sigma^>) or
+    'identity' (complex symmetric: Sigma^R, the system matrix)."""
+    if op is None:
+        return "conj"
+    probe = np.array([1.0 + 2.0j])
+    r = np.asarray(op(probe))
+    for kind, want in (("conj", 1.0 - 2.0j), ("neg_conj", -1.0 + 2.0j), ("identity", 1.0 + 2.0j)):
+        if r.shape == (1,) and r[0] == want:
+            return kind
+    raise NotImplementedError("symmetry_op must be conj, -conj or the identity")
+
+
+def _apply_sym(kind: str, x):
+    """symmetry_op of `kind` applied to the transpose of x (numpy or torch)."""
+    xt = x.swapaxes(-1, -2) if isinstance(x, np.ndarray) else x.transpose(-1, -2)
+    if kind == "identity":
+        return xt
+    xc = xt.conj() if isinstance(x, np.ndarray) else xt.conj().resolve_conj()
+    return xc if kind == "conj" else -xc
 
 
 def block_sort_index(rows: np.ndarray, cols: np.ndarray, block_sizes) -> np.ndarray:
@@ -213,7 +284,8 @@ class _BlockIndexer:
 class DSDBCOO:
     """Stack of block-tridiagonal sparse matrices in the DSDBCOO layout."""
 
-    def __init__(self, data, rows, cols, block_sizes, global_stack_shape, symmetry: bool = False):
+    def __init__(self, data, rows, cols, block_sizes, global_stack_shape, symmetry: bool = False,
+                 symmetry_op=np.conj):
         if isinstance(global_stack_shape, int):
             global_stack_shape = (global_stack_shape,)
         self.data = data
@@ -221,6 +293,8 @@ class DSDBCOO:
         self.cols = np.asarray(cols, dtype=np.int64)
         self.global_stack_shape = tuple(global_stack_shape)
         self.symmetry = bool(symmetry)
+        self.symmetry_op = symmetry_op
+        self._sym_kind = symmetry_kind(symmetry_op) if self.symmetry else "conj"
         self.layout = btd_layout_from_coords(self.rows, self.cols, block_sizes)
         self.block_sizes = np.asarray(block_sizes, dtype=np.int64)
         self.block_offsets = np.concatenate(([0], np.cumsum(self.block_sizes)))
@@ -255,7 +329,8 @@ class DSDBCOO:
 
     # -- construction ----------------------------------------------------
     @classmethod
-    def from_sparray(cls, sparray, block_sizes, global_stack_shape, symmetry: bool = False, device=None):
+    def from_sparray(cls, sparray, block_sizes, global_stack_shape, symmetry: bool = False, device=None,
+                     symmetry_op=np.conj):
         """Same contract as ``DSDBCOO.from_sparray`` (``dsdbcoo.py:873-964``), single rank:
         the sparse matrix is broadcast over the stack."""
         from scipy import sparse
@@ -272,13 +347,18 @@ class DSDBCOO:
             order_h = order.cpu().numpy()
             vals = torch.as_tensor(coo.data.astype(np.complex128)).to(order.device)[order]
             data = vals.expand(tuple(global_stack_shape) + (vals.shape[0],)).contiguous()
-            return cls(data, coo.row[order_h], coo.col[order_h], block_sizes, global_stack_shape, symmetry)
+            return cls._from_sorted(data, coo.row[order_h], coo.col[order_h], block_sizes, global_stack_shape,
+                                    symmetry, symmetry_op)
         order = block_sort_index(coo.row, coo.col, block_sizes)
         rows, cols, vals = coo.row[order], coo.col[order], coo.data[order].astype(np.complex128)
         data = np.broadcast_to(vals, tuple(global_stack_shape) + (len(vals),)).copy()
         if device is not None:
             data = torch.as_tensor(data).to(device)
-        return cls(data, rows, cols, block_sizes, global_stack_shape, symmetry)
+        return cls._from_sorted(data, rows, cols, block_sizes, global_stack_shape, symmetry, symmetry_op)
+
+    @classmethod
+    def _from_sorted(cls, data, rows, cols, block_sizes, global_stack_shape, symmetry, symmetry_op):
+        return cls(data, rows, cols, block_sizes, global_stack_shape, symmetry, symmetry_op)
 
     @classmethod
     def zeros_like(cls, other) -> "DSDBCOO":
@@ -287,7 +367,7 @@ class DSDBCOO:
         else:
             data = np.zeros_like(other.data)
         return cls(data, other.rows, other.cols, other.block_sizes, getattr(other, "global_stack_shape", other.data.shape[:-1]),
-                   getattr(other, "symmetry", False))
+                   getattr(other, "symmetry", False), getattr(other, "symmetry_op", np.conj))
 
     @classmethod
     def from_blocks(cls, diag, upper, lower, device=None) -> "DSDBCOO":
@@ -314,11 +394,12 @@ class DSDBCOO:
             data = np.concatenate(chunks, axis=-1)
             if device is not None:
                 data = torch.as_tensor(data).to(device)
-        return cls(data, np.concatenate(rows_l), np.concatenate(cols_l), sizes, stack)
+        return cls._from_sorted(data, np.concatenate(rows_l), np.concatenate(cols_l), sizes, stack, False, np.conj)
 
     def to(self, device) -> "DSDBCOO":
         data = self.data if isinstance(self.data, torch.Tensor) else torch.as_tensor(self.data)
-        return DSDBCOO(data.to(device), self.rows, self.cols, self.block_sizes, self.global_stack_shape, self.symmetry)
+        return DSDBCOO(data.to(device), self.rows, self.cols, self.block_sizes, self.global_stack_shape, self.symmetry,
+                       self.symmetry_op)
 
     def numpy_data(self) -> np.ndarray:
         if isinstance(self.data, torch.Tensor):
@@ -337,7 +418,7 @@ class DSDBCOO:
         i, j = i % nb, j % nb
         bi, bj = int(self.block_sizes[i]), int(self.block_sizes[j])
         if self.symmetry and j < i:
-            return np.ascontiguousarray(np.conj(self.get_block(j, i).swapaxes(-1, -2)))
+            return np.ascontiguousarray(_apply_sym(self._sym_kind, self.get_block(j, i)))
         out = np.zeros(self.stack_shape + (bi, bj), dtype=np.complex128)
         if abs(i - j) > 1:
             return out
@@ -350,7 +431,7 @@ class DSDBCOO:
         flat = out.reshape(self.stack_shape + (bi * bj,))
         flat[..., lin] = vals
         if self.symmetry and i == j:
-            out = out + np.conj(out.swapaxes(-1, -2))
+            out = out + _apply_sym(self._sym_kind, out)
             out[..., np.arange(bi), np.arange(bi)] /= 2
         return out
 
@@ -358,7 +439,7 @@ class DSDBCOO:
         nb = self.num_blocks
         i, j = i % nb, j % nb
         if self.symmetry and j < i:
-            self.set_block(j, i, np.conj(np.asarray(value).swapaxes(-1, -2)))
+            self.set_block(j, i, _apply_sym(self._sym_kind, np.asarray(value)))
             return
         k, st, n = self._slice(i, j)
         if st < 0 or n == 0:
@@ -378,9 +459,82 @@ class DSDBCOO:
         out = np.zeros(self.stack_shape + (n, n), dtype=np.complex128)
         out[..., self.rows, self.cols] = self.numpy_data()
         if self.symmetry:
-            out = out + np.conj(out.swapaxes(-1, -2))
+            out = out + _apply_sym(self._sym_kind, out)
             out[..., np.arange(n), np.arange(n)] /= 2
         return out
+
+
+class DSDBCSR(DSDBCOO):
+    """Stack of block-tridiagonal sparse matrices in the DSDBCSR layout
+    (``src/qttools/datastructures/dsdbcsr.py:23-869``): the block-sorted data
+    order of DSDBCOO, described by ``rowptr_map`` and ``cols``."""
+
+    def __init__(self, data, cols, rowptr_map, block_sizes, global_stack_shape, symmetry: bool = False,
+                 symmetry_op=np.conj):
+        nnz = int(data.shape[-1])
+        self.rowptr_map = {tuple(int(v) for v in k): np.asarray(rp, dtype=np.int64) for k, rp in rowptr_map.items()}
+        rows = rows_from_rowptr(self.rowptr_map, nnz, block_sizes)
+        super().__init__(data, rows, cols, block_sizes, global_stack_shape, symmetry, symmetry_op)
+
+    @classmethod
+    def _from_sorted(cls, data, rows, cols, block_sizes, global_stack_shape, symmetry, symmetry_op):
+        rp = rowptr_map_from_coords(np.asarray(rows, dtype=np.int64), np.asarray(cols, dtype=np.int64), block_sizes)
+        return cls(data, cols, rp, block_sizes, global_stack_shape, symmetry, symmetry_op)
+
+    @classmethod
+    def zeros_like(cls, other) -> "DSDBCSR":
+        data = torch.zeros_like(other.data) if isinstance(other.data, torch.Tensor) else np.zeros_like(other.data)
+        return cls(data, other.cols, other.rowptr_map, other.block_sizes,
+                   getattr(other, "global_stack_shape", other.data.shape[:-1]), getattr(other, "symmetry", False),
+                   getattr(other, "symmetry_op", np.conj))
+
+    def to(self, device) -> "DSDBCSR":
+        data = self.data if isinstance(self.data, torch.Tensor) else torch.as_tensor(self.data)
+        return DSDBCSR(data.to(device), self.cols, self.rowptr_map, self.block_sizes, self.global_stack_shape,
+                       self.symmetry, self.symmetry_op)
+
+
+def _dense_block_device(m, lay: "BtdLayout", data: torch.Tensor, i: int, j: int) -> torch.Tensor:
+    """Block (i, j) of stored data as a dense (stack, bi, bj) tensor (zeros
+    where the pattern has no entry)."""
+    bi, bj = int(lay.block_sizes[i]), int(lay.block_sizes[j])
+    k = 2 * i + j
+    st, n = int(lay.block_offset[k]), int(lay.block_nnz[k])
+    out = torch.zeros(data.shape[:-1] + (bi * bj,), dtype=data.dtype, device=data.device)
+    if st >= 0 and n > 0:
+        ix = lay.local_index[k]
+        if ix is None:
+            out[..., :n] = data[..., st:st + n]
+        else:
+            out[..., torch.as_tensor(ix, dtype=torch.int64, device=data.device)] = data[..., st:st + n]
+    return out.reshape(data.shape[:-1] + (bi, bj))
+
+
+def expand_symmetric(m, device: int) -> DSDBCOO:
+    """Full-storage device copy of a symmetric-storage DSDBSparse (ours or
+    upstream's): every block of the block-tridiagonal pattern dense, block
+    (j, i) = symmetry_op(X_ij^T), diagonal blocks U + symmetry_op(U^T) with
+    the diagonal halved (``dsdbcoo.py:321-400`` block access)."""
+    lay = layout_of(m)
+    kind = symmetry_kind(getattr(m, "symmetry_op", None))
+    data = m.data if isinstance(m.data, torch.Tensor) else torch.as_tensor(np.asarray(m.data))
+    data = data.to(device=f"cuda:{device}", dtype=torch.complex128)
+    stack = tuple(data.shape[:-1])
+    data = data.reshape(-1, data.shape[-1])
+    nb = lay.num_blocks
+    diag, upper, lower = [], [], []
+    for i in range(nb):
+        u = _dense_block_device(m, lay, data, i, i)
+        d = u + _apply_sym(kind, u)
+        idx = torch.arange(u.shape[-1], device=u.device)
+        d[..., idx, idx] = d[..., idx, idx] / 2
+        diag.append(d.reshape(stack + d.shape[-2:]))
+        if i + 1 < nb:
+            up = _dense_block_device(m, lay, data, i, i + 1)
+            upper.append(up.reshape(stack + up.shape[-2:]))
+            lo = _apply_sym(kind, up).contiguous()
+            lower.append(lo.reshape(stack + lo.shape[-2:]))
+    return DSDBCOO.from_blocks(diag, upper, lower)
 
 
 def layout_of(m) -> BtdLayout:
@@ -391,7 +545,11 @@ def layout_of(m) -> BtdLayout:
     cached = getattr(m, "_qtx_layout", None)
     if cached is not None:
         return cached
-    lay = btd_layout_from_coords(np.asarray(m.rows), np.asarray(m.cols), np.asarray(m.block_sizes))
+    if getattr(m, "rows", None) is None and getattr(m, "rowptr_map", None) is not None:
+        rows = rows_from_rowptr(m.rowptr_map, int(m.data.shape[-1]), np.asarray(m.block_sizes))
+    else:
+        rows = np.asarray(m.rows)
+    lay = btd_layout_from_coords(rows, np.asarray(m.cols), np.asarray(m.block_sizes))
     try:
         m._qtx_layout = lay
     except AttributeError:

@@ -39,7 +39,7 @@ import numpy as np
 import torch
 
 from quatrex_b200 import _lib
-from quatrex_b200.datastructures import DSDBCOO, layout_of
+from quatrex_b200.datastructures import DSDBCOO, expand_symmetric, layout_of
 
 _PRECISIONS = {"fp64": _lib.QTX_PREC_FP64, "mixed": _lib.QTX_PREC_MIXED}
 
@@ -86,6 +86,11 @@ class _Operand:
     host pointer for the streamed host-buffer mode)."""
 
     def __init__(self, m, device: int, writable: bool, host: bool = False):
+        if not writable and getattr(m, "symmetry", False):
+            # symmetric-storage input: full storage on the device (the lower
+            # blocks and lower diagonal triangles are not stored)
+            m = expand_symmetric(m, device)
+            host = False
         self.m = m
         self.layout = layout_of(m)
         data = m.data
@@ -205,7 +210,8 @@ class RGF(GFSolver):
         if obc_blocks is None:
             obc_blocks = OBCBlocks(num_blocks=a.num_blocks)
         x = out if out is not None else _zeros_like(a)
-        host = all(_is_host(m.data) for m in (a, x)) and all(_is_host(b) for b in obc_blocks.retarded)
+        host = (all(_is_host(m.data) for m in (a, x)) and not getattr(a, "symmetry", False)
+                and all(_is_host(b) for b in obc_blocks.retarded))
         A = _Operand(a, dev, writable=False, host=host)
         X = _Operand(x, dev, writable=True, host=host)
         keep: list = []
@@ -241,7 +247,8 @@ class RGF(GFSolver):
             xg = _zeros_like(a)
             xr = _zeros_like(a) if return_retarded else None
         mats = [a, sigma_lesser, sigma_greater, xl, xg] + ([xr] if xr is not None else [])
-        host = all(_is_host(m.data) for m in mats) and all(
+        host = all(_is_host(m.data) for m in mats) and not any(
+            getattr(m, "symmetry", False) for m in (a, sigma_lesser, sigma_greater)) and all(
             _is_host(b) for blocks in (obc_blocks.retarded, obc_blocks.lesser, obc_blocks.greater) for b in blocks)
         A = _Operand(a, dev, writable=False, host=host)
         SL = _Operand(sigma_lesser, dev, writable=False, host=host)

@@ -25,7 +25,11 @@ never runs on the GPU machine and nothing imports it.  It imports the upstream
   upstream G^R and the energies that upstream ``ElectronSolver._filter_peaks``
   zeroes for a peak limit set to the median of the largest DOS slopes.
 
-Usage:  QTX_UPSTREAM=<upstream checkout> python tests/golden/make_golden.py
+* ``dsdb_layouts.npz`` -- upstream DSDBCOO and DSDBCSR layouts (full and
+  symmetric storage) of one seeded sparse BTD pattern with mixed block sizes,
+  and upstream ``RGF.selected_solve`` on symmetric-storage operands.
+
+Usage:  QTX_UPSTREAM=<upstream checkout> python tests/golden/make_golden.py [generator ...]
 """
 
 from __future__ import annotations
@@ -59,7 +63,7 @@ _cfg = {k: "device_mpi" for k in ("all_to_all", "all_gather", "all_reduce", "bca
 comm.configure(block_comm_size=1, block_comm_config=_cfg, stack_comm_config=_cfg, override=True)
 
 from qttools.boundary_conditions.obc import SanchoRubio  # noqa: E402
-from qttools.datastructures import DSDBCOO  # noqa: E402
+from qttools.datastructures import DSDBCOO, DSDBCSR  # noqa: E402
 from qttools.greens_function_solver import RGF  # noqa: E402
 from qttools.greens_function_solver.solver import OBCBlocks  # noqa: E402
 
@@ -252,10 +256,67 @@ def observables_small():
     print("observables_small written", int(mask.sum()), "of", len(mask), "energies masked")
 
 
+def _rowptr_arrays(m):
+    keys = sorted(m.rowptr_map.keys())
+    ptrs = [np.asarray(m.rowptr_map[k], dtype=np.int64) for k in keys]
+    return (np.array(keys, dtype=np.int64).reshape(-1, 2), np.concatenate(ptrs),
+            np.array([len(p) for p in ptrs], dtype=np.int64))
+
+
+def dsdb_layouts():
+    """Upstream DSDBCOO / DSDBCSR layouts (full and symmetric storage) of one
+    seeded sparse BTD pattern with mixed block sizes, and upstream
+    RGF.selected_solve on symmetric-storage operands: a complex-symmetric
+    system matrix (symmetry_op = identity), skew-Hermitian self-energies and
+    outputs (symmetry_op = -conj), G^R diagonal stored complex-symmetric, as
+    quatrex's SCBA stores them (src/quatrex/core/scba.py:164-183)."""
+    rng = np.random.default_rng(21)
+    block_sizes = np.array([3, 3, 5, 4, 4, 3])
+    dense = bt_dense(rng, block_sizes)
+    out = {"block_sizes": block_sizes, "a": dense}
+    for sym in (False, True):
+        tag = "sym" if sym else "full"
+        coo = DSDBCOO.from_sparray(sparse.coo_matrix(dense), block_sizes, (1,), symmetry=sym)
+        out[f"coo_{tag}_rows"] = np.asarray(coo.rows)
+        out[f"coo_{tag}_cols"] = np.asarray(coo.cols)
+        out[f"coo_{tag}_data"] = np.asarray(coo.data[0])
+        csr = DSDBCSR.from_sparray(sparse.coo_matrix(dense), block_sizes, (1,), symmetry=sym)
+        keys, ptrs, lens = _rowptr_arrays(csr)
+        out[f"csr_{tag}_cols"] = np.asarray(csr.cols)
+        out[f"csr_{tag}_data"] = np.asarray(csr.data[0])
+        out[f"csr_{tag}_keys"], out[f"csr_{tag}_ptrs"], out[f"csr_{tag}_lens"] = keys, ptrs, lens
+    # symmetric-storage selected solve
+    a_sym = 0.5 * (dense + dense.T)
+    s = random_block(rng, dense.shape[0], dense.shape[0]) * (np.abs(dense) > 0)
+    sl = s - s.conj().T
+    s = random_block(rng, dense.shape[0], dense.shape[0]) * (np.abs(dense) > 0)
+    sg = s - s.conj().T
+    stack = 3
+    ident = lambda x: x  # noqa: E731
+    neg_conj = lambda x: -x.conj()  # noqa: E731
+    A = DSDBCOO.from_sparray(sparse.coo_matrix(a_sym), block_sizes, (stack,), symmetry=True, symmetry_op=ident)
+    SL = DSDBCOO.from_sparray(sparse.coo_matrix(sl), block_sizes, (stack,), symmetry=True, symmetry_op=neg_conj)
+    SG = DSDBCOO.from_sparray(sparse.coo_matrix(sg), block_sizes, (stack,), symmetry=True, symmetry_op=neg_conj)
+    xl = DSDBCOO.zeros_like(SL)
+    xg = DSDBCOO.zeros_like(SL)
+    xr = DSDBCOO.zeros_like(A)
+    RGF(max_batch_size=2).selected_solve(A, SL, SG, out=[xl, xg, xr], return_retarded=True)
+    out.update(sym_a=a_sym, sym_sigma_lesser=sl, sym_sigma_greater=sg, sym_xl=xl.to_dense()[0],
+               sym_xg=xg.to_dense()[0], sym_xr=xr.to_dense()[0], sym_xl_data=np.asarray(xl.data[0]),
+               sym_xr_data=np.asarray(xr.data[0]))
+    np.savez_compressed(os.path.join(HERE, "dsdb_layouts.npz"), **out)
+    print("dsdb_layouts written: nnz", len(out["coo_full_rows"]), "(symmetric", len(out["coo_sym_rows"]), ")")
+
+
 if __name__ == "__main__":
     warnings.simplefilter("ignore", FutureWarning)
+    if len(sys.argv) > 1:
+        for name in sys.argv[1:]:
+            globals()[name]()
+        sys.exit(0)
     btd_case("constant", [2] * 10, 10, seed=11)
     btd_case("mixed", [2, 2, 2, 4, 4, 2, 2, 2], 10, seed=12)
     transport_small()
     transport_cfg_small_subset()
     observables_small()
+    dsdb_layouts()

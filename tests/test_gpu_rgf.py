@@ -17,7 +17,7 @@ import torch
 from scipy import sparse
 
 from oracle import rgf_oracle as orc
-from quatrex_b200.datastructures import DSDBCOO
+from quatrex_b200.datastructures import DSDBCOO, DSDBCSR
 from quatrex_b200.greens_function_solver import RGF, OBCBlocks
 from quatrex_b200.workloads import make_device
 
@@ -52,6 +52,9 @@ def _bt_dense(rng, block_sizes):
 
 BLOCK_SIZES = [np.array([2] * 10), np.array([2] * 3 + [4] * 2 + [2] * 3)]
 STACKS = [(10,), (7, 2), (9, 2, 4)]
+# both storage layouts, as the upstream solver tests parametrise them
+# (tests/qttools/greens_function_solver/conftest.py:12)
+DSDB_TYPES = [DSDBCOO, DSDBCSR]
 
 
 @pytest.mark.parametrize("block_sizes", BLOCK_SIZES, ids=["constant", "mixed"])
@@ -59,15 +62,17 @@ STACKS = [(10,), (7, 2), (9, 2, 4)]
 @pytest.mark.parametrize("use_out", [True, False])
 @pytest.mark.parametrize("stack", STACKS, ids=["1D", "2D", "3D"])
 @pytest.mark.parametrize("on_device", [True, False])
-def test_selected_inv_upstream_criterion(block_sizes, max_batch_size, use_out, stack, on_device):
+@pytest.mark.parametrize("dsdb_type", DSDB_TYPES, ids=["DSDBCOO", "DSDBCSR"])
+def test_selected_inv_upstream_criterion(block_sizes, max_batch_size, use_out, stack, on_device, dsdb_type):
     rng = np.random.default_rng(len(block_sizes) * 7 + max_batch_size)
     bt = _bt_dense(rng, block_sizes)
     mask = bt.astype(bool)
     ref = np.linalg.inv(bt) * mask
-    a = DSDBCOO.from_sparray(sparse.coo_matrix(bt), block_sizes, stack, device="cuda" if on_device else None)
+    a = dsdb_type.from_sparray(sparse.coo_matrix(bt), block_sizes, stack, device="cuda" if on_device else None)
+    assert type(a) is dsdb_type
     solver = RGF(max_batch_size=max_batch_size)
     if use_out:
-        x = DSDBCOO.zeros_like(a)
+        x = dsdb_type.zeros_like(a)
         assert solver.selected_inv(a, out=x) is None
     else:
         x = solver.selected_inv(a)
@@ -81,7 +86,8 @@ def test_selected_inv_upstream_criterion(block_sizes, max_batch_size, use_out, s
 @pytest.mark.parametrize("use_out", [True, False])
 @pytest.mark.parametrize("return_retarded", [True, False])
 @pytest.mark.parametrize("stack", STACKS, ids=["1D", "2D", "3D"])
-def test_selected_solve_upstream_criterion(block_sizes, max_batch_size, use_out, return_retarded, stack):
+@pytest.mark.parametrize("dsdb_type", DSDB_TYPES, ids=["DSDBCOO", "DSDBCSR"])
+def test_selected_solve_upstream_criterion(block_sizes, max_batch_size, use_out, return_retarded, stack, dsdb_type):
     rng = np.random.default_rng(len(block_sizes) * 11 + max_batch_size)
     bt = _bt_dense(rng, block_sizes)
     bl = bt - bt.conj().T
@@ -89,12 +95,12 @@ def test_selected_solve_upstream_criterion(block_sizes, max_batch_size, use_out,
     ref_r = np.linalg.inv(bt)
     ref_l = ref_r @ bl @ ref_r.conj().T
     ref_g = ref_r @ bg @ ref_r.conj().T
-    A = DSDBCOO.from_sparray(sparse.coo_matrix(bt), block_sizes, stack, device="cuda")
-    BL = DSDBCOO.from_sparray(sparse.coo_matrix(bl), block_sizes, stack, device="cuda")
-    BG = DSDBCOO.from_sparray(sparse.coo_matrix(bg), block_sizes, stack, device="cuda")
+    A = dsdb_type.from_sparray(sparse.coo_matrix(bt), block_sizes, stack, device="cuda")
+    BL = dsdb_type.from_sparray(sparse.coo_matrix(bl), block_sizes, stack, device="cuda")
+    BG = dsdb_type.from_sparray(sparse.coo_matrix(bg), block_sizes, stack, device="cuda")
     solver = RGF(max_batch_size=max_batch_size)
     if use_out:
-        XR, XL, XG = (DSDBCOO.zeros_like(A) for _ in range(3))
+        XR, XL, XG = (dsdb_type.zeros_like(A) for _ in range(3))
         assert solver.selected_solve(A, BL, BG, out=[XL, XG, XR], return_retarded=return_retarded) is None
     elif return_retarded:
         XL, XG, XR = solver.selected_solve(A, BL, BG, return_retarded=True)
@@ -359,3 +365,70 @@ def test_partially_zero_self_energies(return_current):
         assert _rel(xr.blocks[i, i], ref["xr_diag"][i]) < TOL
     if return_current:
         assert _rel(res[3].cpu().numpy(), ref["current"]) < 1e-9
+
+
+@pytest.mark.parametrize("dsdb_type", DSDB_TYPES, ids=["DSDBCOO", "DSDBCSR"])
+def test_symmetric_storage_against_upstream_fixture(dsdb_type):
+    """Symmetric storage as quatrex's SCBA uses it (upper block triangle and
+    upper triangle of each diagonal block): a complex-symmetric system matrix
+    (symmetry_op = identity), skew-Hermitian self-energies and outputs
+    (symmetry_op = -conj), G^R diagonal stored complex-symmetric.  Against
+    upstream RGF.selected_solve on the same symmetric-storage operands
+    (tests/golden/dsdb_layouts.npz), on the stored entries and the completed
+    dense matrices."""
+    g = np.load(os.path.join(GOLDEN, "dsdb_layouts.npz"))
+    sizes = g["block_sizes"]
+    ident = lambda x: x  # noqa: E731
+    neg_conj = lambda x: -x.conj()  # noqa: E731
+    stack = (3,)
+    A = dsdb_type.from_sparray(sparse.coo_matrix(g["sym_a"]), sizes, stack, symmetry=True, symmetry_op=ident,
+                               device="cuda")
+    SL = dsdb_type.from_sparray(sparse.coo_matrix(g["sym_sigma_lesser"]), sizes, stack, symmetry=True,
+                                symmetry_op=neg_conj, device="cuda")
+    SG = dsdb_type.from_sparray(sparse.coo_matrix(g["sym_sigma_greater"]), sizes, stack, symmetry=True,
+                                symmetry_op=neg_conj, device="cuda")
+    XL, XG = dsdb_type.zeros_like(SL), dsdb_type.zeros_like(SL)
+    XR = dsdb_type.zeros_like(A)
+    assert RGF(max_batch_size=2).selected_solve(A, SL, SG, out=[XL, XG, XR], return_retarded=True) is None
+    assert _rel(XL.numpy_data()[1], g["sym_xl_data"]) < 1e-12
+    assert _rel(XR.numpy_data()[1], g["sym_xr_data"]) < 1e-12
+    for X, key in ((XL, "sym_xl"), (XG, "sym_xg"), (XR, "sym_xr")):
+        m = g[key] != 0
+        assert _rel(X.to_dense()[2] * m, g[key] * m) < 1e-12, key
+    # and against the dense definition on full storage
+    a = g["sym_a"]
+    ref_r = np.linalg.inv(a)
+    ref_l = ref_r @ g["sym_sigma_lesser"] @ ref_r.conj().T
+    m = XL.to_dense()[0] != 0
+    assert np.allclose(XL.to_dense()[0] * m, ref_l * m)
+
+
+class _UpstreamDSDBCOOStandIn:
+    """An object carrying only the attributes an upstream qttools DSDBCOO
+    exposes to a solver: data, rows, cols, block_sizes, num_blocks,
+    symmetry, symmetry_op (no method of this package's classes)."""
+
+    def __init__(self, data, rows, cols, block_sizes):
+        self.data = data
+        self.rows = rows
+        self.cols = cols
+        self.block_sizes = block_sizes
+        self.num_blocks = len(block_sizes)
+        self.symmetry = False
+        self.symmetry_op = np.conj
+
+
+def test_upstream_attribute_stand_in():
+    """The boundary reads only the upstream layout attributes: a stand-in
+    with rows / cols / block_sizes / data (NumPy data, as the upstream NumPy
+    backend holds it) is solved and written in place."""
+    g = np.load(os.path.join(GOLDEN, "dsdb_layouts.npz"))
+    sizes = g["block_sizes"]
+    a = g["a"]
+    stack = 4
+    data = np.broadcast_to(g["coo_full_data"], (stack, len(g["coo_full_data"]))).copy()
+    A = _UpstreamDSDBCOOStandIn(data, g["coo_full_rows"], g["coo_full_cols"], sizes)
+    out = _UpstreamDSDBCOOStandIn(np.zeros_like(data), g["coo_full_rows"], g["coo_full_cols"], sizes)
+    assert RGF(max_batch_size=3).selected_inv(A, out=out) is None
+    ref = np.linalg.inv(a)[g["coo_full_rows"], g["coo_full_cols"]]
+    assert _rel(out.data[2], ref) < 1e-12

@@ -14,6 +14,8 @@ from quatrex_b200.datastructures import DSDBCOO, block_sort_index, btd_layout_fr
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
 def _header_symbols():
     text = open(os.path.join(ROOT, "include", "qtx_rgf.h")).read()
     return sorted(set(re.findall(r"^\s*(?:qtx_status|const char\*|int64_t|size_t)\s+(qtx_\w+)\s*\(", text, re.M)))
@@ -184,3 +186,65 @@ def test_uneven_batch_job_plan():
     assert cost == sorted(cost, reverse=True)
     plain = BatchedTransport.jobs(SimpleNamespace(group_small=False), insts)
     assert all(kind == "one" and len(idx) == 1 for kind, idx in plain) and len(plain) == len(specs)
+
+
+def _fixture_rowptr(g, tag):
+    keys, ptrs, lens = g[f"csr_{tag}_keys"], g[f"csr_{tag}_ptrs"], g[f"csr_{tag}_lens"]
+    out, at = {}, 0
+    for k, n in zip(keys, lens):
+        out[(int(k[0]), int(k[1]))] = ptrs[at:at + n]
+        at += n
+    return out
+
+
+@pytest.mark.parametrize("sym", [False, True], ids=["full", "symmetric"])
+def test_layouts_match_upstream_fixture(sym):
+    """DSDBCOO and DSDBCSR built here from the same sparse matrix hold the data
+    in upstream's order, with upstream's row/column indices and row-pointer
+    map (tests/golden/dsdb_layouts.npz, written by upstream from_sparray)."""
+    from quatrex_b200.datastructures import DSDBCSR, layout_of
+
+    g = np.load(os.path.join(GOLDEN, "dsdb_layouts.npz"))
+    tag = "sym" if sym else "full"
+    sizes = g["block_sizes"]
+    coo = DSDBCOO.from_sparray(sparse.coo_matrix(g["a"]), sizes, (1,), symmetry=sym)
+    assert np.array_equal(coo.rows, g[f"coo_{tag}_rows"])
+    assert np.array_equal(coo.cols, g[f"coo_{tag}_cols"])
+    assert np.array_equal(coo.data[0], g[f"coo_{tag}_data"])
+    csr = DSDBCSR.from_sparray(sparse.coo_matrix(g["a"]), sizes, (1,), symmetry=sym)
+    assert np.array_equal(csr.cols, g[f"csr_{tag}_cols"])
+    assert np.array_equal(csr.data[0], g[f"csr_{tag}_data"])
+    ref_map = _fixture_rowptr(g, tag)
+    assert set(csr.rowptr_map) == set(ref_map)
+    for k, rp in ref_map.items():
+        assert np.array_equal(csr.rowptr_map[k], rp), k
+
+    class StandIn:  # only the attributes an upstream DSDBCSR exposes
+        pass
+
+    s = StandIn()
+    s.data, s.cols, s.rowptr_map, s.block_sizes = csr.data, csr.cols, ref_map, sizes
+    lay_s, lay_c = layout_of(s), layout_of(coo)
+    assert np.array_equal(lay_s.block_offset, lay_c.block_offset)
+    assert np.array_equal(lay_s.block_nnz, lay_c.block_nnz)
+    for a, b in zip(lay_s.local_index, lay_c.local_index):
+        assert (a is None and b is None) or np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("kind", ["conj", "neg_conj", "identity"])
+def test_symmetric_storage_completion(kind):
+    """get_block / to_dense of symmetric storage complete the lower blocks as
+    symmetry_op(X_ij^T) and the diagonal blocks as U + symmetry_op(U^T) with
+    the diagonal halved, for the three operators quatrex uses."""
+    from quatrex_b200.datastructures import DSDBCSR
+
+    rng = np.random.default_rng(4)
+    sizes = np.array([3, 4, 3])
+    full = _bt_pattern(list(sizes), 1.0, rng)
+    op = {"conj": np.conj, "neg_conj": lambda x: -np.conj(x), "identity": lambda x: x}[kind]
+    m = {"conj": full + full.conj().T, "neg_conj": full - full.conj().T, "identity": full + full.T}[kind]
+    for cls in (DSDBCOO, DSDBCSR):
+        x = cls.from_sparray(sparse.coo_matrix(m), sizes, (2,), symmetry=True, symmetry_op=op)
+        assert np.allclose(x.to_dense()[1], m)
+        assert np.allclose(x.blocks[2, 1], m[7:10, 3:7])
+        assert np.allclose(x.blocks[1, 1], m[3:7, 3:7])
