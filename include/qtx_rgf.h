@@ -193,6 +193,46 @@ qtx_status qtx_obc_fixed_point(qtx_ctx* ctx, int32_t n, int64_t batch, const voi
                                const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
                                const void* x, void* x_ref, double* abs_res, double* rel_res, qtx_stream stream);
 
+/* Spectral open-boundary condition (QuaTrEx's default OBC) in two device
+ * steps around a small dense eigenproblem that the caller solves:
+ *
+ * 1. qtx_beyn_moments: Beyn's contour moments of the lead's quadratic
+ *    eigenvalue problem (a_ji / w + a_ii + a_ij w) v = 0, for every energy
+ *    p0 = q0 y and p1 = q1 y (batch, n, m0) with
+ *    q0 = sum_q (z_o T(z_o)^-1 - z_i T(z_i)^-1) / N, q1 likewise with z^2,
+ *    T(z) = a_ji / z + a_ii + a_ij z, z on circles of radius r_o and r_i at
+ *    phases exp(2 pi i (q + 1.5) / N), q = 0..N-1 (N = num_quad_points), and
+ *    y (batch, n, m0) the caller's probe block.  QTX_E_SINGULAR when a
+ *    quadrature point hits an eigenvalue exactly.
+ *    <- Beyn._contour_integrate / _one_sided (src/qttools/nevp/beyn.py:187-330)
+ *       with the contour operator of src/qttools/kernels/operator.py:122-179.
+ * 2. (caller) the SVD projection and the m0 x m0 eigenproblem
+ *    (beyn.py:99-144, 241-289) give eigenvalues ws (batch, m0) and
+ *    eigenvectors vs (batch, n, m0); padding entries have ws = 0.
+ * 3. qtx_spectral_surface: normalises the columns of vs in place, classifies
+ *    the modes (propagating with Re dE/dk < 0 or decaying into the lead, with
+ *    residual below the tolerance; mask (device int32 (batch, m0), may be
+ *    NULL) receives the choice), builds x a_ij = V_r diag(1/w_r) (V_r^H V_r)^-1
+ *    V_r^H over the chosen modes, x = inv(a_ii + a_ji x a_ij) and then
+ *    num_ref_iterations fixed-point steps x = inv(a_ii - a_ji x a_ij).
+ *    <- Spectral._find_reflected_modes, _compute_x_ii and __call__
+ *       (src/qttools/boundary_conditions/obc/spectral.py:196-526),
+ *       block_sections = 1. */
+typedef struct qtx_spectral_params {
+  double min_decay, max_decay, min_propagation, residual_tolerance, eta_decay;
+  int32_t residual_normalization;
+  int32_t num_ref_iterations;
+} qtx_spectral_params;
+
+qtx_status qtx_beyn_moments(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                            const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji, double r_o,
+                            double r_i, int32_t num_quad_points, const void* y, int32_t m0, void* p0, void* p1,
+                            qtx_stream stream);
+qtx_status qtx_spectral_surface(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                                const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
+                                const void* ws, void* vs, int32_t m0, const qtx_spectral_params* params,
+                                int32_t* mask, void* x, qtx_stream stream);
+
 /* Contact self-energies from a surface Green's function g (batch, n, n):
  * sigma_r = m_ji g m_ij, gamma = i (sigma_r - sigma_r^H),
  * sigma_l = i f gamma, sigma_g = i (f - 1) gamma with f = occupancy[batch]

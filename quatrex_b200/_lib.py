@@ -55,6 +55,18 @@ class BtdDesc(ctypes.Structure):
     ]
 
 
+class SpectralParams(ctypes.Structure):
+    _fields_ = [
+        ("min_decay", c_double),
+        ("max_decay", c_double),
+        ("min_propagation", c_double),
+        ("residual_tolerance", c_double),
+        ("eta_decay", c_double),
+        ("residual_normalization", c_int32),
+        ("num_ref_iterations", c_int32),
+    ]
+
+
 class Obc(ctypes.Structure):
     _fields_ = [
         ("retarded", ctypes.POINTER(c_void_p)),
@@ -156,6 +168,16 @@ SIGNATURES = {
         c_int32,
         [c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_double, c_int32, c_void_p,
          c_void_p, c_void_p, ctypes.c_char_p, c_int32],
+    ),
+    "qtx_beyn_moments": (
+        c_int32,
+        [c_void_p, c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_double, c_double,
+         c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_void_p],
+    ),
+    "qtx_spectral_surface": (
+        c_int32,
+        [c_void_p, c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p,
+         c_int32, c_void_p, c_void_p, c_void_p, c_void_p],
     ),
     "qtx_obc_fixed_point": (
         c_int32,

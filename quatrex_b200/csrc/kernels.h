@@ -158,3 +158,29 @@ int64_t grouped_ws_elems(int max_nb, int b);
 void launch_transport_grouped(int b, const GroupedProblem* problems, int count, int64_t items,
                               unsigned long long* counter, int* flags, cplx* ws, int64_t ws_elems, int max_nb, int grid,
                               cudaStream_t stream);
+
+// ---- spectral open-boundary condition (spectral.cu) -----------------------
+// Mode-classification thresholds of qttools' Spectral OBC
+// (src/qttools/boundary_conditions/obc/spectral.py:63-94).
+struct SpectralFilter {
+  double min_decay = 1e-3, max_decay = 6.9, min_propagation = 0.01, residual_tolerance = 1e-3, eta_decay = 1e-14;
+  int residual_normalization = 1;
+};
+// out (batch * 2 nq, n, n) contiguous: a_ji / z + a_ii + a_ij z at the nq
+// points of the outer circle, then the nq of the inner one.
+void launch_contour_operator(int n, int64_t batch, int nq, double r_o, double r_i, MatView a_ii, MatView a_ij,
+                             MatView a_ji, cplx* out, cudaStream_t stream);
+// q0, q1 (batch, n, n) from the inverses (batch * 2 nq, n, n) of the operator.
+void launch_contour_moments(int n, int64_t batch, int nq, double r_o, double r_i, const cplx* inv, MutView q0,
+                            MutView q1, cudaStream_t stream);
+// Unit 2-norm columns of vs (batch, n, m), in place.
+void launch_normalize_columns(int n, int m, int64_t batch, cplx* vs, cudaStream_t stream);
+// mask (batch, m) of the reflected modes, from ws (batch, m), unit-column vs
+// (batch, n, m) and r_x = a_x vs (x = ji, ii, ij).
+void launch_mode_filter(int n, int m, int64_t batch, const cplx* ws, const cplx* vs, const cplx* r_ji,
+                        const cplx* r_ii, const cplx* r_ij, const SpectralFilter& f, int* mask, cudaStream_t stream);
+// vm = vs diag(mask), vw = vs diag(mask / w)   (batch, n, m)
+void launch_masked_modes(int n, int m, int64_t batch, const cplx* ws, const cplx* vs, const int* mask, cplx* vm,
+                         cplx* vw, cudaStream_t stream);
+// g[e] += diag(1 - mask[e])   (batch, m, m)
+void launch_gram_identity(int m, int64_t batch, const int* mask, cplx* g, cudaStream_t stream);

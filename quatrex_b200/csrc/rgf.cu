@@ -1970,6 +1970,116 @@ qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
   return st;
 }
 
+qtx_status qtx_beyn_moments(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                            const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji, double r_o,
+                            double r_i, int32_t num_quad_points, const void* y, int32_t m0, void* p0, void* p1,
+                            qtx_stream stream) {
+  return guarded(ctx, [&] {
+    if (n < 1 || batch < 0 || m0 < 1 || num_quad_points < 1 || !a_ii || !a_ij || !a_ji || !y || !p0 || !p1 ||
+        !(r_o > r_i) || !(r_i > 0))
+      throw QtxError(QTX_E_INVAL, "qtx_beyn_moments: bad arguments");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int nq = num_quad_points;
+    const int64_t nn = (int64_t)n * n;
+    // energies per pass: the 2 nq operator inverses of a pass stay below 4 GiB
+    const int64_t per_energy = (int64_t)2 * nq * nn * (int64_t)sizeof(cplx);
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(batch, ((int64_t)4 << 30) / per_energy));
+    DevBuf buf(sizeof(cplx) * (size_t)(chunk * 2 * nq * nn + 2 * chunk * nn) + sizeof(int) * (size_t)(chunk * 2 * nq),
+               s);
+    cplx* ops = buf.as<cplx>();
+    cplx* q = ops + chunk * 2 * nq * nn;
+    int* info = reinterpret_cast<int*>(q + 2 * chunk * nn);
+    QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * (size_t)(chunk * 2 * nq), s));
+    for (int64_t e0 = 0; e0 < batch; e0 += chunk) {
+      const int64_t ne = std::min(chunk, batch - e0);
+      MatView aii{reinterpret_cast<const cplx*>(a_ii) + e0 * stride_ii, n, stride_ii};
+      MatView aij{reinterpret_cast<const cplx*>(a_ij) + e0 * stride_ij, n, stride_ij};
+      MatView aji{reinterpret_cast<const cplx*>(a_ji) + e0 * stride_ji, n, stride_ji};
+      launch_contour_operator(n, ne, nq, r_o, r_i, aii, aij, aji, ops, s);
+      zinv(n, ne * 2 * nq, MatView{ops, n, nn}, MutView{ops, n, nn}, info, nullptr, s);
+      MutView q0{q, n, nn}, q1{q + ne * nn, n, nn};
+      launch_contour_moments(n, ne, nq, r_o, r_i, ops, q0, q1, s);
+      const int64_t ym = (int64_t)n * m0;
+      MatView yv{reinterpret_cast<const cplx*>(y) + e0 * ym, m0, ym};
+      gemm(n, m0, n, ne, ONE, q0, OP_N, yv, OP_N, MutView{reinterpret_cast<cplx*>(p0) + e0 * ym, m0, ym}, s);
+      gemm(n, m0, n, ne, ONE, q1, OP_N, yv, OP_N, MutView{reinterpret_cast<cplx*>(p1) + e0 * ym, m0, ym}, s);
+    }
+    read_info_or_throw(ctx, info, chunk * 2 * nq, s, "qtx_beyn_moments (contour operator)");
+  });
+}
+
+qtx_status qtx_spectral_surface(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
+                                const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
+                                const void* ws, void* vs, int32_t m0, const qtx_spectral_params* params,
+                                int32_t* mask, void* x, qtx_stream stream) {
+  return guarded(ctx, [&] {
+    if (n < 1 || batch < 0 || m0 < 1 || !a_ii || !a_ij || !a_ji || !ws || !vs || !params || !x ||
+        params->num_ref_iterations < 1)
+      throw QtxError(QTX_E_INVAL, "qtx_spectral_surface: bad arguments");
+    if (batch == 0) return;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int64_t nn = (int64_t)n * n, nm = (int64_t)n * m0, mm = (int64_t)m0 * m0;
+    DevBuf buf(sizeof(cplx) * (size_t)(batch * (5 * nm + 2 * mm + 3 * nn)) + sizeof(int) * (size_t)(batch * (m0 + 1)),
+               s);
+    cplx* p = buf.as<cplx>();
+    cplx* r_ji = p;
+    cplx* r_ii = r_ji + batch * nm;
+    cplx* r_ij = r_ii + batch * nm;
+    cplx* vm = r_ij + batch * nm;
+    cplx* vw = vm + batch * nm;
+    cplx* g = vw + batch * nm;
+    cplx* gi = g + batch * mm;
+    cplx* t0 = gi + batch * mm;
+    cplx* t1 = t0 + batch * nn;
+    cplx* t2 = t1 + batch * nn;
+    int* d_mask = reinterpret_cast<int*>(t2 + batch * nn);
+    int* info = d_mask + batch * m0;
+    QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * (size_t)batch, s));
+    MatView aii{reinterpret_cast<const cplx*>(a_ii), n, stride_ii};
+    MatView aij{reinterpret_cast<const cplx*>(a_ij), n, stride_ij};
+    MatView aji{reinterpret_cast<const cplx*>(a_ji), n, stride_ji};
+    cplx* v = reinterpret_cast<cplx*>(vs);
+    const cplx* w = reinterpret_cast<const cplx*>(ws);
+    // unit eigenvectors (spectral.py:355-358), then the mode classification
+    launch_normalize_columns(n, m0, batch, v, s);
+    MatView vv{v, m0, nm};
+    gemm(n, m0, n, batch, ONE, aji, OP_N, vv, OP_N, MutView{r_ji, m0, nm}, s);
+    gemm(n, m0, n, batch, ONE, aii, OP_N, vv, OP_N, MutView{r_ii, m0, nm}, s);
+    gemm(n, m0, n, batch, ONE, aij, OP_N, vv, OP_N, MutView{r_ij, m0, nm}, s);
+    SpectralFilter f;
+    f.min_decay = params->min_decay;
+    f.max_decay = params->max_decay;
+    f.min_propagation = params->min_propagation;
+    f.residual_tolerance = params->residual_tolerance;
+    f.eta_decay = params->eta_decay;
+    f.residual_normalization = params->residual_normalization;
+    launch_mode_filter(n, m0, batch, w, v, r_ji, r_ii, r_ij, f, d_mask, s);
+    // x a_ij = V_r diag(1 / w_r) (V_r^H V_r)^-1 V_r^H over the reflected modes
+    // (spectral.py:400-415): with the unselected columns zeroed and the
+    // unselected block of the Gram matrix set to the identity, one batched
+    // product covers every energy whatever its number of modes
+    launch_masked_modes(n, m0, batch, w, v, d_mask, vm, vw, s);
+    gemm(m0, m0, n, batch, ONE, MatView{vm, m0, nm}, OP_C, MatView{vm, m0, nm}, OP_N, MutView{g, m0, mm}, s);
+    launch_gram_identity(m0, batch, d_mask, g, s);
+    zinv(m0, batch, MatView{g, m0, mm}, MutView{gi, m0, mm}, nullptr, nullptr, s);
+    // t0 (m0 x n) = G^-1 V_m^H ; t1 = V_w t0 = x a_ij
+    gemm(m0, n, m0, batch, ONE, MatView{gi, m0, mm}, OP_N, MatView{vm, m0, nm}, OP_C, MutView{t0, n, nm}, s);
+    gemm(n, n, m0, batch, ONE, MatView{vw, m0, nm}, OP_N, MatView{t0, n, nm}, OP_N, MutView{t1, n, nn}, s);
+    // x = inv(a_ii + a_ji (x a_ij)), then num_ref_iterations fixed-point
+    // steps x = inv(a_ii - a_ji x a_ij) (spectral.py:491-526)
+    gemm(n, n, n, batch, ONE, aji, OP_N, MatView{t1, n, nn}, OP_N, MutView{t2, n, nn}, s, aii, ONE);
+    MutView xv{reinterpret_cast<cplx*>(x), n, nn};
+    zinv(n, batch, MatView{t2, n, nn}, xv, info, nullptr, s);
+    for (int it = 0; it < params->num_ref_iterations; ++it) {
+      gemm(n, n, n, batch, ONE, aji, OP_N, xv, OP_N, MutView{t0, n, nn}, s);
+      gemm(n, n, n, batch, MONE, MatView{t0, n, nn}, OP_N, aij, OP_N, MutView{t2, n, nn}, s, aii, ONE);
+      zinv(n, batch, MatView{t2, n, nn}, xv, info, nullptr, s);
+    }
+    if (mask) QTX_CUDA_TRY(cudaMemcpyAsync(mask, d_mask, sizeof(int) * (size_t)(batch * m0), cudaMemcpyDeviceToDevice, s));
+    read_info_or_throw(ctx, info, batch, s, "qtx_spectral_surface");
+  });
+}
+
 qtx_status qtx_obc_fixed_point(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
                                const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
                                const void* x, void* x_ref, double* abs_res, double* rel_res, qtx_stream stream) {

@@ -12,6 +12,7 @@ O(tol^2) per extra iteration, far below the parity tolerance.
 
 from __future__ import annotations
 
+import ctypes
 import math
 
 import numpy as np
@@ -78,6 +79,85 @@ class SanchoRubio:
         if host:
             return x.cpu().numpy()
         return x
+
+
+class Spectral:
+    """Surface Green's function from the lead's eigenmodes on the GPU (the
+    default OBC of quatrex, ``src/quatrex/core/config.py:163``).
+
+    Mirrors ``src/qttools/boundary_conditions/obc/spectral.py:15-526``: the
+    same constructor and defaults, the same mode classification
+    (propagating with Re dE/dk < 0 or decaying into the lead, residual below
+    ``residual_tolerance``), x a_ij = V_r diag(1/w_r) pinv(V_r), then
+    ``num_ref_iterations`` fixed-point steps.  The eigenpairs come from
+    ``nevp`` (``quatrex_b200.nevp.Beyn``); the mode classification, the
+    selection and the surface recursion run in ``qtx_spectral_surface``.
+    Only ``block_sections = 1`` and ``return_injected = False`` are offered
+    (the wave-function formalism's injection vectors are out of scope).
+    """
+
+    def __init__(self, nevp, block_sections: int = 1, min_decay: float = 1e-3, max_decay: float = 6.9,
+                 num_ref_iterations: int = 2, min_propagation: float = 0.01, residual_tolerance: float = 1e-3,
+                 residual_normalization: bool = True, warning_threshold: float = 1e-1, eta_decay: float = 1e-14):
+        if num_ref_iterations < 1:
+            raise ValueError("Number of refinement iterations must be at least 1.")
+        if block_sections != 1:
+            raise NotImplementedError("Spectral on the device: block_sections = 1 only")
+        self.nevp = nevp
+        self.block_sections = block_sections
+        self.min_decay = min_decay
+        self.max_decay = max_decay
+        self.num_ref_iterations = num_ref_iterations
+        self.min_propagation = min_propagation
+        self.residual_tolerance = residual_tolerance
+        self.residual_normalization = residual_normalization
+        self.warning_threshold = warning_threshold
+        self.eta_decay = eta_decay
+        self.last_mask = None
+
+    def __call__(self, a_ii, a_ij, a_ji, contact: str = "", return_injected: bool = False):
+        """Returns the surface Green's function x = inv(a_ii - a_ji x a_ij)."""
+        if return_injected:
+            raise NotImplementedError("injection vectors (wave-function formalism) are not offered")
+        if not torch.cuda.is_available():
+            raise RuntimeError("quatrex_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
+        dev = torch.cuda.current_device()
+        tii, host = _as_device(a_ii, dev)
+        tij, _ = _as_device(a_ij, dev)
+        tji, _ = _as_device(a_ji, dev)
+        squeeze = tii.dim() == 2
+        if squeeze:
+            tii = tii[None]
+        n = tii.shape[-1]
+        batch_shape = tuple(tii.shape[:-2])
+        batch = int(math.prod(batch_shape))
+        tii = tii.reshape(batch, n, n)
+        tij = tij.reshape(-1, n, n) if tij.dim() > 2 else tij
+        tji = tji.reshape(-1, n, n) if tji.dim() > 2 else tji
+        ws, vs = self.nevp((tji, tii, tij))
+        m0 = ws.shape[-1]
+        ws = ws.reshape(batch, m0).contiguous()
+        vs = vs.reshape(batch, n, m0).contiguous()
+        _, sii = _batch_view(tii)
+        _, sij = _batch_view(tij)
+        _, sji = _batch_view(tji)
+        params = _lib.SpectralParams(min_decay=self.min_decay, max_decay=self.max_decay,
+                                     min_propagation=self.min_propagation, residual_tolerance=self.residual_tolerance,
+                                     eta_decay=self.eta_decay, residual_normalization=int(bool(self.residual_normalization)),
+                                     num_ref_iterations=int(self.num_ref_iterations))
+        mask = torch.empty((batch, m0), dtype=torch.int32, device=f"cuda:{dev}")
+        x = torch.empty((batch, n, n), dtype=torch.complex128, device=f"cuda:{dev}")
+        lib = _lib.load()
+        ctx = _lib.context(dev)
+        st = lib.qtx_spectral_surface(ctx, n, batch, tii.data_ptr(), sii, tij.data_ptr(), sij, tji.data_ptr(), sji,
+                                      ws.data_ptr(), vs.data_ptr(), m0, ctypes.byref(params), mask.data_ptr(),
+                                      x.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        _lib.check(st, ctx, "Spectral")
+        self.last_mask = mask.reshape(batch_shape + (m0,))
+        x = x.reshape(batch_shape + (n, n))
+        if squeeze:
+            x = x[0]
+        return x.cpu().numpy() if host else x
 
 
 def contact_self_energies(g, m_ji, m_ij, occupancy):

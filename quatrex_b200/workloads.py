@@ -98,3 +98,24 @@ def uneven_instances(count: int, seed: int = 4321):
         ne = int(rng.integers(64, 513))
         out.append(dict(num_blocks=nb, block_size=b, num_energies=ne, seed=seed + 1 + k))
     return out
+
+
+def make_lead(block_size: int, coupling_rank: int, num_energies: int, seed: int = 0, e_min: float = -1.0,
+              e_max: float = 1.0, eta: float = 1e-6):
+    """Boundary blocks of a semi-infinite lead whose cells couple through
+    their last / first ``coupling_rank`` orbitals only (as the boundary
+    orbitals of a real wire do), for the spectral OBC: the quadratic
+    eigenproblem (a_ji / w + a_ii + a_ij w) v = 0 then has 2 coupling_rank
+    finite nonzero eigenvalues.  H_00 as in ``make_device``; the coupling
+    block Y / sqrt(k) sits in rows b-k.., columns ..k.  Returns
+    (a_ii (E, b, b), a_ij (b, b), a_ji (b, b), energies)."""
+    b, k = int(block_size), int(coupling_rank)
+    rng = np.random.default_rng(seed)
+    x = (rng.standard_normal((b, b)) + 1j * rng.standard_normal((b, b))) / np.sqrt(2.0)
+    h = (x + x.conj().T) / (2.0 * np.sqrt(b)) + np.diag(rng.normal(0.0, 0.5, b))
+    y = (rng.standard_normal((k, k)) + 1j * rng.standard_normal((k, k))) / np.sqrt(2.0)
+    t = np.zeros((b, b), dtype=np.complex128)
+    t[b - k:, :k] = y / np.sqrt(k)
+    energies = np.linspace(e_min, e_max, int(num_energies))
+    a_ii = (energies[:, None, None] + 1j * eta) * np.eye(b) - h[None]
+    return a_ii, -t, -t.conj().T, energies

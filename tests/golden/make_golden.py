@@ -25,6 +25,9 @@ never runs on the GPU machine and nothing imports it.  It imports the upstream
   upstream G^R and the energies that upstream ``ElectronSolver._filter_peaks``
   zeroes for a peak limit set to the median of the largest DOS slopes.
 
+* ``spectral_small.npz`` -- upstream ``Spectral(Beyn(...))`` surface Green's
+  functions of a seeded b=16 lead with a rank-4 coupling at 8 energies, with
+  the NEVP eigenpairs of the first call and upstream Sancho-Rubio's result.
 * ``dsdb_layouts.npz`` -- upstream DSDBCOO and DSDBCSR layouts (full and
   symmetric storage) of one seeded sparse BTD pattern with mixed block sizes,
   and upstream ``RGF.selected_solve`` on symmetric-storage operands.
@@ -256,6 +259,32 @@ def observables_small():
     print("observables_small written", int(mask.sum()), "of", len(mask), "energies masked")
 
 
+def spectral_small():
+    """Upstream Spectral(Beyn) surface Green's functions of a seeded lead
+    whose cells couple through 4 of their 16 orbitals (workloads.make_lead,
+    8 energies; Beyn with r_o=10, r_i=0.8, m_0=16, 20 quadrature points, the
+    other Spectral parameters at their defaults), with the eigenpairs of the
+    first call and the Sancho-Rubio result of the same lead."""
+    from qttools.boundary_conditions.obc import Spectral
+    from qttools.nevp import Beyn
+
+    from quatrex_b200.workloads import make_lead
+
+    a_ii, a_ij, a_ji, energies = make_lead(16, 4, 8, seed=5)
+    out = {"energies": energies, "r_o": 10.0, "r_i": 0.8, "m_0": 16, "num_quad_points": 20,
+           "a_ii": a_ii, "a_ij": a_ij, "a_ji": a_ji}
+    bij = np.broadcast_to(a_ij, a_ii.shape).copy()
+    bji = np.broadcast_to(a_ji, a_ii.shape).copy()
+    nevp = Beyn(r_o=10.0, r_i=0.8, m_0=16, num_quad_points=20)
+    ws, vs = nevp((bji, a_ii, bij))
+    nevp.rng = np.random.default_rng(42)  # the probe block of a first call again
+    out["x"] = Spectral(nevp=nevp)(a_ii, bij, bji, contact="left")
+    out["ws"], out["vs"] = ws, vs
+    out["x_sancho_rubio"] = SanchoRubio(max_iterations=200, convergence_tol=1e-12)(a_ii, bij, bji, contact="left")
+    np.savez_compressed(os.path.join(HERE, "spectral_small.npz"), **out)
+    print("spectral_small written")
+
+
 def _rowptr_arrays(m):
     keys = sorted(m.rowptr_map.keys())
     ptrs = [np.asarray(m.rowptr_map[k], dtype=np.int64) for k in keys]
@@ -320,3 +349,4 @@ if __name__ == "__main__":
     transport_cfg_small_subset()
     observables_small()
     dsdb_layouts()
+    spectral_small()

@@ -209,3 +209,22 @@ def test_keldysh_recursion_is_linear_in_the_contact_sources():
             got_g = (f_l - 1) * x_l[f"xl_{part}"][i] + (f_r - 1) * x_r[f"xl_{part}"][i]
             assert _rel(got_l, want_l) < 1e-12, (part, i)
             assert _rel(got_g, want_g) < 1e-12, (part, i)
+
+
+def test_spectral_oracle_against_upstream():
+    """The spectral-OBC restatement (Beyn + Spectral, block_sections = 1)
+    reproduces upstream's surface Green's functions and eigenvalues on the
+    fixture written by upstream Spectral(Beyn(...)) (tests/golden/spectral_small.npz)."""
+    from oracle import spectral_oracle as so
+
+    g = np.load(os.path.join(GOLDEN, "spectral_small.npz"))
+    x, info = so.spectral(g["a_ii"], g["a_ij"], g["a_ji"], r_o=float(g["r_o"]), r_i=float(g["r_i"]),
+                          m_0=int(g["m_0"]), num_quad_points=int(g["num_quad_points"]), rng=np.random.default_rng(42))
+    rel = np.linalg.norm(x - g["x"], axis=(-2, -1)) / np.linalg.norm(g["x"], axis=(-2, -1))
+    assert rel.max() < 1e-12
+    # the eigenvalues of the first call (same probe block), as sets
+    for e in range(len(g["energies"])):
+        assert np.allclose(np.sort_complex(info["ws"][e]), np.sort_complex(g["ws"][e]), rtol=0, atol=1e-12)
+    # on this lead (rank-4 coupling) the spectral OBC agrees with Sancho-Rubio
+    rel_sr = np.linalg.norm(x - g["x_sancho_rubio"], axis=(-2, -1)) / np.linalg.norm(g["x_sancho_rubio"], axis=(-2, -1))
+    assert rel_sr.max() < 2e-9
