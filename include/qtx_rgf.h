@@ -131,6 +131,17 @@ qtx_status qtx_zgemm(qtx_ctx* ctx, int32_t m, int32_t n, int32_t k, int64_t batc
                      double beta_im, const void* c, int64_t ldc, int64_t stride_c, void* d, int64_t ldd,
                      int64_t stride_d, int32_t precision, qtx_stream stream);
 
+/* Batched block combination out = alpha op(x) + beta op(y), op = 0 (none) or
+ * 1 (conjugate transpose; op(x) is rows x cols, x itself cols x rows); y may
+ * be NULL.  The element-wise glue of the partitioned solver (RGFDist), whose
+ * block products run through qtx_zgemm and inverses through qtx_inv.  No
+ * reference counterpart as a call: upstream forms these sums with NumPy /
+ * CuPy array expressions (src/qttools/greens_function_solver/_serinv.py). */
+qtx_status qtx_block_combine(qtx_ctx* ctx, int32_t rows, int32_t cols, int64_t batch, double alpha_re,
+                             double alpha_im, const void* x, int64_t ldx, int64_t stride_x, int32_t op_x,
+                             double beta_re, double beta_im, const void* y, int64_t ldy, int64_t stride_y,
+                             int32_t op_y, void* out, int64_t ldo, int64_t stride_out, qtx_stream stream);
+
 /* Selected inversion: out receives X = A^-1 on the BTD pattern of out_desc.
  * obc_retarded: NULL or host [nb] of device pointers subtracted from A_ii.
  * <- RGF.selected_inv(a, obc_blocks, out) (rgf.py:25-113). */

@@ -169,6 +169,11 @@ SIGNATURES = {
         [c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_double, c_int32, c_void_p,
          c_void_p, c_void_p, ctypes.c_char_p, c_int32],
     ),
+    "qtx_block_combine": (
+        c_int32,
+        [c_void_p, c_int32, c_int32, c_int64, c_double, c_double, c_void_p, c_int64, c_int64, c_int32, c_double,
+         c_double, c_void_p, c_int64, c_int64, c_int32, c_void_p, c_int64, c_int64, c_void_p],
+    ),
     "qtx_beyn_moments": (
         c_int32,
         [c_void_p, c_int32, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_double, c_double,

@@ -276,6 +276,69 @@ __global__ void fill_int_kernel(int* p, int64_t count, int value) {
     p[t] = value;
 }
 
+// out = alpha op(x) + beta op(y) over (batch, rows, cols) blocks, op(z) = z or
+// z^H (then z is cols x rows).  Transposed operands go through a 32 x 33
+// shared-memory tile so that both the read and the write are coalesced.
+template <int OPX, int OPY>
+__global__ void block_combine_kernel(int rows, int cols, int64_t batch, cplx alpha, const cplx* x, int64_t ldx,
+                                     int64_t sx, cplx beta, const cplx* y, int64_t ldy, int64_t sy, cplx* out,
+                                     int64_t ldo, int64_t so) {
+  __shared__ cplx tx[32][33];
+  __shared__ cplx ty[32][33];
+  const int tiles_c = (cols + 31) / 32;
+  const int tr = blockIdx.x / tiles_c, tc = blockIdx.x % tiles_c;
+  const int r0 = tr * 32, c0 = tc * 32;
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;  // 32 x 8 threads
+  for (int64_t e = blockIdx.y; e < batch; e += gridDim.y) {
+    const cplx* xe = x + e * sx;
+    const cplx* ye = y ? y + e * sy : nullptr;
+    if (OPX || OPY) {
+      // stage the transposed operands: element (c, r) of the source lands at tile[r - r0][c - c0]
+      for (int k = ly; k < 32; k += 8) {
+        const int sr = c0 + k, sc = r0 + lx;  // source row (an output column), source column
+        if (OPX) tx[lx][k] = (sr < cols && sc < rows) ? xe[(int64_t)sr * ldx + sc] : cmk(0, 0);
+        if (OPY && ye) ty[lx][k] = (sr < cols && sc < rows) ? ye[(int64_t)sr * ldy + sc] : cmk(0, 0);
+      }
+      __syncthreads();
+    }
+    for (int k = ly; k < 32; k += 8) {
+      const int r = r0 + k, c = c0 + lx;
+      if (r < rows && c < cols) {
+        const cplx vx = OPX ? cconj(tx[k][lx]) : xe[(int64_t)r * ldx + c];
+        cplx v = cmul(alpha, vx);
+        if (ye) {
+          const cplx vy = OPY ? cconj(ty[k][lx]) : ye[(int64_t)r * ldy + c];
+          v = cfma(beta, vy, v);
+        }
+        out[e * so + (int64_t)r * ldo + c] = v;
+      }
+    }
+    if (OPX || OPY) __syncthreads();
+  }
+}
+
+// Small status reads for the host without a copy engine: one CTA scans
+// src[0, n) and stores into mapped page-locked host memory
+// out[0] = 1 + index of the first nonzero entry (0: none), out[1] = that
+// entry, out[2] = src[0].  (A cudaMemcpy of a status word queues behind any
+// large device-to-host copy in flight on the copy engine.)
+__global__ void flag_reduce_kernel(const int* src, int64_t n, int* out) {
+  __shared__ unsigned long long first;
+  if (threadIdx.x == 0) first = ~0ull;
+  __syncthreads();
+  for (int64_t t = threadIdx.x; t < n; t += blockDim.x)
+    if (src[t] != 0) atomicMin(&first, (unsigned long long)t);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile int* o = out;
+    const bool any = first != ~0ull;
+    o[0] = any ? (int)(first + 1) : 0;
+    o[1] = any ? src[first] : 0;
+    o[2] = n > 0 ? src[0] : 0;
+    __threadfence_system();
+  }
+}
+
 // One CTA column per block slice (blockIdx.y), CTAs stride over the data rows:
 // flags[k] = 1 once any entry of slice k is nonzero (NaN counts as nonzero).
 // Slice k is entries [slices[2k], slices[2k] + slices[2k + 1]) of every row.
@@ -440,6 +503,32 @@ void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream) {
   if (count <= 0) return;
   fill_int_kernel<<<grid_for(count), TB, 0, stream>>>(p, count, value);
   qtx_check_launch("fill_int_kernel");
+}
+
+void launch_flag_reduce(const int* src, int64_t n, int* mapped_out, cudaStream_t stream) {
+  flag_reduce_kernel<<<1, 256, 0, stream>>>(src, n, mapped_out);
+  qtx_check_launch("flag_reduce_kernel");
+}
+
+void launch_block_combine(int rows, int cols, int64_t batch, cplx alpha, MatView x, int op_x, cplx beta, MatView y,
+                          int op_y, MutView out, cudaStream_t stream) {
+  if (rows <= 0 || cols <= 0 || batch <= 0) return;
+  const unsigned tiles = (unsigned)(((rows + 31) / 32) * ((cols + 31) / 32));
+  const dim3 grid(tiles, (unsigned)std::min<int64_t>(batch, 65535));
+  const cplx* yp = y.ptr;
+  if (op_x == OP_N && op_y == OP_N)
+    block_combine_kernel<0, 0><<<grid, 256, 0, stream>>>(rows, cols, batch, alpha, x.ptr, x.ld, x.stride, beta, yp,
+                                                         y.ld, y.stride, out.ptr, out.ld, out.stride);
+  else if (op_x == OP_C && op_y == OP_N)
+    block_combine_kernel<1, 0><<<grid, 256, 0, stream>>>(rows, cols, batch, alpha, x.ptr, x.ld, x.stride, beta, yp,
+                                                         y.ld, y.stride, out.ptr, out.ld, out.stride);
+  else if (op_x == OP_N && op_y == OP_C)
+    block_combine_kernel<0, 1><<<grid, 256, 0, stream>>>(rows, cols, batch, alpha, x.ptr, x.ld, x.stride, beta, yp,
+                                                         y.ld, y.stride, out.ptr, out.ld, out.stride);
+  else
+    block_combine_kernel<1, 1><<<grid, 256, 0, stream>>>(rows, cols, batch, alpha, x.ptr, x.ld, x.stride, beta, yp,
+                                                         y.ld, y.stride, out.ptr, out.ld, out.stride);
+  qtx_check_launch("block_combine_kernel");
 }
 
 void launch_block_nonzero(int num_slices, const int64_t* slices, const cplx* data, int64_t stride, int64_t rows,

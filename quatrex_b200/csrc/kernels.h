@@ -101,6 +101,14 @@ void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream);
 void launch_residual_norm(int n, int64_t batch, MatView x_ref, MatView x, double* abs_res, double* rel_res,
                           cudaStream_t stream);
 void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t stream);
+// mapped_out (device alias of mapped page-locked host memory, 3 ints):
+// [0] = 1 + index of the first nonzero src entry or 0, [1] = that entry,
+// [2] = src[0].  The host reads it after synchronising the stream.
+void launch_flag_reduce(const int* src, int64_t n, int* mapped_out, cudaStream_t stream);
+// out = alpha op(x) + beta op(y) (rows x cols each; y optional: ptr == nullptr),
+// op = OP_N or OP_C.  out must not overlap x or y when an operand is transposed.
+void launch_block_combine(int rows, int cols, int64_t batch, cplx alpha, MatView x, int op_x, cplx beta, MatView y,
+                          int op_y, MutView out, cudaStream_t stream);
 // flags[k] = 1 if block slice k of a DSDBSparse data stack holds any nonzero
 // entry in any of `rows` data rows (flags zeroed by the caller).  slices
 // (device int64 [2 * num_slices]): (offset, nnz) of each slice in a row;

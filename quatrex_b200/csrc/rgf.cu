@@ -198,7 +198,8 @@ struct qtx_ctx {
   std::string last_error;
   int64_t launches = 0;
   size_t mem_limit = 0;
-  int* h_pinned = nullptr;     // pinned host word (process-wide pool)
+  int* h_pinned = nullptr;     // pinned host words (process-wide pool)
+  int* d_pinned = nullptr;     // their device alias: status words are stored there by a kernel
   PinRing* ring = nullptr;     // page-locked staging of the host-buffer mode (process-wide pool)
   bool timing = false;
   std::vector<TimedLaunch> timed;
@@ -453,15 +454,26 @@ BlockStack carve(cplx*& cursor, const std::vector<int>& sizes, int64_t ne, int b
   return st;
 }
 
-void read_info_or_throw(qtx_ctx* ctx, const int* d_info, int64_t n, cudaStream_t s, const char* what) {
-  // reduce: any nonzero -> first nonzero column
-  std::vector<int> h(n);
-  QTX_CUDA_TRY(cudaMemcpyAsync(h.data(), d_info, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+// Status words of a call, read through a kernel store into the context's
+// mapped page-locked words (no copy engine: a status read must not queue
+// behind a caller's large download running on another stream).
+struct StatusRead {
+  int first;  // 1 + index of the first nonzero entry, 0 if none
+  int value;  // that entry
+  int head;   // entry 0
+};
+StatusRead read_status(qtx_ctx* ctx, const int* d, int64_t n, cudaStream_t s) {
+  launch_flag_reduce(d, n, ctx->d_pinned, s);
   QTX_CUDA_TRY(cudaStreamSynchronize(s));
-  for (int64_t e = 0; e < n; ++e)
-    if (h[e]) throw QtxError(QTX_E_SINGULAR, std::string(what) + ": exactly singular diagonal block (stack entry " +
-                                                 std::to_string(e) + ", pivot " + std::to_string(h[e]) + ")");
-  (void)ctx;
+  volatile int* h = ctx->h_pinned;
+  return StatusRead{h[0], h[1], h[2]};
+}
+
+void read_info_or_throw(qtx_ctx* ctx, const int* d_info, int64_t n, cudaStream_t s, const char* what) {
+  const StatusRead r = read_status(ctx, d_info, n, s);
+  if (r.first)
+    throw QtxError(QTX_E_SINGULAR, std::string(what) + ": exactly singular diagonal block (stack entry " +
+                                       std::to_string(r.first - 1) + ", pivot " + std::to_string(r.value) + ")");
 }
 
 // ---------------------------------------------------------------------------
@@ -863,9 +875,7 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
     std::swap(beta.ptr, t2.ptr);
     QTX_CUDA_TRY(cudaMemsetAsync(num_active, 0, sizeof(int), s));
     launch_sr_norm_update(n, batch, alpha, beta, tol, active, its, num_active, s);
-    QTX_CUDA_TRY(cudaMemcpyAsync(ctx->h_pinned, num_active, sizeof(int), cudaMemcpyDeviceToHost, s));
-    QTX_CUDA_TRY(cudaStreamSynchronize(s));
-    if (ctx->h_pinned[0] == 0) {
+    if (read_status(ctx, num_active, 1, s).head == 0) {
       converged = true;
       break;
     }
@@ -1674,6 +1684,12 @@ qtx_status qtx_ctx_create(int device, qtx_ctx** out) {
     delete c;
     return QTX_E_NOMEM;
   }
+  if (cudaHostGetDevicePointer((void**)&c->d_pinned, c->h_pinned, 0) != cudaSuccess) {
+    cudaGetLastError();
+    pinned_give(c->h_pinned);
+    delete c;
+    return QTX_E_CUDA;
+  }
   *out = c;
   return QTX_OK;
 }
@@ -1968,6 +1984,22 @@ qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
     return QTX_E_NOT_CONVERGED;
   }
   return st;
+}
+
+qtx_status qtx_block_combine(qtx_ctx* ctx, int32_t rows, int32_t cols, int64_t batch, double alpha_re,
+                             double alpha_im, const void* x, int64_t ldx, int64_t stride_x, int32_t op_x,
+                             double beta_re, double beta_im, const void* y, int64_t ldy, int64_t stride_y,
+                             int32_t op_y, void* out, int64_t ldo, int64_t stride_out, qtx_stream stream) {
+  return guarded(ctx, [&] {
+    if (rows < 0 || cols < 0 || batch < 0 || !x || !out || (op_x != 0 && op_x != 1) || (op_y != 0 && op_y != 1))
+      throw QtxError(QTX_E_INVAL, "qtx_block_combine: bad arguments");
+    if ((op_x == OP_C && x == out) || (y && op_y == OP_C && y == out))
+      throw QtxError(QTX_E_INVAL, "qtx_block_combine: a transposed operand may not alias the output");
+    launch_block_combine(rows, cols, batch, cmk(alpha_re, alpha_im),
+                         MatView{reinterpret_cast<const cplx*>(x), ldx, stride_x}, op_x, cmk(beta_re, beta_im),
+                         MatView{reinterpret_cast<const cplx*>(y), ldy, stride_y}, op_y,
+                         MutView{reinterpret_cast<cplx*>(out), ldo, stride_out}, reinterpret_cast<cudaStream_t>(stream));
+  });
 }
 
 qtx_status qtx_beyn_moments(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,

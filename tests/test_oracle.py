@@ -228,3 +228,47 @@ def test_spectral_oracle_against_upstream():
     # on this lead (rank-4 coupling) the spectral OBC agrees with Sancho-Rubio
     rel_sr = np.linalg.norm(x - g["x_sancho_rubio"], axis=(-2, -1)) / np.linalg.norm(g["x_sancho_rubio"], axis=(-2, -1))
     assert rel_sr.max() < 2e-9
+
+
+@pytest.mark.parametrize("num_partitions", [2, 3, 4, 6])
+def test_partitioned_oracle_equals_rgf_oracle(num_partitions):
+    """The nested-dissection restatement (RGFDist / _serinv) returns the
+    blocks of the plain RGF restatement -- pinned to upstream fixtures -- to
+    rounding, for selected inversion and selected solve with contact blocks
+    and interior self-energies (upstream RGFDist needs several MPI ranks and
+    cannot run in this container, so it is pinned through this equality)."""
+    from oracle import rgf_dist_oracle as rd
+
+    rng = np.random.default_rng(num_partitions)
+
+    def rnd(*s):
+        return rng.standard_normal(s) + 1j * rng.standard_normal(s)
+
+    def skew(x):
+        return x - x.conj().swapaxes(-1, -2)
+
+    nb, b, ne = 13, 4, 3
+    diag = [rnd(ne, b, b) + 6 * np.eye(b) for _ in range(nb)]
+    upper = [rnd(ne, b, b) for _ in range(nb - 1)]
+    lower = [rnd(ne, b, b) for _ in range(nb - 1)]
+    sl_d, sl_u = [skew(rnd(ne, b, b)) for _ in range(nb)], [rnd(ne, b, b) for _ in range(nb - 1)]
+    sg_d, sg_u = [skew(rnd(ne, b, b)) for _ in range(nb)], [rnd(ne, b, b) for _ in range(nb - 1)]
+    pad = [None] * (nb - 2)
+    obc_r = [rnd(ne, b, b), *pad, rnd(ne, b, b)]
+    obc_l = [skew(rnd(ne, b, b)), *pad, skew(rnd(ne, b, b))]
+    obc_g = [skew(rnd(ne, b, b)), *pad, skew(rnd(ne, b, b))]
+
+    def rel(a, r):
+        return np.linalg.norm(a - r) / np.linalg.norm(r)
+
+    ref_inv = orc.selected_inv(diag, upper, lower, obc_r)
+    got_inv = rd.selected_inv(diag, upper, lower, obc_r, num_partitions=num_partitions)
+    for k in range(3):
+        assert max(rel(a, r) for a, r in zip(got_inv[k], ref_inv[k])) < 1e-12
+    ref = orc.selected_solve(diag, upper, lower, sl_d, sl_u, sg_d, sg_u, obc_r, obc_l, obc_g)
+    got = rd.selected_solve(diag, upper, lower, sl_d, sl_u, sg_d, sg_u, obc_r, obc_l, obc_g,
+                            num_partitions=num_partitions)
+    for key in ("xl_diag", "xl_upper", "xl_lower", "xg_diag", "xg_upper", "xg_lower", "xr_diag"):
+        assert max(rel(a, r) for a, r in zip(got[key], ref[key])) < 1e-12, key
+    with pytest.raises(ValueError):
+        rd.partition_bounds(5, 3)
