@@ -363,6 +363,11 @@ __global__ void block_nonzero_kernel(const int64_t* slices, const cplx* data, in
   }
 }
 
+__global__ void copy_int_kernel(int* dst, int64_t dst_stride, const int* src, int64_t src_stride, int64_t count) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
+    dst[t * dst_stride] = src[t * src_stride];
+}
+
 __global__ void real_part_kernel(int64_t count, const cplx* src, double* dst) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
     dst[t] = src[t].x;
@@ -537,6 +542,13 @@ void launch_block_nonzero(int num_slices, const int64_t* slices, const cplx* dat
   const unsigned gx = (unsigned)std::min<int64_t>(rows, 256);
   block_nonzero_kernel<<<dim3(gx, (unsigned)num_slices), TB, 0, stream>>>(slices, data, stride, rows, flags);
   qtx_check_launch("block_nonzero_kernel");
+}
+
+void launch_copy_int(int* dst, int64_t dst_stride, const int* src, int64_t src_stride, int64_t count,
+                     cudaStream_t stream) {
+  if (count <= 0) return;
+  copy_int_kernel<<<grid_for(count), TB, 0, stream>>>(dst, dst_stride, src, src_stride, count);
+  qtx_check_launch("copy_int_kernel");
 }
 
 void launch_real_part(int64_t count, const cplx* src, double* dst, cudaStream_t stream) {

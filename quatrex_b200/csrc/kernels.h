@@ -97,6 +97,12 @@ void launch_obc_lesser_greater(int n, int64_t batch, MatView sigma_r, const doub
 // occ[e] = 1 / (1 + exp((E_e - mu) / kT))
 void launch_fermi(int64_t batch, const double* energies, double mu, double kt, double* occ, cudaStream_t stream);
 void launch_fill_int(int* p, int64_t count, int value, cudaStream_t stream);
+// dst[t * dst_stride] = src[t * src_stride], t < count.  The solver's small
+// fills and copies run as kernels, not cudaMemset / cudaMemcpy: those go to a
+// copy engine and wait there behind any large download a caller has in
+// flight on another stream.
+void launch_copy_int(int* dst, int64_t dst_stride, const int* src, int64_t src_stride, int64_t count,
+                     cudaStream_t stream);
 // abs_res[e] = ||x_ref - x||_F, rel_res[e] = abs_res[e] / ||x_ref||_F (contiguous n x n matrices)
 void launch_residual_norm(int n, int64_t batch, MatView x_ref, MatView x, double* abs_res, double* rel_res,
                           cudaStream_t stream);

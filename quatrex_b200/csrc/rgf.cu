@@ -498,10 +498,10 @@ void selected_inv_impl(qtx_ctx* ctx, const Btd& a, const void* const* obc_r, con
   cplx* T[7];
   for (int q = 0; q < 7; ++q) { T[q] = cur; cur += tmp; }
   Workspace ws{s, ne_max, bmax, cur};
-  QTX_CUDA_TRY(cudaMemsetAsync(ws.zero, 0, sizeof(cplx) * bmax * bmax, s));
+  launch_fill_int(reinterpret_cast<int*>(ws.zero), (int64_t)4 * bmax * bmax, 0, s);
   cur += (size_t)bmax * bmax;
   int* info = reinterpret_cast<int*>(cur);
-  QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * ne_max * nb, s));
+  launch_fill_int(info, ne_max * nb, 0, s);
 
   for (size_t q = 0; q + 1 < offs.size(); ++q) {
     const int64_t e0 = offs[q], ne = offs[q + 1] - offs[q];
@@ -589,7 +589,7 @@ std::vector<char> sigma_nonzero_blocks(const Btd& m, cudaStream_t s) {
   int64_t* d_slices = buf.as<int64_t>();
   int* d_flags = reinterpret_cast<int*>(d_slices + slices.size());
   QTX_CUDA_TRY(cudaMemcpyAsync(d_slices, slices.data(), sizeof(int64_t) * slices.size(), cudaMemcpyHostToDevice, s));
-  QTX_CUDA_TRY(cudaMemsetAsync(d_flags, 0, sizeof(int) * nk, s));
+  launch_fill_int(d_flags, nk, 0, s);
   for (int k0 = 0; k0 < nk; k0 += 65535)
     launch_block_nonzero(std::min(nk - k0, 65535), d_slices + 2 * k0, m.data, m.d->stack_stride, m.d->stack_size,
                          d_flags + k0, s);
@@ -634,10 +634,10 @@ void selected_solve_impl(qtx_ctx* ctx, const SolveArgs& A, cudaStream_t s) {
   cplx* T[NT];
   for (int q = 0; q < NT; ++q) { T[q] = cur; cur += tmp; }
   Workspace ws{s, ne_max, bmax, cur};
-  QTX_CUDA_TRY(cudaMemsetAsync(ws.zero, 0, sizeof(cplx) * bmax * bmax, s));
+  launch_fill_int(reinterpret_cast<int*>(ws.zero), (int64_t)4 * bmax * bmax, 0, s);
   cur += (size_t)bmax * bmax;
   int* info = reinterpret_cast<int*>(cur);
-  QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * ne_max * nb, s));
+  launch_fill_int(info, ne_max * nb, 0, s);
 
   const void* const* obc_r = A.obc ? A.obc->retarded : nullptr;
   const void* const* obc_l = A.obc ? A.obc->lesser : nullptr;
@@ -853,13 +853,13 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
   int* its = active + batch;
   int* num_active = its + batch;
   int* info = num_active + 2;  // zero pivots of the decimation inverses (sticky over the iterations)
-  QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * batch, s));
+  launch_fill_int(info, batch, 0, s);
   launch_axpby(n, n, batch, ONE, a_ii, ZERO, {}, eps, s);
   launch_axpby(n, n, batch, ONE, a_ii, ZERO, {}, eps_s, s);
   launch_axpby(n, n, batch, ONE, a_ji, ZERO, {}, alpha, s);
   launch_axpby(n, n, batch, ONE, a_ij, ZERO, {}, beta, s);
   launch_fill_int(active, batch, 1, s);
-  QTX_CUDA_TRY(cudaMemsetAsync(its, 0, sizeof(int) * batch, s));
+  launch_fill_int(its, batch, 0, s);
   bool converged = false;
   for (int it = 0; it < max_iter; ++it) {
     zinv(n, batch, eps, inv, info, active, s);
@@ -873,7 +873,7 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
     gemm(n, n, n, batch, ONE, t1, OP_N, beta, OP_N, t2, s, {}, ZERO, {}, ZERO, active);     // b inv b
     std::swap(alpha.ptr, t3.ptr);
     std::swap(beta.ptr, t2.ptr);
-    QTX_CUDA_TRY(cudaMemsetAsync(num_active, 0, sizeof(int), s));
+    launch_fill_int(num_active, 1, 0, s);
     launch_sr_norm_update(n, batch, alpha, beta, tol, active, its, num_active, s);
     if (read_status(ctx, num_active, 1, s).head == 0) {
       converged = true;
@@ -881,7 +881,7 @@ bool sancho_rubio_impl(qtx_ctx* ctx, int n, int64_t batch, MatView a_ii, MatView
     }
   }
   zinv(n, batch, eps_s, x, info, nullptr, s);
-  if (iterations) QTX_CUDA_TRY(cudaMemcpyAsync(iterations, its, sizeof(int) * batch, cudaMemcpyDeviceToDevice, s));
+  if (iterations) launch_copy_int(iterations, 1, its, 1, batch, s);
   read_info_or_throw(ctx, info, batch, s, "sancho_rubio (decimation block)");
   return converged;
 }
@@ -967,16 +967,12 @@ bool transport_contacts(qtx_ctx* ctx, const TransportWS& w, const qtx_transport_
   launch_assemble_diag(b, ne, h_diag, en, P.eta, V(w.T[0]), s);
   bool okl = sancho_rubio_impl(ctx, b, ne, V(w.T[0]), up(0), lo(0), P.sr_tol, P.sr_max_iterations, V(w.C[0]), w.its,
                                s);
-  if (O.sr_iterations)
-    QTX_CUDA_TRY(cudaMemcpy2DAsync(O.sr_iterations + 2 * e0, 2 * sizeof(int), w.its, sizeof(int), sizeof(int), ne,
-                                   cudaMemcpyDeviceToDevice, s));
+  if (O.sr_iterations) launch_copy_int(O.sr_iterations + 2 * e0, 2, w.its, 1, ne, s);
   // right: g_R = SR(A_nn, A_nm, A_mn)
   launch_assemble_diag(b, ne, h_diag + (int64_t)(nb - 1) * bb, en, P.eta, V(w.T[0]), s);
   bool okr = sancho_rubio_impl(ctx, b, ne, V(w.T[0]), lo(nb - 2), up(nb - 2), P.sr_tol, P.sr_max_iterations,
                                V(w.C[1]), w.its, s);
-  if (O.sr_iterations)
-    QTX_CUDA_TRY(cudaMemcpy2DAsync(O.sr_iterations + 2 * e0 + 1, 2 * sizeof(int), w.its, sizeof(int), sizeof(int),
-                                   ne, cudaMemcpyDeviceToDevice, s));
+  if (O.sr_iterations) launch_copy_int(O.sr_iterations + 2 * e0 + 1, 2, w.its, 1, ne, s);
   // Sigma^R_L = A_10 g_L A_01 ; Sigma^R_R = A_mn g_R A_nm
   gemm(b, b, b, ne, ONE, lo(0), OP_N, V(w.C[0]), OP_N, V(w.T[1]), s);
   gemm(b, b, b, ne, ONE, V(w.T[1]), OP_N, up(0), OP_N, V(w.C[2]), s);
@@ -1076,8 +1072,8 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     launch_keldysh_combine(b, ne, yl.view(n), yr.view(n), fl, fr, 1.0, true, T[6], bb, T[7], bb, s);
     launch_trace_product(b, b, ne, V(C[7]), tv(6), ONE, cr, false, s);
     launch_trace_product(b, b, ne, tv(7), V(C[5]), MONE, cr, true, s);
-    QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_right) + e0, cr, sizeof(cplx) * ne,
-                                 cudaMemcpyDeviceToDevice, s));
+    launch_axpby(1, 1, ne, ONE, MatView{cr, 1, 1}, ZERO, {}, MutView{reinterpret_cast<cplx*>(O.current_right) + e0, 1, 1},
+                 s);
   }
   cplx* corner = T[8];
   cplx* corner2 = T[9];
@@ -1131,8 +1127,8 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     launch_keldysh_combine(b, ne, yl.view(0), yr.view(0), fl, fr, 1.0, true, T[6], bb, T[7], bb, s);
     launch_trace_product(b, b, ne, V(C[6]), tv(6), ONE, cl, false, s);
     launch_trace_product(b, b, ne, tv(7), V(C[4]), MONE, cl, true, s);
-    QTX_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<cplx*>(O.current_left) + e0, cl, sizeof(cplx) * ne,
-                                 cudaMemcpyDeviceToDevice, s));
+    launch_axpby(1, 1, ne, ONE, MatView{cl, 1, 1}, ZERO, {}, MutView{reinterpret_cast<cplx*>(O.current_left) + e0, 1, 1},
+                 s);
   }
   if (O.transmission) {
     // T = Tr[Gamma_L G_0N Gamma_R G_0N^H]
@@ -1154,7 +1150,7 @@ void transport_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qtx_tran
   DevBuf mem(transport_ws_bytes(nb, b, ne_max), s);
   TransportWS w = carve_transport_ws(mem.as<void>(), nb, b, ne_max);
   transport_couplings(w, reinterpret_cast<const cplx*>(P.h_upper), s);
-  QTX_CUDA_TRY(cudaMemsetAsync(w.info, 0, sizeof(int) * nb * ne_max, s));
+  launch_fill_int(w.info, (int64_t)nb * ne_max, 0, s);
   for (size_t q = 0; q + 1 < offs.size(); ++q) {
     const int64_t e0 = offs[q], ne = offs[q + 1] - offs[q];
     all_converged = transport_contacts(ctx, w, P, O, e0, ne, s) && all_converged;
@@ -1200,7 +1196,7 @@ void transport_graph_impl(qtx_ctx* ctx, const qtx_transport_problem& P, const qt
   }
   TransportWS w = carve_transport_ws(g->mem, nb, b, ne);
   transport_couplings(w, reinterpret_cast<const cplx*>(P.h_upper), s);
-  QTX_CUDA_TRY(cudaMemsetAsync(w.info, 0, sizeof(int) * nb * ne, s));
+  launch_fill_int(w.info, (int64_t)nb * ne, 0, s);
   all_converged = transport_contacts(ctx, w, P, O, 0, ne, s) && all_converged;
   if (!g->exec) {
     std::lock_guard<std::mutex> capture_lock(g_capture_mutex);
@@ -1785,7 +1781,7 @@ qtx_status qtx_inv(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a, int64_
     if (n < 1 || batch < 0 || !a || !x) throw QtxError(QTX_E_INVAL, "qtx_inv: bad arguments");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     DevBuf info(sizeof(int) * std::max<int64_t>(batch, 1), s);
-    QTX_CUDA_TRY(cudaMemsetAsync(info.as<int>(), 0, sizeof(int) * std::max<int64_t>(batch, 1), s));
+    launch_fill_int(info.as<int>(), std::max<int64_t>(batch, 1), 0, s);
     zinv(n, batch, MatView{reinterpret_cast<const cplx*>(a), n, stride_a},
                 MutView{reinterpret_cast<cplx*>(x), n, stride_x}, info.as<int>(), nullptr, s);
     read_info_or_throw(ctx, info.as<int>(), batch, s, "qtx_inv");
@@ -2021,7 +2017,7 @@ qtx_status qtx_beyn_moments(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
     cplx* ops = buf.as<cplx>();
     cplx* q = ops + chunk * 2 * nq * nn;
     int* info = reinterpret_cast<int*>(q + 2 * chunk * nn);
-    QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * (size_t)(chunk * 2 * nq), s));
+    launch_fill_int(info, chunk * 2 * nq, 0, s);
     for (int64_t e0 = 0; e0 < batch; e0 += chunk) {
       const int64_t ne = std::min(chunk, batch - e0);
       MatView aii{reinterpret_cast<const cplx*>(a_ii) + e0 * stride_ii, n, stride_ii};
@@ -2066,7 +2062,7 @@ qtx_status qtx_spectral_surface(qtx_ctx* ctx, int32_t n, int64_t batch, const vo
     cplx* t2 = t1 + batch * nn;
     int* d_mask = reinterpret_cast<int*>(t2 + batch * nn);
     int* info = d_mask + batch * m0;
-    QTX_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int) * (size_t)batch, s));
+    launch_fill_int(info, batch, 0, s);
     MatView aii{reinterpret_cast<const cplx*>(a_ii), n, stride_ii};
     MatView aij{reinterpret_cast<const cplx*>(a_ij), n, stride_ij};
     MatView aji{reinterpret_cast<const cplx*>(a_ji), n, stride_ji};
@@ -2129,7 +2125,7 @@ qtx_status qtx_obc_fixed_point(qtx_ctx* ctx, int32_t n, int64_t batch, const voi
     gemm(n, n, n, batch, ONE, aji, OP_N, xv, OP_N, t0, s);
     gemm(n, n, n, batch, MONE, t0, OP_N, aij, OP_N, t1, s, aii, ONE);
     DevBuf info(sizeof(int) * batch, s);
-    QTX_CUDA_TRY(cudaMemsetAsync(info.as<int>(), 0, sizeof(int) * batch, s));
+    launch_fill_int(info.as<int>(), batch, 0, s);
     zinv(n, batch, t1, MutView{reinterpret_cast<cplx*>(x_ref), n, bb}, info.as<int>(), nullptr, s);
     if (abs_res && rel_res)
       launch_residual_norm(n, batch, MatView{reinterpret_cast<cplx*>(x_ref), n, bb}, xv, abs_res, rel_res, s);
