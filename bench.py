@@ -66,8 +66,15 @@ def _flops_per_energy(nb, b, sr_iterations):
       backward step: P1, P2, P4, G^R_ij, G^R_ji, corner chain,
                      4 for X_L, 2 for X_R, x_i                      = 13 per step
       contacts: Sigma^R 2 x 2; transmission: 2                      =  6
-      Sancho-Rubio: 7 per iteration + final inverse, per contact"""
-    units = 3 + 2 + (nb - 1) * (6 + 13) + 6 + sum(7 * it + 1 for it in sr_iterations)
+      Sancho-Rubio: 7 per iteration + final inverse, per contact
+    The products whose result is anti-Hermitian (X_L,0, X_R,n, the forward
+    W X_L W^H and the two backward X_L / X_R updates: 3 per block step) compute
+    the upper triangle of 64 x 64 tiles only: T (T + 1) / 2 of T^2 tiles,
+    T = ceil(b / 64); they count with that fraction."""
+    t = -(-b // 64)
+    frac = t * (t + 1) / 2 / (t * t)
+    skew = 2 + 3 * (nb - 1)
+    units = 3 + 2 + (nb - 1) * (6 + 13) + 6 + sum(7 * it + 1 for it in sr_iterations) - skew * (1 - frac)
     return 8.0 * b ** 3 * units
 
 
