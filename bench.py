@@ -66,15 +66,8 @@ def _flops_per_energy(nb, b, sr_iterations):
       backward step: P1, P2, P4, G^R_ij, G^R_ji, corner chain,
                      4 for X_L, 2 for X_R, x_i                      = 13 per step
       contacts: Sigma^R 2 x 2; transmission: 2                      =  6
-      Sancho-Rubio: 7 per iteration + final inverse, per contact
-    The products whose result is anti-Hermitian (X_L,0, X_R,n, the forward
-    W X_L W^H and the two backward X_L / X_R updates: 3 per block step) compute
-    the upper triangle of 64 x 64 tiles only: T (T + 1) / 2 of T^2 tiles,
-    T = ceil(b / 64); they count with that fraction."""
-    t = -(-b // 64)
-    frac = t * (t + 1) / 2 / (t * t)
-    skew = 2 + 3 * (nb - 1)
-    units = 3 + 2 + (nb - 1) * (6 + 13) + 6 + sum(7 * it + 1 for it in sr_iterations) - skew * (1 - frac)
+      Sancho-Rubio: 7 per iteration + final inverse, per contact"""
+    units = 3 + 2 + (nb - 1) * (6 + 13) + 6 + sum(7 * it + 1 for it in sr_iterations)
     return 8.0 * b ** 3 * units
 
 
@@ -389,6 +382,11 @@ def run_ours(args):
             line["mixed"] = mixed
         if world == 1 and not args.no_dropin_e2e:
             line["e2e_dropin"] = _e2e_dropin(args)
+        if world == 1 and not args.no_serve:
+            torch.cuda.empty_cache()
+            line["serve"] = {ln["precision"]: {k: v for k, v in ln.items()
+                                               if k not in ("metric", "impl", "workload", "precision")}
+                             for ln in serve_lines(args)}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -609,6 +607,13 @@ def run_uneven(args):
 def run_serve(args):
     """Serving: a seeded Poisson stream of requests (b in 32..256, nb 8..32,
     16-64 energies each), continuous batching, both precisions; p50/p99."""
+    for line in serve_lines(args):
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def serve_lines(args) -> list:
+    """The serving measurement of run_serve, one dict per precision."""
     import torch
 
     from quatrex_b200.autotune import Autotuner
@@ -623,6 +628,7 @@ def run_serve(args):
         ne = int(rng.integers(16, 65))
         reqs.append(make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=5000 + k))
     arrivals = poisson_arrivals(len(reqs), rate_hz=args.rate, seed=7)
+    lines = []
     for prec in ("fp64", "mixed"):
         tuner = Autotuner(cache_path=os.path.join(ROOT, "_build", "autotune.json"))
         server = TransportServer(slots=args.streams, precision=prec, tuner=tuner, group_small=not args.no_group)
@@ -651,16 +657,16 @@ def run_serve(args):
         # latencies of the timed requests only (the server's own statistics include the warm-up)
         lat = np.array([r["latency_s"] for r in results])
         solves = int(sum(len(d.energies) for d in reqs))
-        print(json.dumps({"metric": "rgf_energy_solves_per_s", "impl": "ours", "workload": "serve",
-                          "precision": prec, "value": solves / dt, "unit": "solves/s", "seconds": dt,
-                          "requests": len(results), "p50_latency_s": float(np.percentile(lat, 50)),
-                          "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
-                          "peak_concurrency": st["peak_concurrency"], "arrival_rate_hz": args.rate,
-                          "slots": args.streams, "server": "native qtx_server (C++ workers, one stream each)",
-                          "grouped_small": not args.no_group,
-                          "grouped_launches": st["grouped_launches"], "grouped_requests": st["grouped_requests"]}),
-              flush=True)
-    return 0
+        lines.append({"metric": "rgf_energy_solves_per_s", "impl": "ours", "workload": "serve",
+                      "precision": prec, "value": solves / dt, "unit": "solves/s", "seconds": dt,
+                      "requests": len(results), "p50_latency_s": float(np.percentile(lat, 50)),
+                      "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
+                      "peak_concurrency": st["peak_concurrency"], "arrival_rate_hz": args.rate,
+                      "slots": args.streams, "server": "native qtx_server (C++ workers, one stream each)",
+                      "grouped_small": not args.no_group,
+                      "grouped_launches": st["grouped_launches"], "grouped_requests": st["grouped_requests"],
+                      "requests_drawn": "seeded: b = 2^U{5..8}, nb U[8, 32], 16-64 energies"})
+    return lines
 
 
 def run_dropin(args):
@@ -751,6 +757,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the precision-form sub-line")
     ap.add_argument("--no-dropin-e2e", action="store_true", help="skip the plugin-call end-to-end key")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving (p50/p99) key")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -33,11 +33,6 @@ struct GemmCall {
   const int* active = nullptr;
   // optional per-batch-entry diagonal shift: D[r][r] += diag_shift[e] (e.g. (E + i eta) I)
   const cplx* diag_shift = nullptr;
-  // the caller guarantees an anti-Hermitian result (D = -D^H; m == n, C and C2
-  // anti-Hermitian, alpha, beta, gamma real): the FP64 kernel computes the
-  // upper tile triangle only and mirrors it (the mixed-precision kernel
-  // ignores the flag and computes every tile)
-  bool skew_out = false;
 };
 void launch_zgemm(const GemmCall& g, cudaStream_t stream);
 

@@ -409,26 +409,6 @@ void gemm(int m, int n, int k, int64_t batch, cplx alpha, MatView a, int op_a, M
   else launch_zgemm(g, s);
 }
 
-// A product whose result is anti-Hermitian (X = W Y W^H with Y = -Y^H, and
-// sums of such terms): the FP64 kernel computes the tiles on and above the
-// tile diagonal only and mirrors them.  Timed with the flops it executes.
-void gemm_skew(int n, int k, int64_t batch, cplx alpha, MatView a, int op_a, MatView b, int op_b, MutView d,
-               cudaStream_t s, MatView c = MatView{}, cplx beta = ZERO, MatView c2 = MatView{}, cplx gamma = ZERO,
-               int precision = QTX_PREC_FP64) {
-  GemmCall g;
-  g.m = n; g.n = n; g.k = k; g.batch = batch;
-  g.a = a; g.op_a = op_a; g.b = b; g.op_b = op_b;
-  g.c = c; g.beta = beta; g.c2 = c2; g.gamma = gamma;
-  g.d = d; g.alpha = alpha;
-  const bool mixed = precision == QTX_PREC_MIXED && mixed_supported(g);
-  g.skew_out = !mixed;
-  const double t = (double)((n + 63) / 64);
-  const double frac = g.skew_out ? (t * (t + 1) / 2) / (t * t) : 1.0;
-  TimedScope ts(0, 8.0 * n * n * (double)k * batch * frac, s);
-  if (mixed) launch_zgemm_mixed(g, s);
-  else launch_zgemm(g, s);
-}
-
 // Block inverse with timing (8 n^3 algorithmic flops per matrix: getrf + getri).
 void zinv(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t s) {
   TimedScope ts(1, 8.0 * n * (double)n * n * batch, s);
@@ -1063,7 +1043,7 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
   gemm(b, b, 0, ne, ONE, tv(0), OP_N, tv(0), OP_N, tv(1), s, hd(0), MONE, obc_r(0), MONE, nullptr, shift);
   zinv(b, ne, tv(1), xr.view(0), info, nullptr, s);
   gemm(b, b, b, ne, I1, xr.view(0), OP_N, V(C[8]), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-  gemm_skew(b, b, ne, ONE, tv(2), OP_N, xr.view(0), OP_C, yl.view(0), s, {}, ZERO, {}, ZERO, prec);
+  gemm(b, b, b, ne, ONE, tv(2), OP_N, xr.view(0), OP_C, yl.view(0), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
   // ---- forward sweep
   for (int i = 0; i + 1 < nb; ++i) {
     const int j = i + 1;
@@ -1075,12 +1055,12 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     // (no source past block 0)
     gemm(b, b, b, ne, ONE, xr.view(j), OP_N, lo(i), OP_N, tv(3), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
     gemm(b, b, b, ne, ONE, tv(3), OP_N, yl.view(i), OP_N, tv(4), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    gemm_skew(b, b, ne, ONE, tv(4), OP_N, tv(3), OP_C, yl.view(j), s, {}, ZERO, {}, ZERO, prec);
+    gemm(b, b, b, ne, ONE, tv(4), OP_N, tv(3), OP_C, yl.view(j), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
   }
   // ---- last block: X_R,n = x_n (i Gamma_R) x_n^H, outputs, corner chain start
   const int n = nb - 1;
   gemm(b, b, b, ne, I1, xr.view(n), OP_N, V(C[9]), OP_N, tv(2), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-  gemm_skew(b, b, ne, ONE, tv(2), OP_N, xr.view(n), OP_C, yr.view(n), s, {}, ZERO, {}, ZERO, prec);
+  gemm(b, b, b, ne, ONE, tv(2), OP_N, xr.view(n), OP_C, yr.view(n), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
   launch_keldysh_combine(b, ne, yl.view(n), yr.view(n), fl, fr, 1.0, true, out_ptr(O.gl_diag, nb, n), nb * bb,
                          out_ptr(O.gg_diag, nb, n), nb * bb, s);
   if (O.gr_diag) launch_axpby(b, b, ne, ONE, xr.view(n), ZERO, {}, out_at(O.gr_diag, nb, n), s);
@@ -1124,10 +1104,11 @@ void transport_sweep(TransportWS w, const qtx_transport_problem& P, const qtx_tr
     gemm(b, b, b, ne, ONE, tv(0), OP_N, yl.view(j), OP_N, tv(6), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
     if (uppers)
       gemm(b, b, b, ne, MONE, yl.view(i), OP_N, tv(1), OP_C, tv(7), s, tv(6), MONE, {}, ZERO, nullptr, nullptr, prec);
-    gemm_skew(b, b, ne, ONE, tv(6), OP_N, tv(0), OP_C, yl.view(i), s, yl.view(i), ONE, tv(5), ONE, prec);
+    gemm(b, b, b, ne, ONE, tv(6), OP_N, tv(0), OP_C, yl.view(i), s, yl.view(i), ONE, tv(5), ONE, nullptr, nullptr,
+         prec);
     // X_R (zero in the forward sweep): t2 = P1 X_j ; X_ij = -t2 ; X_i = t2 P1^H
     gemm(b, b, b, ne, ONE, tv(0), OP_N, yr.view(j), OP_N, tv(5), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
-    gemm_skew(b, b, ne, ONE, tv(5), OP_N, tv(0), OP_C, yr.view(i), s, {}, ZERO, {}, ZERO, prec);
+    gemm(b, b, b, ne, ONE, tv(5), OP_N, tv(0), OP_C, yr.view(i), s, {}, ZERO, {}, ZERO, nullptr, nullptr, prec);
     if (uppers)
       launch_keldysh_combine(b, ne, tv(7), tv(5), fl, fr, -1.0, false, out_ptr(O.gl_upper, nb - 1, i),
                              (nb - 1) * bb, out_ptr(O.gg_upper, nb - 1, i), (nb - 1) * bb, s);

@@ -50,11 +50,6 @@ struct Params {
   cplx* d; int64_t ldd, sd; cplx alpha;
   const int* active;
   const cplx* diag_shift;
-  // anti-Hermitian result (D^H = -D, m == n): only the tiles on and above the
-  // tile diagonal are computed (blockIdx.x enumerates them row by row); a tile
-  // above the diagonal also writes its mirror -conj(v)
-  int skew;
-  int tiles;  // tiles per side when skew
 };
 
 // Load one K-slice of op(A) (BM x BK) into shared memory.
@@ -123,19 +118,7 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_dmma_kernel(Params p) {
   const int warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t = lane & 3;
   const int wm0 = (warp >> 1) * 32, wn0 = (warp & 1) * 32;
-  int tm = blockIdx.y, tn = blockIdx.x;
-  if (p.skew) {
-    // upper-triangular tile tm <= tn from the linear index blockIdx.x
-    int rem = blockIdx.x;
-    tm = 0;
-    while (rem >= p.tiles - tm) {
-      rem -= p.tiles - tm;
-      ++tm;
-    }
-    tn = tm + rem;
-  }
-  const bool mirror = p.skew && tn > tm;
-  const int m0 = tm * BM, n0 = tn * BN;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   const int ktiles = (p.k + BK - 1) / BK;
 
   for (int64_t e = blockIdx.z; e < p.batch; e += gridDim.z) {
@@ -224,7 +207,6 @@ __global__ void __launch_bounds__(THREADS, 2) zgemm_dmma_kernel(Params p) {
             if (c2) v = cfma(p.gamma, c2[(int64_t)row * p.ldc2 + col], v);
             if (p.diag_shift && row == col) v = cadd(v, p.diag_shift[e]);
             d[(int64_t)row * p.ldd + col] = v;
-            if (mirror) d[(int64_t)col * p.ldd + row] = cmk(-v.x, v.y);
           }
         }
       }
@@ -237,7 +219,6 @@ void launch_t(const Params& p, cudaStream_t stream) {
   // opt-in to the large shared-memory carve-out (per device)
   qtx_opt_in_smem((const void*)zgemm_dmma_kernel<OPA, OPB>, SMEM_BYTES);
   dim3 grid(ceil_div_u(p.n, BN), ceil_div_u(p.m, BM), (unsigned)(p.batch < 65535 ? p.batch : 65535));
-  if (p.skew) grid = dim3((unsigned)(p.tiles * (p.tiles + 1) / 2), 1, grid.z);
   zgemm_dmma_kernel<OPA, OPB><<<grid, THREADS, SMEM_BYTES, stream>>>(p);
 }
 
@@ -254,8 +235,6 @@ void launch_zgemm(const GemmCall& g, cudaStream_t stream) {
   p.d = g.d.ptr; p.ldd = g.d.ld; p.sd = g.d.stride; p.alpha = g.alpha;
   p.active = g.active;
   p.diag_shift = g.diag_shift;
-  p.skew = g.skew_out && g.m == g.n && !g.diag_shift ? 1 : 0;
-  p.tiles = (int)ceil_div_u(g.n, BN);
   if (g.op_a == OP_N && g.op_b == OP_N) launch_t<OP_N, OP_N>(p, stream);
   else if (g.op_a == OP_N && g.op_b == OP_C) launch_t<OP_N, OP_C>(p, stream);
   else if (g.op_a == OP_C && g.op_b == OP_N) launch_t<OP_C, OP_N>(p, stream);

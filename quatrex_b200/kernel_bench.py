@@ -10,7 +10,10 @@ transport solve (one persistent launch for every energy of several seeded
 devices of one block size, nb uniform in [8, 128], 64-512 energies; with
 ``--instances 1`` the single device nb=22 / 467 energies or, at b = 32,
 nb=12 / 456 energies) against the layered solve of the same devices one after
-the other, each after one warm-up call, with device-resident inputs.  The same invocations are the targets of the ncu captures
+the other, each after one warm-up call, with device-resident inputs.
+``rgfdist --b 256 --nb 64 --energies 4 --partitions 2,4,8`` times the
+selected solve of one seeded device by RGF and by RGFDist (partitions on
+their own CUDA streams).  The same invocations are the targets of the ncu captures
 summarised under profiles/.  Inputs are seeded, in HBM, and larger than L2 for
 the default shapes (3 x 128 MiB operands at b = 256).
 """
@@ -168,9 +171,63 @@ def probe_fp64_peak() -> dict:
     return {"kernel": "fp64_peak_probe", **out}
 
 
+def bench_rgfdist(b: int, nb: int, energies: int, partitions: list[int], repeats: int = 2) -> dict:
+    """Selected solve of one seeded transport device (device-resident
+    DSDBCOO operands, contact blocks, zero interior self-energies) by RGF and
+    by RGFDist with each partition count; wall time per call after a
+    warm-up call, and the largest per-block difference of G^< against RGF."""
+    import time
+
+    from quatrex_b200.datastructures import DSDBCOO
+    from quatrex_b200.greens_function_solver import RGF, OBCBlocks
+    from quatrex_b200.obc import SanchoRubio, contact_self_energies
+    from quatrex_b200.rgf_dist import RGFDist
+    from quatrex_b200.workloads import make_device
+
+    dev = make_device(num_blocks=nb, block_size=b, num_energies=energies, seed=3)
+    d, u, lo = dev.system_blocks()
+    e = dev.energies
+    sr = SanchoRubio(dev.sr_max_iter, dev.sr_tol)
+    f_l = 1.0 / (1.0 + np.exp((e - dev.mu_left) / dev.kt))
+    f_r = 1.0 / (1.0 + np.exp((e - dev.mu_right) / dev.kt))
+    left = contact_self_energies(sr(d[0], u[0], lo[0]), lo[0], u[0], f_l)
+    right = contact_self_energies(sr(d[-1], lo[-1], u[-1]), u[-1], lo[-1], f_r)
+    A = DSDBCOO.from_blocks(d, u, lo, device="cuda")
+    Z = DSDBCOO.zeros_like(A)
+    ob = OBCBlocks(nb)
+    ob.retarded[0], ob.lesser[0], ob.greater[0] = (torch.from_numpy(x).cuda() for x in left)
+    ob.retarded[-1], ob.lesser[-1], ob.greater[-1] = (torch.from_numpy(x).cuda() for x in right)
+    outs = [DSDBCOO.zeros_like(A) for _ in range(3)]
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(repeats):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / repeats
+
+    rgf = RGF(max_batch_size=energies)
+    t_rgf = timed(lambda: rgf.selected_solve(A, Z, Z, obc_blocks=ob, out=outs, return_retarded=True))
+    ref = outs[0].data.clone()
+    res = {"kernel": "rgf_vs_rgfdist", "b": b, "nb": nb, "energies": energies, "rgf_s": t_rgf}
+    for p in partitions:
+        solver = RGFDist(max_batch_size=energies, num_partitions=p)
+        t = timed(lambda: solver.selected_solve(A, Z, Z, outs, ob, return_retarded=True))
+        diff = float((outs[0].data - ref).abs().max() / ref.abs().max())
+        res[f"rgfdist_p{p}_s"] = t
+        res[f"rgfdist_p{p}_speedup"] = t_rgf / t
+        res[f"rgfdist_p{p}_max_rel_diff_gl"] = diff
+    return res
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="fixed-shape kernel timing")
-    ap.add_argument("kernel", choices=["gemm", "gemm_h", "inv", "sr", "fp64peak", "grouped"])
+    ap.add_argument("kernel", choices=["gemm", "gemm_h", "inv", "sr", "fp64peak", "grouped", "rgfdist"])
+    ap.add_argument("--nb", type=int, default=64)
+    ap.add_argument("--energies", type=int, default=4)
+    ap.add_argument("--partitions", type=str, default="2,4,8")
     ap.add_argument("--instances", type=int, default=6)
     ap.add_argument("--b", type=int, default=256)
     ap.add_argument("--batch", type=int, default=128)
@@ -188,6 +245,8 @@ def main(argv=None) -> int:
         r = bench_inv(args.b, args.batch, args.launches)
     elif args.kernel == "grouped":
         r = bench_grouped(args.b, args.instances)
+    elif args.kernel == "rgfdist":
+        r = bench_rgfdist(args.b, args.nb, args.energies, [int(x) for x in args.partitions.split(",")])
     else:
         r = bench_sr(args.b, args.batch, args.launches)
     print(json.dumps(r), flush=True)

@@ -29,13 +29,12 @@ def test_reference_arm_json_line():
     assert "nb=64 b=256" in line["config"]["workload"]
 
 
-@pytest.mark.parametrize("nb,its,units", [(64, (22, 22), 3 + 2 + 63 * 19 + 6 + 2 * (7 * 22 + 1) - (2 + 3 * 63) * 0.375),
-                                          (2, (1, 3), 3 + 2 + 19 + 6 + 8 + 22 - 5 * 0.375)])
+@pytest.mark.parametrize("nb,its,units", [(64, (22, 22), 3 + 2 + 63 * 19 + 6 + 2 * (7 * 22 + 1)),
+                                          (2, (1, 3), 3 + 2 + 19 + 6 + 8 + 22)])
 def test_flop_accounting(nb, its, units):
     """8 b^3 per block product or inverse; 19 per block step with every output
     (6 forward, 13 backward), 5 for the end blocks, 6 for contacts and
-    transmission, 7 per Sancho-Rubio iteration + 1 per lead; the 2 + 3 (nb - 1)
-    anti-Hermitian products at 10 of 16 tiles (b = 256)."""
+    transmission, 7 per Sancho-Rubio iteration + 1 per lead."""
     import bench
 
     assert bench._flops_per_energy(nb, 256, list(its)) == 8.0 * 256 ** 3 * units
