@@ -69,7 +69,8 @@ def test_zgemm_broadcast_operand():
     assert _rel(d, a @ b) < 1e-13
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 8, 16, 24, 31, 48, 64, 96, 100, 128, 200, 256, 257, 300, 512])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 8, 16, 24, 31, 48, 64, 96, 100, 128, 129, 161, 200, 250, 255, 256, 257, 300,
+                               512])
 def test_inverse_matches_lapack(n):
     rng = np.random.default_rng(n)
     batch = 5
@@ -98,6 +99,45 @@ def test_inverse_needs_pivoting():
     ctx = _lib.context(0)
     _lib.check(lib.qtx_inv(ctx, 3, 1, ta.data_ptr(), 9, x.data_ptr(), 9, 0), ctx, "inv")
     assert _rel(x, np.linalg.inv(a)) < 1e-14
+
+
+@pytest.mark.parametrize("n", [64, 200, 256])
+def test_inverse_pivoting_large_blocks(n):
+    """Row-permuted, well-conditioned blocks with a zero diagonal: every
+    column needs a row interchange, across panels (the 129-256 kernel keeps
+    the next panel's elimination under the current panel's update)."""
+    rng = np.random.default_rng(n + 1)
+    batch = 6
+    base = rng.standard_normal((batch, n, n)) + 1j * rng.standard_normal((batch, n, n))
+    base += 2 * np.sqrt(n) * np.eye(n)
+    perm = np.roll(np.arange(n), n // 3 + 1)
+    a = np.ascontiguousarray(base[:, perm, :])
+    assert np.all(np.abs(np.diagonal(a, axis1=1, axis2=2)) < 2 * np.sqrt(n) - 1e-9)
+    ta = torch.from_numpy(a).cuda()
+    x = torch.empty_like(ta)
+    lib = _lib.load()
+    ctx = _lib.context(0)
+    _lib.check(lib.qtx_inv(ctx, n, batch, ta.data_ptr(), n * n, x.data_ptr(), n * n, 0), ctx, "inv")
+    assert _rel(x, np.linalg.inv(a)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [4, 200])
+def test_inverse_singular_block_flags_its_energy(n):
+    """A block with a zero column in the middle of a batch returns
+    QTX_E_SINGULAR; the other blocks are still inverted correctly."""
+    rng = np.random.default_rng(7)
+    a = rng.standard_normal((3, n, n)) + 1j * rng.standard_normal((3, n, n)) + np.sqrt(n) * np.eye(n)
+    a[1, :, n // 2] = 0
+    ta = torch.from_numpy(a).cuda()
+    x = torch.empty_like(ta)
+    lib = _lib.load()
+    ctx = _lib.context(0)
+    st = lib.qtx_inv(ctx, n, 3, ta.data_ptr(), n * n, x.data_ptr(), n * n, 0)
+    assert st == _lib.QTX_E_SINGULAR
+    torch.cuda.synchronize()
+    xc = x.cpu().numpy()
+    for e in (0, 2):
+        assert _rel(xc[e], np.linalg.inv(a[e])) < 1e-10
 
 
 def test_inverse_singular_block_raises():
