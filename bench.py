@@ -618,18 +618,26 @@ def serve_lines(args) -> list:
 
     from quatrex_b200.autotune import Autotuner
     from quatrex_b200.serving import TransportServer, poisson_arrivals
-    from quatrex_b200.workloads import make_device
+    from quatrex_b200.workloads import make_device, uneven_instances
 
-    rng = np.random.default_rng(99)
     reqs = []
-    for k in range(args.requests):
-        b = int(2 ** rng.integers(5, 9))
-        nb = int(rng.integers(8, 33))
-        ne = int(rng.integers(16, 65))
-        reqs.append(make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=5000 + k))
+    if getattr(args, "serve_sizes", "small") == "uneven":
+        # the size distribution of the uneven-instance batch (b up to 512, nb up to 128, 64-512 energies)
+        for k, kw in enumerate(uneven_instances(args.requests, seed=99)):
+            reqs.append(make_device(**kw))
+        drawn = "seeded: the uneven-batch distribution, b = 2^U{5..9}, nb U[8, 128], 64-512 energies"
+    else:
+        rng = np.random.default_rng(99)
+        for k in range(args.requests):
+            b = int(2 ** rng.integers(5, 9))
+            nb = int(rng.integers(8, 33))
+            ne = int(rng.integers(16, 65))
+            reqs.append(make_device(num_blocks=nb, block_size=b, num_energies=ne, seed=5000 + k))
+        drawn = "seeded: b = 2^U{5..8}, nb U[8, 32], 16-64 energies"
     arrivals = poisson_arrivals(len(reqs), rate_hz=args.rate, seed=7)
     lines = []
-    for prec in ("fp64", "mixed"):
+    precs = ("fp64", "mixed") if getattr(args, "serve_precision", "both") == "both" else (args.serve_precision,)
+    for prec in precs:
         tuner = Autotuner(cache_path=os.path.join(ROOT, "_build", "autotune.json"))
         server = TransportServer(slots=args.streams, precision=prec, tuner=tuner, group_small=not args.no_group)
         try:
@@ -665,7 +673,7 @@ def serve_lines(args) -> list:
                       "slots": args.streams, "server": "native qtx_server (C++ workers, one stream each)",
                       "grouped_small": not args.no_group,
                       "grouped_launches": st["grouped_launches"], "grouped_requests": st["grouped_requests"],
-                      "requests_drawn": "seeded: b = 2^U{5..8}, nb U[8, 32], 16-64 energies"})
+                      "requests_drawn": drawn})
     return lines
 
 
@@ -746,6 +754,9 @@ def main():
     ap.add_argument("--streams", type=int, default=4, help="uneven/serve: concurrent streams (slots)")
     ap.add_argument("--requests", type=int, default=48, help="serve workload: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serve workload: Poisson arrival rate (1/s)")
+    ap.add_argument("--serve-sizes", choices=["small", "uneven"], default="small",
+                    help="serve workload: request sizes (small: b <= 256, nb <= 32; uneven: the uneven-batch draw)")
+    ap.add_argument("--serve-precision", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--uneven-precision", choices=["both", "fp64", "mixed"], default="both")
     ap.add_argument("--no-group", action="store_true",
                     help="uneven/serve: solve b <= 64 instances (requests) one by one instead of grouped launches")

@@ -1,4 +1,4 @@
-"""Partitioned (nested-dissection) RGF on one GPU: ``RGFDist``.
+"""Partitioned (nested-dissection) RGF: ``RGFDist``.
 
 Mirrors ``qttools.greens_function_solver.RGFDist``
 (``src/qttools/greens_function_solver/rgf_dist.py:16-384``, algorithm in
@@ -8,11 +8,14 @@ upwards, the middle ones with the permuted Schur complement that keeps their
 first block coupled through buffer blocks; the 2 (P - 1) partition-boundary
 blocks form a reduced block-tridiagonal system that is solved by RGF; the
 results are mapped back and every partition finishes with its own selected
-inversion.  Upstream gives each partition its own MPI rank; here the
-partitions are independent chains of block operations on their own CUDA
-streams of one device, so a long device with few energies keeps the GPU busy
-(P chains of batched products in flight instead of one), and the reduced
-system is the only sequential part.
+inversion.  Upstream gives each partition its own MPI rank.  Here the
+partitions are either independent chains of block operations on their own
+CUDA streams of one device (a long device with few energies keeps the GPU
+busy with P chains of batched products in flight, and the reduced system is
+the only sequential part), or, given a ``torch.distributed`` process group,
+one partition per rank: the two boundary slots of every partition are
+all-gathered (one collective per stack batch; NCCL over NVLink between GPUs)
+and every rank solves the small reduced system itself, as upstream does.
 
 Every block operation runs in ``libqtxrgf``: products and their
 accumulations on the DMMA GEMM (``qtx_zgemm``, with its C epilogue), block
@@ -20,7 +23,8 @@ inverses on the batched Gauss-Jordan (``qtx_inv``), sums and conjugate
 transposes on ``qtx_block_combine``.  There is no CPU path.
 
 Differences from upstream, by design: the partition count is a constructor
-argument (upstream takes it from the MPI block communicator); upstream's
+argument or the size of the given process group (upstream takes it from its
+MPI block communicator); upstream's
 ``permuted_selinv`` forms its product ``tmp2`` only when it solves for G^< /
 G^> (``_serinv.py:1403``) yet uses it for G^R too (``:1515``), so upstream
 ``selected_inv`` fails with three or more partitions -- here it is formed in
@@ -183,11 +187,19 @@ class RGFDist(GFSolver):
     return_retarded=False)`` take upstream's arguments (``out`` required) and
     write ``out`` in place."""
 
-    def __init__(self, max_batch_size: int = 100, num_partitions: int = 2) -> None:
-        if num_partitions < 2:
+    def __init__(self, max_batch_size: int = 100, num_partitions: int = 2, comm=None) -> None:
+        """``comm``: a ``torch.distributed`` process group; then every rank
+        solves one partition (the partition count is the group size, as
+        upstream takes it from its block communicator), every rank passes the
+        same full operands, the reduced system is all-gathered (NCCL: device
+        memory; gloo: through host memory) and solved on every rank, and each
+        rank writes the blocks of its own partition (its block rows and the
+        coupling to the next partition) into ``out``."""
+        if comm is None and num_partitions < 2:
             raise ValueError("RGFDist needs at least two partitions (use RGF for one)")
         self.max_batch_size = max_batch_size
         self.num_partitions = num_partitions
+        self.comm = comm
 
     # -- the shared driver ---------------------------------------------------
     def _run(self, a, sl, sg, outs, obc_blocks, ss: bool, return_retarded: bool):
@@ -195,8 +207,20 @@ class RGFDist(GFSolver):
             raise RuntimeError("quatrex_b200 needs a CUDA device (B200, sm_100a); there is no CPU path")
         dev = torch.cuda.current_device()
         nb = a.num_blocks if hasattr(a, "num_blocks") else len(a.block_sizes)
-        bounds = partition_bounds(nb, self.num_partitions)
-        P = len(bounds)
+        if self.comm is not None:
+            import torch.distributed as dist
+
+            rank, P = dist.get_rank(self.comm), dist.get_world_size(self.comm)
+            if P < 2:
+                raise ValueError("RGFDist needs at least two partitions (use RGF for one)")
+            bounds = partition_bounds(nb, P)
+            mine = [rank]
+        else:
+            bounds = partition_bounds(nb, self.num_partitions)
+            P = len(bounds)
+            mine = list(range(P))
+        shapes = _slot_shapes(np.asarray(a.block_sizes), bounds)
+        bmax = int(np.max(np.asarray(a.block_sizes)))
         if obc_blocks is None:
             obc_blocks = OBCBlocks(num_blocks=nb)
         stack = tuple(np.shape(a.data)[:-1])
@@ -212,7 +236,7 @@ class RGFDist(GFSolver):
             td = (t if t is not None else torch.as_tensor(np.asarray(m.data)).to(f"cuda:{dev}"))
             out_dev.append((m, layout_of(m), td.reshape(-1, td.shape[-1]), t is None))
         main = torch.cuda.current_stream(dev)
-        streams = [torch.cuda.Stream(device=dev) for _ in range(P)]
+        streams = {p: torch.cuda.Stream(device=dev) for p in mine}
         A_all = _Operand(a, dev)
         SL_all = _Operand(sl, dev) if ss else None
         SG_all = _Operand(sg, dev) if ss else None
@@ -233,30 +257,38 @@ class RGFDist(GFSolver):
 
             ev0 = torch.cuda.Event()
             ev0.record(main)
-            parts, states = [], []
-            for p_idx, (s, e) in enumerate(bounds):
+            parts = {}
+            for p_idx in mine:
+                s, e = bounds[p_idx]
                 streams[p_idx].wait_event(ev0)
                 part = _Part(p_idx, P, s, e, A, SL, SG, obc, _Ops(dev, streams[p_idx]), ss)
                 with torch.cuda.stream(streams[p_idx]):
                     part.schur()
-                parts.append(part)
+                parts[p_idx] = part
             # reduced system on the main stream once every partition is eliminated
-            for st_ in streams:
+            for st_ in streams.values():
                 main.wait_stream(st_)
             ops = _Ops(dev, main)
             with torch.cuda.stream(main):
-                red = _gather_reduced(parts, ss)
+                if self.comm is None:
+                    red = _gather_reduced([parts[p] for p in range(P)], ss)
+                else:
+                    part = parts[mine[0]]
+                    buf = _pack_slots(_local_slots(part, ss), ss, e1 - e0, bmax, main.device)
+                    red, neg_h = _reduced_from_gathered(_exchange_slots(buf, self.comm), shapes, P, ss)
+                    for kind, i in neg_h:
+                        red[kind][i] = ops.comb(red[kind][i], alpha=-1.0, op_x=_C)
                 _reduced_solve(ops, red, ss)
                 ev1 = torch.cuda.Event()
                 ev1.record(main)
             blocks_out = []
-            for p_idx, part in enumerate(parts):
+            for p_idx, part in parts.items():
                 streams[p_idx].wait_event(ev1)
                 with torch.cuda.stream(streams[p_idx]):
                     part.map_back(red)
                     part.selinv()
                 blocks_out.append(part.out)
-            for st_ in streams:
+            for st_ in streams.values():
                 main.wait_stream(st_)
             # write the blocks of this stack batch into the outputs
             with torch.cuda.stream(main):
@@ -559,32 +591,155 @@ class _Part:
             self.out[c][(s, 1 + s)] = o.comb(self.xb[c][0], alpha=-1.0, op_x=_C)
 
 
-def _gather_reduced(parts, ss):
-    """The reduced system of the partition boundary blocks (_serinv.py:373-442)."""
-    P = len(parts)
+# -- the reduced system: slots, their order, and the exchange between ranks --
+#
+# Every partition p contributes the blocks of its first block row (slot 0,
+# p > 0) and of its last block row (slot 1, p < P - 1) to the reduced system
+# of the 2 (P - 1) partition-boundary blocks (_serinv.py:373-442; upstream
+# all-gathers two slots per rank, :258-330).  Kinds per slot: the retarded
+# diagonal "xr", the couplings "up" / "lo" and, for a selected solve, the
+# Keldysh diagonals "xl" / "xg" and their upper couplings "xl_up" / "xg_up".
+# Slot 0 of a middle partition couples its first block to its own last block
+# through the buffer blocks; its "x?_up" entry is -(buffer)^H.
+
+_KINDS_R = ("xr", "up", "lo")
+_KINDS_SS = ("xr", "up", "lo", "xl", "xl_up", "xg", "xg_up")
+
+
+def _kinds(ss):
+    return _KINDS_SS if ss else _KINDS_R
+
+
+def _reduced_order(P: int, ss: bool) -> list[tuple[int, int, str]]:
+    """(partition, slot, kind) of every reduced-system entry, in the order of
+    the reduced block lists: per kind, partition by partition, slot 0 before
+    slot 1."""
+    order = []
     kel = "lg" if ss else ""
+    for p in range(P):
+        if p > 0:
+            order.append((p, 0, "xr"))
+            order += [(p, 0, "x" + c) for c in kel]
+            if p < P - 1:
+                order += [(p, 0, "lo"), (p, 0, "up")]
+                order += [(p, 0, "x" + c + "_up") for c in kel]
+        if p < P - 1:
+            order.append((p, 1, "xr"))
+            order += [(p, 1, "x" + c) for c in kel]
+            order += [(p, 1, "up"), (p, 1, "lo")]
+            order += [(p, 1, "x" + c + "_up") for c in kel]
+    return order
+
+
+def _slot_shapes(block_sizes, bounds) -> dict:
+    """(rows, cols) of every (partition, slot, kind) entry as exchanged
+    (f, l: sizes of the partition's first and last block, nxt: the next
+    partition's first block)."""
+    bs = [int(b) for b in block_sizes]
+    shapes = {}
+    for p, (s, e) in enumerate(bounds):
+        f, l = bs[s], bs[e - 1]
+        nxt = bs[e] if e < len(bs) else 0
+        for kind in _KINDS_SS:
+            if kind in ("xr", "xl", "xg"):
+                shapes[(p, 0, kind)], shapes[(p, 1, kind)] = (f, f), (l, l)
+            elif kind == "lo":
+                shapes[(p, 0, kind)], shapes[(p, 1, kind)] = (l, f), (nxt, l)
+            elif kind == "up":
+                shapes[(p, 0, kind)], shapes[(p, 1, kind)] = (f, l), (l, nxt)
+            else:  # xl_up, xg_up: slot 0 holds the raw buffer block (l, f), its entry is -(.)^H
+                shapes[(p, 0, kind)], shapes[(p, 1, kind)] = (l, f), (l, nxt)
+    return shapes
+
+
+def _local_slots(part, ss) -> dict:
+    """The reduced-system entries of one eliminated partition, keyed by
+    (slot, kind); slot 0's "x?_up" is the raw buffer block (negated and
+    conjugate-transposed after the exchange)."""
+    p, P, n = part.idx, part.P, part.n
+    kel = "lg" if ss else ""
+    out = {}
+    if p > 0:
+        out[(0, "xr")] = part.xr[0]
+        for c in kel:
+            out[(0, "x" + c)] = part.x[c][0]
+        if p < P - 1:
+            out[(0, "lo")] = part.bu[n - 2]
+            out[(0, "up")] = part.bl[n - 2]
+            for c in kel:
+                out[(0, "x" + c + "_up")] = part.xb[c][n - 2]
+    if p < P - 1:
+        out[(1, "xr")] = part.xr[n - 1]
+        for c in kel:
+            out[(1, "x" + c)] = part.x[c][n - 1]
+        out[(1, "up")] = part.a(n - 1, n)
+        out[(1, "lo")] = part.a(n, n - 1)
+        for c in kel:
+            out[(1, "x" + c + "_up")] = part.sigma(c, n - 1, n)
+    return out
+
+
+def _pack_slots(slots: dict, ss: bool, batch: int, bmax: int, device) -> torch.Tensor:
+    """One partition's entries in a (2, kinds, batch, bmax, bmax) buffer
+    (zero padded; unused slots zero), the unit of the exchange."""
+    kinds = _kinds(ss)
+    buf = torch.zeros((2, len(kinds), batch, bmax, bmax), dtype=torch.complex128, device=device)
+    for (slot, kind), t in slots.items():
+        buf[slot, kinds.index(kind), :, :t.shape[-2], :t.shape[-1]] = t
+    return buf
+
+
+def _reduced_from(entry, P: int, ss: bool) -> tuple[dict, list]:
+    """Reduced block lists from entry(p, slot, kind) -> (batch, rows, cols),
+    plus the (kind, index) entries that must be replaced by -(.)^H."""
     red = {"xr": [], "up": [], "lo": []}
     for c in "lg":
         red["x" + c], red["x" + c + "_up"] = [], []
-    for p_idx, p in enumerate(parts):
-        n = p.n
-        if p_idx > 0:
-            red["xr"].append(p.xr[0])
-            for c in kel:
-                red["x" + c].append(p.x[c][0])
-            if p_idx < P - 1:
-                red["lo"].append(p.bu[n - 2])
-                red["up"].append(p.bl[n - 2])
-                for c in kel:
-                    red["x" + c + "_up"].append(p.o.comb(p.xb[c][n - 2], alpha=-1.0, op_x=_C))
-        if p_idx < P - 1:
-            red["xr"].append(p.xr[n - 1])
-            for c in kel:
-                red["x" + c].append(p.x[c][n - 1])
-            red["up"].append(p.a(n - 1, n))
-            red["lo"].append(p.a(n, n - 1))
-            for c in kel:
-                red["x" + c + "_up"].append(p.sigma(c, n - 1, n))
+    neg_h = []
+    for p, slot, kind in _reduced_order(P, ss):
+        if slot == 0 and kind.endswith("_up") and kind != "up":
+            neg_h.append((kind, len(red[kind])))
+        red[kind].append(entry(p, slot, kind))
+    return red, neg_h
+
+
+def _reduced_from_gathered(gathered: torch.Tensor, shapes: dict, P: int, ss: bool) -> tuple[dict, list]:
+    """Reduced block lists from the all-gathered (P, 2, kinds, batch, bmax,
+    bmax) buffer: views of each entry at its own shape."""
+    kinds = _kinds(ss)
+
+    def entry(p, slot, kind):
+        r, c = shapes[(p, slot, kind)]
+        return gathered[p, slot, kinds.index(kind), :, :r, :c]
+
+    return _reduced_from(entry, P, ss)
+
+
+def _exchange_slots(buf: torch.Tensor, group) -> torch.Tensor:
+    """All-gather one partition's slot buffer from every rank of ``group``:
+    (P, 2, kinds, batch, bmax, bmax) on ``buf``'s device, rank order.  NCCL
+    exchanges device memory; other backends (gloo) go through host memory
+    (the stream is synchronised first)."""
+    import torch.distributed as dist
+
+    x = torch.view_as_real(buf)
+    if dist.get_backend(group) != "nccl":
+        if x.is_cuda:
+            torch.cuda.current_stream(x.device).synchronize()
+        x = x.cpu()
+    recv = [torch.empty_like(x) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(recv, x, group=group)
+    return torch.view_as_complex(torch.stack(recv).to(buf.device))
+
+
+def _gather_reduced(parts, ss):
+    """The reduced system of the partition boundary blocks (_serinv.py:373-442),
+    all partitions in this process."""
+    slots = [_local_slots(p, ss) for p in parts]
+    red, neg_h = _reduced_from(lambda p, slot, kind: slots[p][(slot, kind)], len(parts), ss)
+    o = parts[0].o
+    for kind, i in neg_h:
+        red[kind][i] = o.comb(red[kind][i], alpha=-1.0, op_x=_C)
     return red
 
 

@@ -7,11 +7,20 @@ partitions: selected inversion and selected solve with contact blocks and
 interior self-energies, stack batching, host (NumPy) operands, mixed block
 sizes and symmetric-storage outputs.  Every block operation of the
 partitioned solver runs in libqtxrgf (GEMM, inverse, block combination).
+The process-group mode (one partition per rank) runs as 2 and 3 processes
+sharing this GPU with a gloo group (the exchange goes through host memory, so
+no kernel of one rank waits on another) and must return, on every rank, the
+blocks of its partition exactly as the single-process solver does.
 """
+
+import os
+import socket
 
 import numpy as np
 import pytest
 import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
 from scipy import sparse
 
 from oracle import rgf_oracle as orc
@@ -162,3 +171,63 @@ def test_rgf_dist_rejects_short_partitions():
         RGFDist(num_partitions=3).selected_inv(A, DSDBCOO.zeros_like(A))
     with pytest.raises(ValueError):
         RGFDist(num_partitions=1)
+
+
+def _free_port():
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def _operands(ss):
+    L, obc = _system(nb=11, b=5, seed=31)
+    A = DSDBCOO.from_blocks(L["diag"], L["upper"], L["lower"], device="cuda")
+    if not ss:
+        return A, None, None, obc
+    SL = DSDBCOO.from_blocks(L["sl_d"], L["sl_u"], _lower_of(L["sl_u"]), device="cuda")
+    SG = DSDBCOO.from_blocks(L["sg_d"], L["sg_u"], _lower_of(L["sg_u"]), device="cuda")
+    return A, SL, SG, obc
+
+
+def _solve(solver, ss):
+    A, SL, SG, obc = _operands(ss)
+    if ss:
+        outs = [DSDBCOO.zeros_like(A) for _ in range(3)]
+        solver.selected_solve(A, SL, SG, outs, obc, return_retarded=True)
+    else:
+        outs = [DSDBCOO.zeros_like(A)]
+        solver.selected_inv(A, outs[0], obc)
+    return [o.to("cpu") for o in outs]
+
+
+def _rank_worker(rank, world, port, ss, out_dir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        torch.cuda.set_device(0)
+        outs = _solve(RGFDist(max_batch_size=2, comm=dist.group.WORLD), ss)
+        np.savez(os.path.join(out_dir, f"r{rank}.npz"), *[o.data for o in outs])
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("ss", [False, True], ids=["inv", "solve"])
+def test_rgf_dist_one_partition_per_rank(tmp_path, world, ss):
+    mp.start_processes(_rank_worker, args=(world, _free_port(), ss, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    want = _solve(RGFDist(max_batch_size=2, num_partitions=world), ss)
+    nb = len(want[0].block_sizes)
+    bounds = [(0, 4), (4, 8), (8, 11)] if world == 3 else [(0, 6), (6, 11)]
+    for rank, (s, e) in enumerate(bounds):
+        got = np.load(tmp_path / f"r{rank}.npz")
+        for k, w in enumerate(want):
+            g = DSDBCOO.zeros_like(w)
+            g.data[...] = got[f"arr_{k}"]
+            keel = ss and k < 2
+            for i in range(s, e):
+                assert np.array_equal(g.blocks[i, i], w.blocks[i, i]), (rank, k, i)
+                if i + 1 < nb and (keel or not ss):
+                    assert np.array_equal(g.blocks[i, i + 1], w.blocks[i, i + 1]), (rank, k, i)
+                    assert np.array_equal(g.blocks[i + 1, i], w.blocks[i + 1, i]), (rank, k, i)
