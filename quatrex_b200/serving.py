@@ -87,6 +87,11 @@ class TransportServer:
         choice = self.tuner.best(device.block_size, len(energies), self.precision)
         ne_call = min(int(choice["energies_per_call"]), len(energies))
         path = choice.get("gemm_path", self.precision)
+        # the tuned call size is chosen on a short probe device: a long device
+        # takes smaller calls, so that one call's work space fits the budget
+        while ne_call > 1 and self._lib.qtx_transport_footprint(device.num_blocks, device.block_size, ne_call,
+                                                                _PRECISIONS[path]) > self.budget:
+            ne_call = max(1, ne_call // 2)
         dev = f"cuda:{self.cuda}"
         nb, b, ne = device.num_blocks, device.block_size, len(energies)
         with torch.cuda.stream(self._copy_stream):

@@ -159,3 +159,29 @@ def test_native_server_groups_waiting_small_requests():
                 ref = solve_grouped([d], [d.energies], keys=KEYS)[0]
         for k in KEYS:
             assert torch.equal(out[k], ref[k]), (b, k)
+
+
+def test_transport_server_shrinks_calls_to_its_budget():
+    """A request whose tuned call size does not fit the server's budget runs
+    in smaller calls (halved until one call's work space fits) instead of
+    being refused; the observables equal a direct solve."""
+    from quatrex_b200.serving import TransportServer
+
+    class _FixedTuner:
+        def best(self, b, ne, precision):
+            return {"energies_per_call": 16, "gemm_path": "fp64"}
+
+    d = make_device(num_blocks=6, block_size=32, num_energies=16, seed=8)
+    lib = _lib.load()
+    budget = lib.qtx_transport_footprint(6, 32, 4, _lib.QTX_PREC_FP64)
+    assert lib.qtx_transport_footprint(6, 32, 16, _lib.QTX_PREC_FP64) > budget
+    server = TransportServer(slots=1, memory_budget=budget, tuner=_FixedTuner(), group_small=False)
+    try:
+        res = server.submit(d, d.energies).result()
+    finally:
+        server.close()
+    ref = TransportSolver(d, max_batch_size=4).solve(d.energies, keys=("density", "transmission"))
+    for k in ("density", "transmission"):
+        got = res[k] if not isinstance(res[k], torch.Tensor) else res[k].cpu().numpy()
+        want = ref[k].cpu().numpy()
+        assert abs(got - want).max() <= 1e-12 * max(abs(want).max(), 1.0), k
