@@ -84,7 +84,15 @@ class Worker:
                 n = len(chunk)
                 if n not in outs:
                     outs[n] = solver.allocate_outputs(n, keys)
-                out = solver.solve(chunk, outs[n])
+                try:
+                    out = solver.solve(chunk, outs[n])
+                except MemoryError:
+                    # memory torch's caching allocator keeps for freed tensors is
+                    # out of reach of the library's stream-ordered pool: hand it
+                    # back once and retry
+                    torch.cuda.synchronize(self.cuda)
+                    torch.cuda.empty_cache()
+                    out = solver.solve(chunk, outs[n])
                 for k in keys:
                     results[k].append(out[k].cpu())
             if graph:
@@ -163,7 +171,8 @@ class BatchedTransport:
 
     def footprint(self, inst: Instance, ne_call: int) -> int:
         return TransportSolver.footprint_bytes(inst.device.num_blocks, inst.device.block_size,
-                                               min(ne_call, len(inst.energies)), ("density", "transmission"))
+                                               min(ne_call, len(inst.energies)), ("density", "transmission"),
+                                               precision=self.precision)
 
     def group_footprint(self, members: list[Instance]) -> int:
         """Device bytes of one grouped launch: its work space, H and the outputs."""

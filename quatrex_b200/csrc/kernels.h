@@ -52,9 +52,14 @@ void mixed_check_error(cudaStream_t stream);
 // X = A^-1 for n x n matrices.  info[e] (device, optional) receives the
 // 1-based column of the first exactly-zero pivot and is left untouched when
 // there is none (callers zero it once and may read it after several
-// launches).  X may alias A.
+// launches).  X may alias A.  Batches smaller than the GPU take a split path
+// whose per-panel scratch comes from the stream-ordered pool; with
+// may_allocate = false the one-CTA-per-matrix kernel runs at every size.
 void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const int* active,
-                 cudaStream_t stream);
+                 cudaStream_t stream, bool may_allocate = true);
+// Scratch the split path of launch_zinv takes for one call (0 when the batch
+// takes the one-CTA-per-matrix kernel).
+size_t zinv_workspace_bytes(int n, int64_t batch);
 
 // out = s + gamma_s * s2 + w^H - w  (n x n), in place allowed for out == s.
 void launch_skew_combine(int n, int64_t batch, MatView s, MatView w, MutView out, cudaStream_t stream);

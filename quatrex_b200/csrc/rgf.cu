@@ -1745,6 +1745,7 @@ size_t qtx_transport_footprint(int32_t num_blocks, int32_t block_size, int64_t e
   bytes += sizeof(cplx) * 9 * b * b * ne + sizeof(int) * (2 * ne + 2);  // Sancho-Rubio
   if (precision == QTX_PREC_MIXED)
     bytes += mixed_workspace_bytes(block_size, block_size, block_size, energies_per_call, energies_per_call);
+  bytes += zinv_workspace_bytes(block_size, energies_per_call);
   return bytes + (4u << 20);  // allocator granularity
 }
 

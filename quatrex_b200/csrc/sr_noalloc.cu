@@ -120,7 +120,7 @@ extern "C" qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const v
         cudaMemsetAsync(info, 0, sizeof(int) * (size_t)batch, s) != cudaSuccess)
       throw QtxError(QTX_E_CUDA, "cudaMemsetAsync failed");
     for (int it = 0; it < max_iterations; ++it) {
-      launch_zinv(n, batch, eps, inv, info, active, s);
+      launch_zinv(n, batch, eps, inv, info, active, s, /*may_allocate=*/false);
       mm(ONE, alpha, inv, t0);                               // a inv
       mm(ONE, beta, inv, t1);                                // b inv
       mm(ONE, t0, beta, t2);                                 // a inv b
@@ -142,7 +142,8 @@ extern "C" qtx_status qtx_sancho_rubio_noalloc(int32_t n, int64_t batch, const v
         break;
       }
     }
-    launch_zinv(n, batch, eps_s, MutView{reinterpret_cast<cplx*>(x), n, (int64_t)n * n}, info, nullptr, s);
+    launch_zinv(n, batch, eps_s, MutView{reinterpret_cast<cplx*>(x), n, (int64_t)n * n}, info, nullptr, s,
+                /*may_allocate=*/false);
     if (iterations &&
         cudaMemcpyAsync(iterations, its, sizeof(int) * (size_t)batch, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
       throw QtxError(QTX_E_CUDA, "iteration count copy failed");

@@ -78,18 +78,23 @@ class TransportSolver:
         self._e_buf = None
 
     @staticmethod
-    def footprint_bytes(num_blocks: int, block_size: int, energies_per_call: int, keys=OUTPUT_KEYS) -> int:
-        """Device bytes one call holds: H and couplings, the work space of one
-        energy batch and the requested outputs (used for admission control)."""
+    def footprint_bytes(num_blocks: int, block_size: int, energies_per_call: int, keys=OUTPUT_KEYS,
+                        precision: str = "fp64") -> int:
+        """Device bytes one call holds: H and couplings, the library's work
+        space for one energy batch (sweep, Sancho-Rubio, the scratch of the
+        block inverse and of the mixed-precision products:
+        ``qtx_transport_footprint``) and the requested outputs (used for
+        admission control)."""
         nb, b, ne = int(num_blocks), int(block_size), int(energies_per_call)
         bb = 16 * b * b
         h = bb * (nb + 3 * max(nb - 1, 1))
-        ws = bb * ne * (3 * nb + 20) + 64 * ne + 4 * (nb + 2) * ne
-        sr = bb * ne * 9
+        lib = _lib.load()
+        prec = _lib.QTX_PREC_MIXED if precision == "mixed" else _lib.QTX_PREC_FP64
+        ws = int(lib.qtx_transport_footprint(nb, b, ne, prec))
         blocks = {"gr_diag": nb, "gr_upper": nb - 1, "gr_lower": nb - 1, "gl_diag": nb, "gl_upper": nb - 1,
                   "gg_diag": nb, "gg_upper": nb - 1}
         out = sum(bb * ne * blocks[k] for k in keys if k in blocks) + 64 * ne * nb
-        return int(h + ws + sr + out)
+        return int(h + ws + out)
 
     def allocate_outputs(self, num_energies: int, keys=OUTPUT_KEYS) -> dict:
         return allocate_outputs(self.nb, self.b, num_energies, keys, self.cuda)
