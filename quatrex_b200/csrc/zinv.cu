@@ -850,6 +850,12 @@ template <int TPR, int RPT, int CPT>
 void launch_split_t(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t stream) {
   const InvShape s = inv_shape(n);
   const int W = s.w;
+  const size_t psmem = inv_smem_bytes(n) - (size_t)slab_elems(n, s) * sizeof(cplx);
+  const size_t usmem = split_update_smem(W);
+  const size_t xsmem = split_unscramble_smem(n);
+  qtx_opt_in_smem((const void*)zinv_split_panel_kernel<TPR, RPT, CPT>, psmem);
+  qtx_opt_in_smem((const void*)zinv_split_update_kernel, usmem);
+  qtx_opt_in_smem((const void*)zinv_split_unscramble_kernel, xsmem);
   const size_t bytes = sizeof(cplx) * (size_t)batch * (3 * (size_t)n * W) + sizeof(int) * (size_t)batch * 2 * n + 256;
   unsigned char* buf = static_cast<unsigned char*>(qtx_malloc_async(bytes, stream));
   if (!buf) throw QtxError(QTX_E_NOMEM, "qtx inverse: scratch allocation failed");
@@ -859,12 +865,7 @@ void launch_split_t(int n, int64_t batch, MatView a, MutView x, int* info, const
   sc.d = sc.r + (size_t)batch * W * n;
   sc.sigma = reinterpret_cast<int*>(sc.d + (size_t)batch * W * n);
   sc.perm = sc.sigma + (size_t)batch * n;
-  const size_t psmem = inv_smem_bytes(n) - (size_t)slab_elems(n, s) * sizeof(cplx);
-  const size_t usmem = split_update_smem(W);
-  const size_t xsmem = split_unscramble_smem(n);
-  qtx_opt_in_smem((const void*)zinv_split_panel_kernel<TPR, RPT, CPT>, psmem);
-  qtx_opt_in_smem((const void*)zinv_split_update_kernel, usmem);
-  qtx_opt_in_smem((const void*)zinv_split_unscramble_kernel, xsmem);
+
   const unsigned gb = (unsigned)(batch < 65535 ? batch : 65535);
   const int nslab = (n + SPLIT_CW - 1) / SPLIT_CW, ngroups = (n + SPLIT_ROWS - 1) / SPLIT_ROWS;
   for (int k0 = 0; k0 < n; k0 += W) {
