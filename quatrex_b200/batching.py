@@ -34,6 +34,9 @@ from quatrex_b200.transport import (GROUPED_MAX_BLOCK_SIZE, TransportSolver, gro
                                     solve_grouped)
 from quatrex_b200.workloads import TransportDevice
 
+# largest block size whose sweeps are captured as CUDA graphs
+GRAPH_MAX_BLOCK_SIZE = 128
+
 OBSERVABLE_KEYS = ("density", "hole_density", "transmission", "current_left", "current_right", "sr_iterations", "dos",
                    "layer_current")
 
@@ -69,7 +72,10 @@ class Worker:
         path = choice.get("gemm_path", precision)
         # a captured sweep pays off only when it is replayed: use it when the
         # instance has at least three full-size calls (same buffers each time)
-        graph = bool(choice.get("graph", False)) and len(energies) // max(ne_call, 1) >= 3
+        # and its launches are short (b <= 128; a captured sweep also keeps
+        # its work space for the life of the instance)
+        graph = (bool(choice.get("graph", False)) and len(energies) // max(ne_call, 1) >= 3
+                 and dev.block_size <= GRAPH_MAX_BLOCK_SIZE)
         energies = np.asarray(energies, dtype=np.float64)
         results = {k: [] for k in keys}
         with torch.cuda.stream(self.stream):
@@ -89,13 +95,17 @@ class Worker:
                 except MemoryError:
                     # memory torch's caching allocator keeps for freed tensors is
                     # out of reach of the library's stream-ordered pool: hand it
-                    # back once and retry
+                    # back, drop this instance's captured sweep (its work space
+                    # stays allocated while it exists) and retry eagerly
+                    if solver.use_graph:
+                        solver.release_graphs()
+                        solver.use_graph = False
                     torch.cuda.synchronize(self.cuda)
                     torch.cuda.empty_cache()
                     out = solver.solve(chunk, outs[n])
                 for k in keys:
                     results[k].append(out[k].cpu())
-            if graph:
+            if solver.use_graph:
                 # the captured sweeps reference this instance's buffers: drop them
                 solver.release_graphs()
             self.stream.synchronize()
