@@ -138,7 +138,7 @@ __device__ inline GjSmem gj_smem_layout(unsigned char* base, int n, int wp, int 
 // permutation sigma (pos2row / row2pos, relative to the current order) and
 // the swaps perm[k0 .. k0 + w), and leave the eliminated panel in P (rows in
 // the current order).  Ends with a CTA barrier.
-template <int TPR, int RPT, int CPT>
+template <int TPR, int RPT, int CPT, int ROT>
 __device__ __forceinline__ void gj_panel(int n, int k0, int w, int WP, const cplx* X, int64_t ldx, const GjSmem& sm,
                                          int& zero_pivot) {
   cplx* P = sm.P;
@@ -155,15 +155,18 @@ __device__ __forceinline__ void gj_panel(int n, int k0, int w, int WP, const cpl
   const int rstride = THREADS / TPR;
   const int r_own = tid / TPR;
   const int c_own = tid % TPR;
-    // ---- 1. stage the panel (rows in the current order of X)
+    // ---- 1. stage the panel (rows in the current order of X), every
+    // element in flight at once (asynchronous copies)
     for (int idx = tid; idx < n * w; idx += THREADS) {
       int r = idx / w, c = idx % w;
-      P[pidx(r, c, WP)] = X[(int64_t)r * ldx + k0 + c];
+      cp_async16(&P[pidx(r, c, WP)], &X[(int64_t)r * ldx + k0 + c], true);
     }
+    cp_async_commit();
     for (int r = tid; r < n; r += THREADS) {
       pos2row[r] = r;
       row2pos[r] = r;
     }
+    cp_async_wait<0>();
     __syncthreads();
 
     // The thread's panel entries live in registers during the elimination:
@@ -180,7 +183,101 @@ __device__ __forceinline__ void gj_panel(int n, int k0, int w, int WP, const cpl
       }
     const int grp0 = lane - c_own;  // first lane of this row's group (groups never straddle warps)
     // rows before k0 are the pivots of earlier panels (rows are in the new order now)
-    if constexpr (CPT == 1) {
+    bool rotated = false;
+    if constexpr (TPR == 1 && RPT == 1 && CPT == 32) {
+      if constexpr (ROT >= 1) {
+        constexpr bool UNIFORM = ROT == 2;
+        // Register rotation: at step kk, reg[0][j] holds panel column
+        // (kk + j) mod 32, so the step's column is always reg[0][0] (no
+        // selects over the row) and every update is unpredicated (columns
+        // at or beyond w stay zero: the published pivot rows carry zeros
+        // there).  Same operations on every element as the generic loop.
+        rotated = true;
+        bool used = r_own < k0;
+        auto rotate = [&]() {
+          const cplx t0 = reg[0][0];
+#pragma unroll
+          for (int j = 0; j < 31; ++j) reg[0][j] = reg[0][j + 1];
+          reg[0][31] = t0;
+        };
+#pragma unroll 1
+        for (int kk = 0; kk < w; ++kk) {
+          const int k = k0 + kk;
+          const cplx colv = reg[0][0];
+          reg[0][0] = cmk(0, 0);
+          double bv = -1.0;
+          int bi = n;
+          if (r_own < n && !used) {
+            bv = cabs1(colv);
+            bi = r_own;
+          }
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            double v2 = __shfl_xor_sync(0xffffffffu, bv, off);
+            int i2 = __shfl_xor_sync(0xffffffffu, bi, off);
+            argmax_combine(bv, bi, v2, i2);
+          }
+          const int par = kk & 1;
+          cplx* my_cand = cand + (size_t)(par * NWARPS + warp) * WP;
+          const int slot = par * NWARPS;
+          if (r_own == bi) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) my_cand[j] = reg[0][j];
+            my_cand[0] = cmk(1, 0);
+            red_piv[slot + warp] = colv;
+          }
+          if (lane == 0) {
+            red_v[slot + warp] = bv;
+            red_i[slot + warp] = bi;
+          }
+          __syncthreads();  // candidates of every warp visible
+          double v = red_v[slot + lane % NWARPS];
+          int p = red_i[slot + lane % NWARPS];
+#pragma unroll
+          for (int off = NWARPS / 2; off > 0; off >>= 1) {
+            const double v2 = __shfl_xor_sync(0xffffffffu, v, off);
+            const int i2 = __shfl_xor_sync(0xffffffffu, p, off);
+            argmax_combine(v, p, v2, i2);
+          }
+          const int pw = p >> 5;  // one row per thread: row p lives in warp p / 32
+          const cplx* prow = cand + (size_t)(par * NWARPS + pw) * WP;
+          const cplx piv = red_piv[slot + pw];
+          if (piv.x == 0.0 && piv.y == 0.0 && !zero_pivot) zero_pivot = k + 1;
+          const cplx d = crecip_pivot(piv);
+          if (tid == 0) pivs[kk] = p;
+          if (r_own < n) {
+            if constexpr (UNIFORM) {
+              // the pivot row as 0 - (-d) p: one update formula for every
+              // row, so the warp holding the pivot row does not run both
+              // branches while the others wait at the next barrier
+              const bool is_p = r_own == p;
+              used = used || is_p;
+              const cplx fd = is_p ? cmk(-d.x, -d.y) : cmul(colv, d);
+              if (is_p) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) reg[0][j] = cmk(0, 0);
+              }
+#pragma unroll
+              for (int j = 0; j < 32; ++j) reg[0][j] = cfms(fd, prow[j], reg[0][j]);
+            } else {
+              if (r_own == p) {
+                used = true;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) reg[0][j] = cmul(prow[j], d);
+              } else {
+                const cplx fd = cmul(colv, d);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) reg[0][j] = cfms(fd, prow[j], reg[0][j]);
+              }
+            }
+          }
+          rotate();
+        }
+        for (int extra = w; extra < 32; ++extra) rotate();  // natural column order again
+      }
+    }
+    if (rotated) {
+    } else if constexpr (CPT == 1) {
       // One column per lane: lane c_own holds column c_own of the rows
       // r_own + q * rstride; the factors of column kk come by shuffle from
       // the lane that holds it, the pivot row is one shared-memory word per
@@ -393,7 +490,7 @@ __device__ __forceinline__ void gj_panel(int n, int k0, int w, int WP, const cpl
     __syncthreads();
 }
 
-template <int TPR, int RPT, int CPT>
+template <int TPR, int RPT, int CPT, int ROT>
 __global__ void __launch_bounds__(THREADS, 1)
     zinv_gj_kernel(int n, int64_t batch, const cplx* __restrict__ a_base, int64_t lda, int64_t sa,
                    cplx* x_base, int64_t ldx, int64_t sx, int* info, const int* active) {
@@ -426,7 +523,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     for (int k0 = 0; k0 < n; k0 += W) {
       const int w = min(W, n - k0);
-      gj_panel<TPR, RPT, CPT>(n, k0, w, WP, X, ldx, sm, zero_pivot);
+      gj_panel<TPR, RPT, CPT, ROT>(n, k0, w, WP, X, ldx, sm, zero_pivot);
 
       // ---- 3. rank-w update of the other columns, slabs of CW columns.
       // Output position i reads X[sigma(i)], and sigma(i) is either i itself or
@@ -594,12 +691,12 @@ __global__ void __launch_bounds__(THREADS, 1)
 // eliminates the panel, then (matrix x 32-column slab x 128-row group) CTAs
 // apply its rank-w update -- so the updates of a few matrices spread over the
 // whole GPU (the column chain of the elimination stays one CTA per matrix).
-// Per matrix the panel launch leaves in global scratch: the eliminated panel
+// Per matrix the panel launch leaves in global scratch the eliminated panel
 // P (n x W, rows in the order before the panel's permutation), sigma
-// (pos2row), the pivot rows R = X[sigma(k0 + j)] and the panel-position rows
-// D = X[k0 + j] (n columns each), and the column swaps; the update CTAs read
-// R and D from the scratch, so no CTA reads a row of X that another CTA of
-// the same launch writes.
+// (pos2row) and the column swaps; a row-copy launch adds the pivot rows
+// R = X[sigma(k0 + j)] and the panel-position rows D = X[k0 + j] (n columns
+// each); the update CTAs read R and D from the scratch, so no CTA reads a row
+// of X that another CTA of the same launch writes.
 
 struct SplitScratch {
   cplx* p;      // batch x n x W
@@ -609,7 +706,7 @@ struct SplitScratch {
   int* perm;    // batch x n
 };
 
-template <int TPR, int RPT, int CPT>
+template <int TPR, int RPT, int CPT, int ROT>
 __global__ void __launch_bounds__(THREADS, 1)
     zinv_split_panel_kernel(int n, int64_t batch, const cplx* __restrict__ a_base, int64_t lda, int64_t sa,
                             cplx* x_base, int64_t ldx, int64_t sx, int k0, SplitScratch sc, int* info,
@@ -634,24 +731,15 @@ __global__ void __launch_bounds__(THREADS, 1)
       __syncthreads();
     }
     int zero_pivot = 0;
-    gj_panel<TPR, RPT, CPT>(n, k0, w, WP, X, ldx, sm, zero_pivot);
+    gj_panel<TPR, RPT, CPT, ROT>(n, k0, w, WP, X, ldx, sm, zero_pivot);
     cplx* pe = sc.p + e * (int64_t)n * W;
-    cplx* re = sc.r + e * (int64_t)W * n;
-    cplx* de = sc.d + e * (int64_t)W * n;
     for (int idx = tid; idx < n * w; idx += THREADS) {
       const int r = idx / w, c = idx % w;
       pe[(int64_t)r * W + c] = sm.P[pidx(r, c, WP)];
     }
-    // pivot rows and panel-position rows before the update moves them (the
-    // panel columns are not read from these copies)
-    for (int idx = tid; idx < w * n; idx += THREADS) {
-      const int j = idx / n, c = idx % n;
-      re[idx] = X[(int64_t)sm.pos2row[k0 + j] * ldx + c];
-      de[idx] = X[(int64_t)(k0 + j) * ldx + c];
-    }
     for (int r = tid; r < n; r += THREADS) sc.sigma[e * n + r] = sm.pos2row[r];
     for (int kk = tid; kk < w; kk += THREADS) sc.perm[e * n + k0 + kk] = sm.perm[k0 + kk];
-    __syncthreads();  // every copy of the old rows made before the panel columns change
+    __syncthreads();  // sigma and the panel copied before the panel columns change
     for (int idx = tid; idx < n * w; idx += THREADS) {
       const int i = idx / w, c = idx % w;
       X[(int64_t)i * ldx + k0 + c] = sm.P[pidx(sm.pos2row[i], c, WP)];
@@ -659,6 +747,27 @@ __global__ void __launch_bounds__(THREADS, 1)
     // the first exact zero pivot of the matrix (earlier panels win)
     if (info && tid == 0 && zero_pivot && info[e] == 0) info[e] = zero_pivot;
     __syncthreads();
+  }
+}
+
+// The pivot rows R = X[sigma(k0 + j)] and the panel-position rows
+// D = X[k0 + j] of every matrix, copied before the update moves them (one
+// CTA per row and matrix; the panel columns of X may already hold their final
+// values, the update does not read them from these copies).
+__global__ void __launch_bounds__(256)
+    zinv_split_rows_kernel(int n, int64_t batch, const cplx* x_base, int64_t ldx, int64_t sx, int k0, int W,
+                           SplitScratch sc, const int* active) {
+  const int j = blockIdx.x;
+  for (int64_t e = blockIdx.y; e < batch; e += gridDim.y) {
+    if (active && !active[e]) continue;
+    const cplx* X = x_base + e * sx;
+    const int src = sc.sigma[e * n + k0 + j];
+    cplx* re = sc.r + (e * (int64_t)W + j) * n;
+    cplx* de = sc.d + (e * (int64_t)W + j) * n;
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+      re[c] = X[(int64_t)src * ldx + c];
+      de[c] = X[(int64_t)(k0 + j) * ldx + c];
+    }
   }
 }
 
@@ -833,27 +942,52 @@ __global__ void __launch_bounds__(THREADS)
 
 namespace {
 
+// Column loop of the 32-column panel elimination (b in 129..256): 1 (the
+// default) register rotation, 0 the select-based loop (QTX_INV_ROTATE); both
+// give the same results bit for bit.  Rotation measured on B200: b = 256
+// batch 148 1.81 ms vs 1.90, batch 16 (split path) 0.97 vs 1.06.  Rotation
+// with the updates of each step deferred into the next step's reduction was
+// slower (1.84 / 1.01: more spills at 255 registers).
+int rotate_panel() {
+  static int v = [] {
+    const char* env = getenv("QTX_INV_ROTATE");
+    return env ? atoi(env) : 1;
+  }();
+  return v;
+}
+
+template <int TPR, int RPT, int CPT, int ROT>
+void launch_inv_r(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, size_t smem,
+                  cudaStream_t stream) {
+  qtx_opt_in_smem((const void*)zinv_gj_kernel<TPR, RPT, CPT, ROT>, smem);
+  int grid = (int)(batch < 65535 ? batch : 65535);
+  zinv_gj_kernel<TPR, RPT, CPT, ROT><<<grid, THREADS, smem, stream>>>(n, batch, a.ptr, a.ld, a.stride, x.ptr,
+                                                                       x.ld, x.stride, info, active);
+}
+
 template <int TPR, int RPT, int CPT>
 void launch_inv_t(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, size_t smem,
                   cudaStream_t stream) {
-  qtx_opt_in_smem((const void*)zinv_gj_kernel<TPR, RPT, CPT>, smem);
-  int grid = (int)(batch < 65535 ? batch : 65535);
-  zinv_gj_kernel<TPR, RPT, CPT><<<grid, THREADS, smem, stream>>>(n, batch, a.ptr, a.ld, a.stride, x.ptr, x.ld,
-                                                                  x.stride, info, active);
+  if constexpr (TPR == 1 && RPT == 1 && CPT == 32) {
+    const int r = rotate_panel();
+    if (r == 2) return launch_inv_r<TPR, RPT, CPT, 2>(n, batch, a, x, info, active, smem, stream);
+    if (r == 1) return launch_inv_r<TPR, RPT, CPT, 1>(n, batch, a, x, info, active, smem, stream);
+  }
+  launch_inv_r<TPR, RPT, CPT, 0>(n, batch, a, x, info, active, smem, stream);
 }
 
 }  // namespace
 
 namespace {
 
-template <int TPR, int RPT, int CPT>
-void launch_split_t(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t stream) {
+template <int TPR, int RPT, int CPT, int ROT>
+void launch_split_r(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t stream) {
   const InvShape s = inv_shape(n);
   const int W = s.w;
   const size_t psmem = inv_smem_bytes(n) - (size_t)slab_elems(n, s) * sizeof(cplx);
   const size_t usmem = split_update_smem(W);
   const size_t xsmem = split_unscramble_smem(n);
-  qtx_opt_in_smem((const void*)zinv_split_panel_kernel<TPR, RPT, CPT>, psmem);
+  qtx_opt_in_smem((const void*)zinv_split_panel_kernel<TPR, RPT, CPT, ROT>, psmem);
   qtx_opt_in_smem((const void*)zinv_split_update_kernel, usmem);
   qtx_opt_in_smem((const void*)zinv_split_unscramble_kernel, xsmem);
   const size_t bytes = sizeof(cplx) * (size_t)batch * (3 * (size_t)n * W) + sizeof(int) * (size_t)batch * 2 * n + 256;
@@ -870,8 +1004,10 @@ void launch_split_t(int n, int64_t batch, MatView a, MutView x, int* info, const
   const int nslab = (n + SPLIT_CW - 1) / SPLIT_CW, ngroups = (n + SPLIT_ROWS - 1) / SPLIT_ROWS;
   for (int k0 = 0; k0 < n; k0 += W) {
     const int w = std::min(W, n - k0);
-    zinv_split_panel_kernel<TPR, RPT, CPT><<<gb, THREADS, psmem, stream>>>(n, batch, a.ptr, a.ld, a.stride, x.ptr,
-                                                                          x.ld, x.stride, k0, sc, info, active);
+    zinv_split_panel_kernel<TPR, RPT, CPT, ROT><<<gb, THREADS, psmem, stream>>>(n, batch, a.ptr, a.ld, a.stride,
+                                                                               x.ptr, x.ld, x.stride, k0, sc, info,
+                                                                               active);
+    zinv_split_rows_kernel<<<dim3(w, gb), 256, 0, stream>>>(n, batch, x.ptr, x.ld, x.stride, k0, W, sc, active);
     zinv_split_update_kernel<<<dim3(nslab * ngroups, gb), SPLIT_THREADS, usmem, stream>>>(n, batch, x.ptr, x.ld,
                                                                                          x.stride, k0, w, W, sc,
                                                                                          active);
@@ -879,6 +1015,16 @@ void launch_split_t(int n, int64_t batch, MatView a, MutView x, int* info, const
   zinv_split_unscramble_kernel<<<dim3((n + UNS_ROWS - 1) / UNS_ROWS, gb), THREADS, xsmem, stream>>>(
       n, batch, x.ptr, x.ld, x.stride, sc, active);
   cudaFreeAsync(buf, stream);
+}
+
+template <int TPR, int RPT, int CPT>
+void launch_split_t(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t stream) {
+  if constexpr (TPR == 1 && RPT == 1 && CPT == 32) {
+    const int r = rotate_panel();
+    if (r == 2) return launch_split_r<TPR, RPT, CPT, 2>(n, batch, a, x, info, active, stream);
+    if (r == 1) return launch_split_r<TPR, RPT, CPT, 1>(n, batch, a, x, info, active, stream);
+  }
+  launch_split_r<TPR, RPT, CPT, 0>(n, batch, a, x, info, active, stream);
 }
 
 // Batches below this many matrices take the split path (measured on B200:
