@@ -942,16 +942,18 @@ __global__ void __launch_bounds__(THREADS)
 
 namespace {
 
-// Column loop of the 32-column panel elimination (b in 129..256): 1 (the
-// default) register rotation, 0 the select-based loop (QTX_INV_ROTATE); both
-// give the same results bit for bit.  Rotation measured on B200: b = 256
-// batch 148 1.81 ms vs 1.90, batch 16 (split path) 0.97 vs 1.06.  Rotation
-// with the updates of each step deferred into the next step's reduction was
-// slower (1.84 / 1.01: more spills at 255 registers).
+// Column loop of the 32-column panel elimination (b in 129..256),
+// QTX_INV_ROTATE: 0 the select-based loop, 1 register rotation (bit for bit
+// the same results), 2 (the default) rotation with the pivot row updated by
+// the same formula as the other rows (0 - (-d) p instead of p d: FP64
+// rounding of the same quantity).  Measured on B200, b = 256: batch 148
+// 1.82 / 1.72 / 1.67 ms, batch 16 (split path) 0.98 / 0.89 / 0.84 ms.
+// Rotation with the updates of each step deferred into the next step's
+// reduction was slower (more spills at 255 registers) and is not built.
 int rotate_panel() {
   static int v = [] {
     const char* env = getenv("QTX_INV_ROTATE");
-    return env ? atoi(env) : 1;
+    return env ? atoi(env) : 2;
   }();
   return v;
 }
