@@ -168,7 +168,7 @@ qtx_status qtx_selected_solve(qtx_ctx* ctx, const qtx_btd_desc* a_desc, const vo
  * each batch entry; converged entries stop iterating (per-entry masks).
  * Returns QTX_E_NOT_CONVERGED (after writing x) when an entry reached
  * max_iterations (sancho_rubio.py:81-82 warns in that case), QTX_E_SINGULAR
- * when a decimation block was exactly singular.
+ * when a decimation block was exactly singular.  batch = 0 is a no-op.
  * <- SanchoRubio(max_iterations, convergence_tol)(a_ii, a_ij, a_ji, contact). */
 qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* a_ii, int64_t stride_ii,
                             const void* a_ij, int64_t stride_ij, const void* a_ji, int64_t stride_ji,
@@ -264,7 +264,7 @@ typedef struct qtx_transport_problem {
   int64_t num_energies;
   const void* h_diag;       /* (nb, b, b) */
   const void* h_upper;      /* (nb-1, b, b): H[i, i+1]; H[i+1, i] = H[i, i+1]^H */
-  const double* energies;   /* (num_energies) device */
+  const double* energies;   /* (num_energies) device; may be NULL when num_energies = 0 (a no-op call) */
   double eta, mu_left, mu_right, kt;
   double sr_tol;
   int32_t sr_max_iterations;

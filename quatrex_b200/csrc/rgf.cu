@@ -1967,8 +1967,9 @@ qtx_status qtx_sancho_rubio(qtx_ctx* ctx, int32_t n, int64_t batch, const void* 
                             qtx_stream stream) {
   bool ok = true;
   qtx_status st = guarded(ctx, [&] {
-    if (n < 1 || batch < 1 || !a_ii || !a_ij || !a_ji || !x || max_iterations < 1)
+    if (n < 1 || batch < 0 || max_iterations < 1 || (batch > 0 && (!a_ii || !a_ij || !a_ji || !x)))
       throw QtxError(QTX_E_INVAL, "qtx_sancho_rubio: bad arguments");
+    if (batch == 0) return;  // an empty energy batch: nothing to decimate
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     ok = sancho_rubio_impl(ctx, n, batch, MatView{reinterpret_cast<const cplx*>(a_ii), n, stride_ii},
                            MatView{reinterpret_cast<const cplx*>(a_ij), n, stride_ij},
@@ -2212,8 +2213,9 @@ qtx_status qtx_transport_solve(qtx_ctx* ctx, const qtx_transport_problem* p, con
   qtx_status st = guarded(ctx, [&] {
     if (!p || !o) throw QtxError(QTX_E_INVAL, "qtx_transport_solve: null problem");
     if (p->num_blocks < 2 || p->block_size < 1 || p->num_energies < 0 || !p->h_diag || !p->h_upper ||
-        !p->energies || p->kt <= 0 || p->sr_max_iterations < 1)
+        (p->num_energies > 0 && !p->energies) || p->kt <= 0 || p->sr_max_iterations < 1)
       throw QtxError(QTX_E_INVAL, "qtx_transport_solve: bad problem");
+    if (p->num_energies == 0) return;  // an empty energy grid: nothing to solve
     const bool use_graph = (flags & QTX_FLAG_GRAPH) != 0 &&
                            (p->max_batch_size <= 0 || p->max_batch_size >= p->num_energies);
     if (use_graph) transport_graph_impl(ctx, *p, *o, precision, reinterpret_cast<cudaStream_t>(stream), ok);
