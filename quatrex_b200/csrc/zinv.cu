@@ -185,13 +185,13 @@ __device__ __forceinline__ void gj_panel(int n, int k0, int w, int WP, const cpl
     // rows before k0 are the pivots of earlier panels (rows are in the new order now)
     bool rotated = false;
     if constexpr (TPR == 1 && RPT == 1 && CPT == 32) {
-      if constexpr (ROT >= 1) {
-        constexpr bool UNIFORM = ROT == 2;
+      if constexpr (ROT == 1) {
         // Register rotation: at step kk, reg[0][j] holds panel column
         // (kk + j) mod 32, so the step's column is always reg[0][0] (no
         // selects over the row) and every update is unpredicated (columns
         // at or beyond w stay zero: the published pivot rows carry zeros
-        // there).  Same operations on every element as the generic loop.
+        // there).  The same pivots and the same update of every non-pivot
+        // row as the generic loop.
         rotated = true;
         bool used = r_own < k0;
         auto rotate = [&]() {
@@ -246,30 +246,18 @@ __device__ __forceinline__ void gj_panel(int n, int k0, int w, int WP, const cpl
           const cplx d = crecip_pivot(piv);
           if (tid == 0) pivs[kk] = p;
           if (r_own < n) {
-            if constexpr (UNIFORM) {
-              // the pivot row as 0 - (-d) p: one update formula for every
-              // row, so the warp holding the pivot row does not run both
-              // branches while the others wait at the next barrier
-              const bool is_p = r_own == p;
-              used = used || is_p;
-              const cplx fd = is_p ? cmk(-d.x, -d.y) : cmul(colv, d);
-              if (is_p) {
+            // the pivot row as 0 - (-d) p: one update formula for every
+            // row, so the warp holding the pivot row does not run two
+            // branches while the others wait at the next barrier
+            const bool is_p = r_own == p;
+            used = used || is_p;
+            const cplx fd = is_p ? cmk(-d.x, -d.y) : cmul(colv, d);
+            if (is_p) {
 #pragma unroll
-                for (int j = 0; j < 32; ++j) reg[0][j] = cmk(0, 0);
-              }
-#pragma unroll
-              for (int j = 0; j < 32; ++j) reg[0][j] = cfms(fd, prow[j], reg[0][j]);
-            } else {
-              if (r_own == p) {
-                used = true;
-#pragma unroll
-                for (int j = 0; j < 32; ++j) reg[0][j] = cmul(prow[j], d);
-              } else {
-                const cplx fd = cmul(colv, d);
-#pragma unroll
-                for (int j = 0; j < 32; ++j) reg[0][j] = cfms(fd, prow[j], reg[0][j]);
-              }
+              for (int j = 0; j < 32; ++j) reg[0][j] = cmk(0, 0);
             }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) reg[0][j] = cfms(fd, prow[j], reg[0][j]);
           }
           rotate();
         }
@@ -943,17 +931,18 @@ __global__ void __launch_bounds__(THREADS)
 namespace {
 
 // Column loop of the 32-column panel elimination (b in 129..256),
-// QTX_INV_ROTATE: 0 the select-based loop, 1 register rotation (bit for bit
-// the same results), 2 (the default) rotation with the pivot row updated by
-// the same formula as the other rows (0 - (-d) p instead of p d: FP64
-// rounding of the same quantity).  Measured on B200, b = 256: batch 148
-// 1.82 / 1.72 / 1.67 ms, batch 16 (split path) 0.98 / 0.89 / 0.84 ms.
-// Rotation with the updates of each step deferred into the next step's
-// reduction was slower (more spills at 255 registers) and is not built.
+// QTX_INV_ROTATE: 1 (the default) the rotated register row with one update
+// formula for every row, 0 the select-based loop of the other shapes.
+// Measured on B200, b = 256, batch 148 / batch 16 (split path): select loop
+// 1.82 / 0.98 ms; rotation alone 1.72 / 0.89 ms (bit for bit the same
+// results as the select loop); rotation with the uniform pivot-row update
+// 1.67 / 0.84 ms (the pivot row then differs by FP64 rounding).  Rotation
+// with each step's updates deferred into the next step's reduction was
+// slower (more spills at 255 registers) and is not built.
 int rotate_panel() {
   static int v = [] {
     const char* env = getenv("QTX_INV_ROTATE");
-    return env ? atoi(env) : 2;
+    return env ? atoi(env) : 1;
   }();
   return v;
 }
@@ -972,8 +961,7 @@ void launch_inv_t(int n, int64_t batch, MatView a, MutView x, int* info, const i
                   cudaStream_t stream) {
   if constexpr (TPR == 1 && RPT == 1 && CPT == 32) {
     const int r = rotate_panel();
-    if (r == 2) return launch_inv_r<TPR, RPT, CPT, 2>(n, batch, a, x, info, active, smem, stream);
-    if (r == 1) return launch_inv_r<TPR, RPT, CPT, 1>(n, batch, a, x, info, active, smem, stream);
+    if (r != 0) return launch_inv_r<TPR, RPT, CPT, 1>(n, batch, a, x, info, active, smem, stream);
   }
   launch_inv_r<TPR, RPT, CPT, 0>(n, batch, a, x, info, active, smem, stream);
 }
@@ -1023,8 +1011,7 @@ template <int TPR, int RPT, int CPT>
 void launch_split_t(int n, int64_t batch, MatView a, MutView x, int* info, const int* active, cudaStream_t stream) {
   if constexpr (TPR == 1 && RPT == 1 && CPT == 32) {
     const int r = rotate_panel();
-    if (r == 2) return launch_split_r<TPR, RPT, CPT, 2>(n, batch, a, x, info, active, stream);
-    if (r == 1) return launch_split_r<TPR, RPT, CPT, 1>(n, batch, a, x, info, active, stream);
+    if (r != 0) return launch_split_r<TPR, RPT, CPT, 1>(n, batch, a, x, info, active, stream);
   }
   launch_split_r<TPR, RPT, CPT, 0>(n, batch, a, x, info, active, stream);
 }
