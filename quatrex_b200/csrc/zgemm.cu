@@ -6,18 +6,19 @@
 // decomposition on split fragments: Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br,
 // four DMMAs per 16x8 complex tile step.
 //
-// CTA tile 64x64 (complex), K step 8, 4-stage cp.async pipeline, 4 warps each
+// CTA tile 64x64 (complex), K step 16, double-buffered cp.async pipeline (one
+// barrier per 128 DMMAs of a warp; 80 KB, two CTAs per SM), 4 warps each
 // owning a 32x32 complex warp tile (2 x 4 DMMA tiles, real and imaginary
 // accumulators: 64 doubles per thread).  Tiles stay complex-interleaved in
 // shared memory so one 16-byte load yields both parts of an element; the
-// padded row strides (12 / 66 complex) make every 8-lane fragment load hit 8
+// padded row strides (20 / 66 complex) make every 8-lane fragment load hit 8
 // distinct 16-byte bank groups.
 #include "kernels.h"
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 8, STAGES = 4, THREADS = 128;
-constexpr int LD_KMAJOR = BK + 4;   // tile stored [row][k]: 12 complex = 192 B rows
+constexpr int BM = 64, BN = 64, BK = 16, STAGES = 2, THREADS = 128;
+constexpr int LD_KMAJOR = BK + 4;   // tile stored [row][k]: 20 complex = 320 B rows
 constexpr int LD_MMAJOR = BM + 2;   // tile stored [k][row]: 66 complex = 1056 B rows
 constexpr int TILE_ELEMS = (BM * LD_KMAJOR > BK * LD_MMAJOR) ? BM * LD_KMAJOR : BK * LD_MMAJOR;
 constexpr int SMEM_BYTES = STAGES * 2 * TILE_ELEMS * (int)sizeof(cplx);
