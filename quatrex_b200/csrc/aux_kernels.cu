@@ -50,7 +50,51 @@ __global__ void skew_combine_kernel(int n, int64_t batch, const cplx* s, int64_t
   }
 }
 
-// x <- x - x^H in place: each thread owns the pair (r, c), (c, r) with r <= c
+// X <- X - X^H in place by pairs of 32 x 32 tiles (ti <= tj) staged in shared
+// memory, so both the rows and the mirrored columns are read and written
+// coalesced.  The same arithmetic per element as sub_herm_kernel.
+__global__ void __launch_bounds__(256)
+    sub_herm_tiled_kernel(int n, int64_t batch, cplx* x, int64_t ld, int64_t sx) {
+  __shared__ cplx ta[32][33], tb[32][33];
+  const int nt = (n + 31) / 32;
+  // triangular index -> (ti, tj), ti <= tj, row-major over the upper triangle
+  const int pidx = blockIdx.x;
+  int ti = 0, rest = pidx;
+  while (rest >= nt - ti) {
+    rest -= nt - ti;
+    ++ti;
+  }
+  const int tj = ti + rest;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int64_t e = blockIdx.y; e < batch; e += gridDim.y) {
+    cplx* base = x + e * sx;
+    for (int r = ty; r < 32; r += 8) {
+      const int ar = ti * 32 + r, ac = tj * 32 + tx;
+      const int br = tj * 32 + r, bc = ti * 32 + tx;
+      ta[r][tx] = (ar < n && ac < n) ? base[(int64_t)ar * ld + ac] : cmk(0, 0);
+      tb[r][tx] = (br < n && bc < n) ? base[(int64_t)br * ld + bc] : cmk(0, 0);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+      const int ar = ti * 32 + r, ac = tj * 32 + tx;
+      if (ar < n && ac < n) {
+        const cplx a = ta[r][tx], b = tb[tx][r];  // b = X[ac][ar]
+        base[(int64_t)ar * ld + ac] = cmk(a.x - b.x, a.y + b.y);
+      }
+      if (ti != tj) {
+        const int br = tj * 32 + r, bc = ti * 32 + tx;
+        if (br < n && bc < n) {
+          const cplx b = tb[r][tx], a = ta[tx][r];  // a = X[bc][br]
+          base[(int64_t)br * ld + bc] = cmk(b.x - a.x, b.y + a.y);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// x <- x - x^H in place (small blocks): each thread owns the pair (r, c), (c, r)
+// with r <= c
 __global__ void sub_herm_kernel(int n, int64_t batch, cplx* x, int64_t ld, int64_t sx) {
   const int64_t pairs = (int64_t)n * (n + 1) / 2;
   const int64_t total = batch * pairs;
@@ -194,19 +238,40 @@ __global__ void trace_product_h_kernel(int rows, int cols, int64_t batch, const 
   }
 }
 
-__global__ void sr_norm_kernel(int n, int64_t batch, const cplx* a, int64_t lda, int64_t sa, const cplx* b,
-                               int64_t ldb, int64_t sb, double tol, int* active, int* iterations, int* num_active) {
+// Sancho-Rubio convergence measure ||abs(alpha) + abs(beta)||_F / 2 of every
+// active energy (sancho_rubio.py:76-79), one CTA of SRN_THREADS per energy,
+// contiguous blocks read by linear index with four independent sums per
+// thread.
+constexpr int SRN_THREADS = 1024;
+
+__device__ __forceinline__ double sr_norm_term(cplx av, cplx bv) {
+  const double s = hypot(av.x, av.y) + hypot(bv.x, bv.y);
+  return s * s;
+}
+
+__global__ void __launch_bounds__(SRN_THREADS)
+    sr_norm_kernel(int n, int64_t batch, const cplx* a, int64_t lda, int64_t sa, const cplx* b, int64_t ldb,
+                   int64_t sb, double tol, int* active, int* iterations, int* num_active) {
+  const int nn = n * n;
   for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
     if (!active[e]) continue;
-    double acc = 0;
-    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-      int r = q / n, c = q % n;
-      cplx av = a[e * sa + (int64_t)r * lda + c];
-      cplx bv = b[e * sb + (int64_t)r * ldb + c];
-      double s = hypot(av.x, av.y) + hypot(bv.x, bv.y);
-      acc += s * s;
+    const cplx* ae = a + e * sa;
+    const cplx* be = b + e * sb;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (lda == n && ldb == n) {
+      int q = threadIdx.x;
+      for (; q + 3 * SRN_THREADS < nn; q += 4 * SRN_THREADS) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[u] += sr_norm_term(ae[q + u * SRN_THREADS], be[q + u * SRN_THREADS]);
+      }
+      for (; q < nn; q += SRN_THREADS) acc[0] += sr_norm_term(ae[q], be[q]);
+    } else {
+      for (int q = threadIdx.x; q < nn; q += SRN_THREADS) {
+        const int r = q / n, c = q % n;
+        acc[0] += sr_norm_term(ae[(int64_t)r * lda + c], be[(int64_t)r * ldb + c]);
+      }
     }
-    cplx s = block_sum(cmk(acc, 0));
+    cplx s = block_sum(cmk((acc[0] + acc[1]) + (acc[2] + acc[3]), 0));
     if (threadIdx.x == 0) {
       double delta = sqrt(s.x) / 2.0;
       if (iterations) iterations[e] += 1;
@@ -411,6 +476,15 @@ void launch_skew_combine(int n, int64_t batch, MatView s, MatView w, MutView out
 }
 
 void launch_sub_herm_inplace(int n, int64_t batch, MutView x, cudaStream_t stream) {
+  if (n <= 0 || batch <= 0) return;
+  if (n >= 64) {
+    const int nt = (n + 31) / 32;
+    const unsigned pairs = (unsigned)(nt * (nt + 1) / 2);
+    const unsigned gy = (unsigned)(batch < 65535 ? batch : 65535);
+    sub_herm_tiled_kernel<<<dim3(pairs, gy), 256, 0, stream>>>(n, batch, x.ptr, x.ld, x.stride);
+    qtx_check_launch("sub_herm_tiled_kernel");
+    return;
+  }
   sub_herm_kernel<<<grid_for(batch * (int64_t)n * (n + 1) / 2), TB, 0, stream>>>(n, batch, x.ptr, x.ld, x.stride);
   qtx_check_launch("sub_herm_kernel");
 }
@@ -473,8 +547,8 @@ void launch_trace_product_h(int rows, int cols, int64_t batch, MatView x, MatVie
 void launch_sr_norm_update(int n, int64_t batch, MatView alpha, MatView beta, double tol, int* active,
                            int* iterations, int* num_active, cudaStream_t stream) {
   unsigned g = (unsigned)(batch < 65535 ? batch : 65535);
-  sr_norm_kernel<<<g, TB, 0, stream>>>(n, batch, alpha.ptr, alpha.ld, alpha.stride, beta.ptr, beta.ld, beta.stride,
-                                       tol, active, iterations, num_active);
+  sr_norm_kernel<<<g, SRN_THREADS, 0, stream>>>(n, batch, alpha.ptr, alpha.ld, alpha.stride, beta.ptr, beta.ld,
+                                                beta.stride, tol, active, iterations, num_active);
   qtx_check_launch("sr_norm_kernel");
 }
 
@@ -631,19 +705,43 @@ __global__ void block_dos_kernel(int n, int64_t batch, const cplx* g, int64_t ld
     if (threadIdx.x == 0) out[e * out_stride + out_col] = -s.x / n;
   }
 }
-__global__ void layer_current_kernel(int n, int64_t batch, const cplx* xl, int64_t ldl, int64_t sl, const cplx* xr,
-                                     int64_t ldr, int64_t sr, const double* occ_l, const double* occ_r,
-                                     double sign_r, const cplx* h, cplx* out, int64_t out_stride, int out_col) {
+// One CTA of LC_THREADS per energy (one energy per SM at the usual batch):
+// contiguous blocks are read by linear index, four independent elements per
+// thread and step, so the reduction streams at HBM speed.
+constexpr int LC_THREADS = 1024;
+
+__device__ __forceinline__ cplx layer_current_term(double fl, double frs, cplx l, cplx r, cplx hv) {
+  const cplx y = keldysh_mix(fl, l, frs, r);
+  return csub(cmul(hv, cmk(-y.x, y.y)), cmul(y, cconj(hv)));
+}
+
+__global__ void __launch_bounds__(LC_THREADS)
+    layer_current_kernel(int n, int64_t batch, const cplx* xl, int64_t ldl, int64_t sl, const cplx* xr,
+                         int64_t ldr, int64_t sr, const double* occ_l, const double* occ_r, double sign_r,
+                         const cplx* h, cplx* out, int64_t out_stride, int out_col) {
+  const int nn = n * n;
   for (int64_t e = blockIdx.x; e < batch; e += gridDim.x) {
-    const double fl = occ_l[e], fr = occ_r[e];
-    cplx acc = cmk(0, 0);
-    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
-      const int r = q / n, c = q % n;
-      const cplx y = keldysh_mix(fl, xl[e * sl + (int64_t)r * ldl + c], sign_r * fr, xr[e * sr + (int64_t)r * ldr + c]);
-      const cplx hv = h[q];
-      acc = cadd(acc, csub(cmul(hv, cmk(-y.x, y.y)), cmul(y, cconj(hv))));
+    const double fl = occ_l[e], frs = sign_r * occ_r[e];
+    const cplx* le = xl + e * sl;
+    const cplx* re = xr + e * sr;
+    cplx acc[4] = {cmk(0, 0), cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+    if (ldl == n && ldr == n) {
+      int q = threadIdx.x;
+      for (; q + 3 * LC_THREADS < nn; q += 4 * LC_THREADS) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int qu = q + u * LC_THREADS;
+          acc[u] = cadd(acc[u], layer_current_term(fl, frs, le[qu], re[qu], h[qu]));
+        }
+      }
+      for (; q < nn; q += LC_THREADS) acc[0] = cadd(acc[0], layer_current_term(fl, frs, le[q], re[q], h[q]));
+    } else {
+      for (int q = threadIdx.x; q < nn; q += LC_THREADS) {
+        const int r = q / n, c = q % n;
+        acc[0] = cadd(acc[0], layer_current_term(fl, frs, le[(int64_t)r * ldl + c], re[(int64_t)r * ldr + c], h[q]));
+      }
     }
-    const cplx s = block_sum(acc);
+    const cplx s = block_sum(cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])));
     if (threadIdx.x == 0) out[e * out_stride + out_col] = s;
   }
 }
@@ -662,7 +760,7 @@ void launch_layer_current(int n, int64_t batch, MatView xl, MatView xr, const do
                           cudaStream_t stream) {
   if (!out) return;
   const unsigned grid = (unsigned)(batch < 65535 ? batch : 65535);
-  layer_current_kernel<<<grid, TB, 0, stream>>>(n, batch, xl.ptr, xl.ld, xl.stride, xr.ptr, xr.ld, xr.stride, occ_l,
-                                                occ_r, sign_r, coupling, out, out_stride, out_col);
+  layer_current_kernel<<<grid, LC_THREADS, 0, stream>>>(n, batch, xl.ptr, xl.ld, xl.stride, xr.ptr, xr.ld, xr.stride,
+                                                        occ_l, occ_r, sign_r, coupling, out, out_stride, out_col);
   qtx_check_launch("layer_current_kernel");
 }
