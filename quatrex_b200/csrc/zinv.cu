@@ -1016,21 +1016,26 @@ void launch_split_t(int n, int64_t batch, MatView a, MutView x, int* info, const
   launch_split_r<TPR, RPT, CPT, 0>(n, batch, a, x, info, active, stream);
 }
 
-// Batches below this many matrices take the split path (measured on B200:
-// the fused kernel keeps one matrix per SM, so a small batch leaves most SMs
-// idle during the updates).  QTX_INV_SPLIT_BELOW overrides it (0: never).
-int64_t split_below() {
-  static int64_t v = [] {
-    const char* env = getenv("QTX_INV_SPLIT_BELOW");
-    return env ? (int64_t)atoll(env) : (int64_t)100;
+// Batches below split_below(n) matrices take the split path (the fused
+// kernel keeps one matrix per SM, so a small batch leaves most SMs idle
+// during the updates).  Crossovers measured on B200 (kernel_bench inv, fused
+// vs split): b = 128 between 64 and 100 matrices, b = 256 at about 105
+// (1.61 vs 1.57 ms at 100, 1.63 vs 1.74 ms at 120), b = 512 between 100 and
+// 148 (12.7 vs 10.9 ms at 100, 13.0 vs 14.9 ms at 148).  QTX_INV_SPLIT_BELOW
+// sets one threshold for every size (0: never split).
+int64_t split_below(int n) {
+  static const int64_t env = [] {
+    const char* v = getenv("QTX_INV_SPLIT_BELOW");
+    return v ? (int64_t)atoll(v) : (int64_t)-1;
   }();
-  return v;
+  if (env >= 0) return env;
+  return n <= 128 ? 80 : (n <= 256 ? 110 : 124);
 }
 
 }  // namespace
 
 size_t zinv_workspace_bytes(int n, int64_t batch) {
-  if (n <= 64 || n > 512 || batch >= split_below()) return 0;
+  if (n <= 64 || n > 512 || batch >= split_below(n)) return 0;
   const size_t W = (size_t)inv_shape(n).w;
   return sizeof(cplx) * (size_t)batch * 3 * (size_t)n * W + sizeof(int) * (size_t)batch * 2 * n + 256;
 }
@@ -1044,7 +1049,7 @@ void launch_zinv(int n, int64_t batch, MatView a, MutView x, int* info, const in
   // every panel row / column must be owned by the elimination mapping
   const int rpt = (n + (THREADS / s.tpr) - 1) / (THREADS / s.tpr);
   const int cpt = (s.w + s.tpr - 1) / s.tpr;
-  if (may_allocate && n > 64 && batch < split_below()) {
+  if (may_allocate && n > 64 && batch < split_below(n)) {
     if (s.tpr == 1 && rpt == 1 && cpt <= 32) launch_split_t<1, 1, 32>(n, batch, a, x, info, active, stream);
     else if (s.tpr == 1 && rpt == 2 && cpt <= 16) launch_split_t<1, 2, 16>(n, batch, a, x, info, active, stream);
     else if (s.tpr == 2 && rpt == 1 && cpt <= 16) launch_split_t<2, 1, 16>(n, batch, a, x, info, active, stream);

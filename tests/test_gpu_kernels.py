@@ -95,16 +95,16 @@ def test_inverse_split_and_fused_paths_agree(n):
     """Small batches take the split path (one launch per panel elimination and
     one per rank-w update over the whole GPU), large batches the fused kernel
     (one CTA per matrix); both apply the same operations in the same order,
-    so the first entries of a 100-matrix batch equal a 5-matrix call bit for
+    so the first entries of a 130-matrix batch equal a 5-matrix call bit for
     bit, and both match LAPACK."""
     rng = np.random.default_rng(n + 7)
-    a = rng.standard_normal((100, n, n)) + 1j * rng.standard_normal((100, n, n))
+    a = rng.standard_normal((130, n, n)) + 1j * rng.standard_normal((130, n, n))
     a[:, np.arange(n), np.arange(n)] += np.sqrt(n)
     ta = torch.from_numpy(a).cuda()
     big, small = torch.empty_like(ta), torch.empty_like(ta[:5])
     lib = _lib.load()
     ctx = _lib.context(0)
-    _lib.check(lib.qtx_inv(ctx, n, 100, ta.data_ptr(), n * n, big.data_ptr(), n * n, 0), ctx, "inv")
+    _lib.check(lib.qtx_inv(ctx, n, 130, ta.data_ptr(), n * n, big.data_ptr(), n * n, 0), ctx, "inv")
     _lib.check(lib.qtx_inv(ctx, n, 5, ta.data_ptr(), n * n, small.data_ptr(), n * n, 0), ctx, "inv")
     assert torch.equal(small, big[:5])
     assert _rel(small, np.linalg.inv(a[:5])) < 1e-10
