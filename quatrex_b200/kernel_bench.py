@@ -222,9 +222,48 @@ def bench_rgfdist(b: int, nb: int, energies: int, partitions: list[int], repeats
     return res
 
 
+def bench_spectral(b: int, energies: int, rank: int, launches: int) -> dict:
+    """Spectral OBC (Beyn contour NEVP + mode filter + surface recursion) and
+    Sancho-Rubio on the same lead (cells coupled through ``rank`` boundary
+    orbitals, make_lead), device-resident inputs: wall time per call after a
+    warm-up call, and how far the two surface Green's functions agree."""
+    import time
+
+    from quatrex_b200.nevp import Beyn
+    from quatrex_b200.obc import SanchoRubio, Spectral
+    from quatrex_b200.workloads import make_lead
+
+    a_ii, a_ij, a_ji, _ = make_lead(b, rank, energies, seed=11)
+    dev = torch.cuda.current_device()
+    tii = torch.from_numpy(a_ii).cuda(dev)
+    tij = torch.from_numpy(np.ascontiguousarray(a_ij)).cuda(dev)
+    tji = torch.from_numpy(np.ascontiguousarray(a_ji)).cuda(dev)
+    m_0 = 4 * rank
+    spec = Spectral(Beyn(r_o=10.0, r_i=0.8, m_0=m_0, num_quad_points=20))
+    sr = SanchoRubio(max_iterations=200, convergence_tol=1e-12)
+
+    def timed(fn):
+        out = fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(launches):
+            out = fn()
+        torch.cuda.synchronize()
+        return out, (time.perf_counter() - t0) / launches
+
+    xs, t_spec = timed(lambda: spec(tii, tij, tji, "left"))
+    xr, t_sr = timed(lambda: sr(tii, tij, tji, "left"))
+    diff = torch.linalg.norm(xs - xr, dim=(-2, -1)) / torch.linalg.norm(xr, dim=(-2, -1))
+    return {"kernel": "spectral_vs_sancho_rubio", "b": b, "energies": energies, "coupling_rank": rank, "m_0": m_0,
+            "spectral_s": t_spec, "spectral_solves_per_s": energies / t_spec, "sancho_rubio_s": t_sr,
+            "sancho_rubio_solves_per_s": energies / t_sr, "median_rel_diff": float(diff.median()),
+            "sr_iterations_mean": float(np.mean(sr.last_iterations))}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="fixed-shape kernel timing")
-    ap.add_argument("kernel", choices=["gemm", "gemm_h", "inv", "sr", "fp64peak", "grouped", "rgfdist"])
+    ap.add_argument("kernel", choices=["gemm", "gemm_h", "inv", "sr", "fp64peak", "grouped", "rgfdist", "spectral"])
+    ap.add_argument("--rank", type=int, default=16, help="spectral: coupling rank of the lead")
     ap.add_argument("--nb", type=int, default=64)
     ap.add_argument("--energies", type=int, default=4)
     ap.add_argument("--partitions", type=str, default="2,4,8")
@@ -245,6 +284,8 @@ def main(argv=None) -> int:
         r = bench_inv(args.b, args.batch, args.launches)
     elif args.kernel == "grouped":
         r = bench_grouped(args.b, args.instances)
+    elif args.kernel == "spectral":
+        r = bench_spectral(args.b, args.energies, args.rank, args.launches)
     elif args.kernel == "rgfdist":
         r = bench_rgfdist(args.b, args.nb, args.energies, [int(x) for x in args.partitions.split(",")])
     else:

@@ -6,17 +6,27 @@ drawn at construction, real parts then imaginary parts per call,
 ``beyn.py:96,310-313``), the same quadrature and the same SVD (or QR)
 projection.  The contour integral -- one n x n inverse per quadrature point
 and energy, the bulk of the work -- and the moment products run in
-``qtx_beyn_moments`` (DMMA GEMM and batched inverse); the projection onto the
-subspace and the small m0 x m0 eigenproblem use the dense SVD / QR / eig of
-``torch.linalg`` on the device (cuSOLVER), in place of upstream's LAPACK
-calls (``eig_compute_location`` / ``project_compute_location``).
+``qtx_beyn_moments`` (DMMA GEMM and batched inverse), the products of the
+projection on the device.  The two small dense factorisations follow
+upstream's ``project_compute_location`` / ``eig_compute_location``: with
+upstream's default ``"numpy"`` the n x m0 SVD (or QR) and the m0 x m0
+eigenproblem run in NumPy/LAPACK on the host, as upstream does
+(``beyn.py:120-125, 265-272``), split over host threads; any other value runs
+them through ``torch.linalg`` on the device.  Measured on B200 for 148
+energies (b = 256, m0 = 64): ``torch.linalg.svd`` 1.38 s and
+``torch.linalg.eig`` 0.49 s on the device (batched small factorisations are
+not what those routines are built for; the latter's hybrid path iterates on
+the host anyway) against the 69 ms contour; the whole Spectral call takes
+0.20 s with the host factorisations and 1.97 s with the device ones.
 """
 
 from __future__ import annotations
 
 import ctypes
 import math
+import os
 from abc import ABC, abstractmethod
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
@@ -47,12 +57,42 @@ def _batched(t: torch.Tensor) -> tuple[int, int]:
     return int(math.prod(t.shape[:-2])), n * n
 
 
+def _host_batched(fn, x: np.ndarray, nout: int):
+    """fn over the leading (batch) axis of x in chunks on host threads (the
+    NumPy linear-algebra loops release the GIL), each chunk with a
+    single-threaded BLAS so the threads do not oversubscribe the cores; nout
+    stacked results."""
+    batch = x.shape[0]
+    workers = max(1, min(batch, os.cpu_count() or 1, 16))
+    if workers == 1:
+        return fn(x)
+    bounds = np.linspace(0, batch, workers + 1).astype(int)
+    try:
+        from threadpoolctl import threadpool_limits
+        limit = threadpool_limits(limits=1)
+    except ImportError:
+        limit = None
+    try:
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            parts = list(ex.map(lambda q: fn(x[bounds[q]:bounds[q + 1]]), range(workers)))
+    finally:
+        if limit is not None:
+            limit.restore_original_limits()
+    return tuple(np.concatenate([p[k] for p in parts]) for k in range(nout))
+
+
+def _on_host(location: str) -> bool:
+    return location == "numpy"
+
+
 class Beyn(NEVP):
     """Beyn's contour-integral method for the eigenpairs inside the annulus
-    r_i < |w| < r_o (``beyn.py:14-95``).  ``num_threads_contour``,
-    ``eig_compute_location``, ``project_compute_location``,
-    ``contour_batch_size`` and ``use_pinned_memory`` are accepted for
-    signature compatibility; the device path sizes its own passes."""
+    r_i < |w| < r_o (``beyn.py:14-95``).  ``eig_compute_location`` and
+    ``project_compute_location`` choose where the small factorisations run
+    ("numpy": the host, as upstream's default; otherwise the device);
+    ``num_threads_contour``, ``contour_batch_size`` and ``use_pinned_memory``
+    are accepted for signature compatibility (the device path sizes its own
+    passes)."""
 
     def __init__(self, r_o: float, r_i: float, m_0: int, num_quad_points: int, num_threads_contour: int = 1024,
                  eig_compute_location: str = "numpy", project_compute_location: str = "numpy", use_qr: bool = False,
@@ -93,11 +133,20 @@ class Beyn(NEVP):
         dropped rows and columns are zero, so the padded problem's extra
         eigenvalues are exactly 0 and never chosen as lead modes."""
         m0 = p0.shape[-1]
+        host = _on_host(self.project_compute_location)
         if self.use_qr:
-            q, r = torch.linalg.qr(p0)
+            if host:
+                q, r = _host_batched(lambda x: np.linalg.qr(x), p0.cpu().numpy(), 2)
+                q, r = torch.from_numpy(q).to(p0.device), torch.from_numpy(r).to(p0.device)
+            else:
+                q, r = torch.linalg.qr(p0)
             a = q.mH @ p1 @ torch.linalg.inv(r)
             return a, q
-        u, s, vh = torch.linalg.svd(p0, full_matrices=False)
+        if host:
+            u, s, vh = _host_batched(lambda x: np.linalg.svd(x, full_matrices=False), p0.cpu().numpy(), 3)
+            u, s, vh = (torch.from_numpy(t).to(p0.device) for t in (u, s, vh))
+        else:
+            u, s, vh = torch.linalg.svd(p0, full_matrices=False)
         keep = s > s.amax(dim=-1, keepdim=True) * m0 * torch.finfo(torch.float64).eps
         s_safe = torch.where(keep, s, torch.ones_like(s))
         a = (u.mH @ p1 @ vh.mH) / s_safe[..., None, :].to(p1.dtype)
@@ -126,6 +175,10 @@ class Beyn(NEVP):
         y = torch.from_numpy(y_h).to(f"cuda:{dev}")
         p0, p1 = self.moments(a_ji, a_ii, a_ij, y)
         a, back = self._project(p0, p1)
-        w, v = torch.linalg.eig(a)
+        if _on_host(self.eig_compute_location):
+            w, v = _host_batched(lambda x: np.linalg.eig(x), a.cpu().numpy(), 2)
+            w, v = torch.from_numpy(w).to(a.device), torch.from_numpy(v).to(a.device)
+        else:
+            w, v = torch.linalg.eig(a)
         vs = back @ v
         return w.reshape(batch_shape + (self.m_0,)), vs.reshape(batch_shape + (n, self.m_0))

@@ -46,8 +46,9 @@ def _oracle_and_spread(a_ii, a_ij, a_ji, m_0, trials=2):
     return x, info, spread
 
 
+@pytest.mark.parametrize("location", ["numpy", "cupy"])
 @pytest.mark.parametrize("case", ["fixture_b16", "b64_rank8"])
-def test_spectral_matches_oracle(case):
+def test_spectral_matches_oracle(case, location):
     if case == "fixture_b16":
         g = np.load(os.path.join(GOLDEN, "spectral_small.npz"))
         a_ii, a_ij, a_ji, m_0 = g["a_ii"], g["a_ij"], g["a_ji"], int(g["m_0"])
@@ -55,7 +56,10 @@ def test_spectral_matches_oracle(case):
         a_ii, a_ij, a_ji, _ = make_lead(64, 8, 6, seed=9)
         m_0 = 32
     x_ref, info, spread = _oracle_and_spread(a_ii, a_ij, a_ji, m_0)
-    spec = Spectral(Beyn(r_o=10.0, r_i=0.8, m_0=m_0, num_quad_points=20))
+    # "numpy" (upstream's default): the small SVD and eig on the host;
+    # "cupy": both on the device through torch.linalg
+    spec = Spectral(Beyn(r_o=10.0, r_i=0.8, m_0=m_0, num_quad_points=20, eig_compute_location=location,
+                         project_compute_location=location))
     x = spec(a_ii, a_ij, a_ji, "left")
     assert isinstance(x, np.ndarray) and x.shape == a_ii.shape
     err = _rel(x, x_ref)
