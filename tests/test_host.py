@@ -248,3 +248,20 @@ def test_symmetric_storage_completion(kind):
         assert np.allclose(x.to_dense()[1], m)
         assert np.allclose(x.blocks[2, 1], m[7:10, 3:7])
         assert np.allclose(x.blocks[1, 1], m[3:7, 3:7])
+
+
+def test_host_batched_factorisations_equal_numpy():
+    """The Spectral OBC's small SVD / eig on host threads (upstream's default
+    compute location) split the batch over threads with single-threaded BLAS
+    and return exactly what one NumPy call returns."""
+    from quatrex_b200.nevp import _host_batched
+
+    rng = np.random.default_rng(3)
+    p0 = rng.standard_normal((37, 24, 8)) + 1j * rng.standard_normal((37, 24, 8))
+    u, s, vh = _host_batched(lambda x: np.linalg.svd(x, full_matrices=False), p0, 3)
+    u1, s1, vh1 = np.linalg.svd(p0, full_matrices=False)
+    assert np.allclose(s, s1, rtol=1e-14, atol=0)
+    assert np.allclose(u @ (s[..., None] * vh), p0, rtol=0, atol=1e-12)
+    a = rng.standard_normal((37, 8, 8)) + 1j * rng.standard_normal((37, 8, 8))
+    w, v = _host_batched(lambda x: np.linalg.eig(x), a, 2)
+    assert np.allclose(a @ v, v * w[..., None, :], atol=1e-11)
