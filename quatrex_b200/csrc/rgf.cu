@@ -1548,7 +1548,7 @@ void stream_host_batches(qtx_ctx* ctx, std::vector<HostArr>& arrs, int64_t NE, i
     QTX_CUDA_TRY(cudaEventRecord(solved, s));
     QTX_CUDA_TRY(cudaStreamWaitEvent(cs, solved, 0));
     if (use_ring) {
-      RingCopier rc{*ctx->ring, cs};
+      RingCopier rc{*ctx->ring, cs, 0, {}};
       CopyWorker w;
       auto upload = [&](int64_t e0, int64_t ne, int set) {
         return w.post([&, e0, ne, set] {

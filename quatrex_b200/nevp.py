@@ -22,7 +22,6 @@ the host anyway) against the 69 ms contour; the whole Spectral call takes
 
 from __future__ import annotations
 
-import ctypes
 import math
 import os
 from abc import ABC, abstractmethod

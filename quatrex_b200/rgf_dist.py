@@ -33,7 +33,6 @@ both cases.
 
 from __future__ import annotations
 
-import ctypes
 import math
 
 import numpy as np

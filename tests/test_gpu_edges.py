@@ -2,7 +2,6 @@
 are no-ops, a block size beyond the inverse's limit is refused with a status
 (the context stays usable), the smallest devices solve."""
 
-import ctypes
 
 import numpy as np
 import pytest

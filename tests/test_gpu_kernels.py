@@ -3,7 +3,6 @@ complex128 matmul, the batched inverse against NumPy/LAPACK, Sancho-Rubio
 against the oracle.  Tolerances: relative Frobenius error 1e-12 for a single
 GEMM, 1e-10 for inverses of well-conditioned blocks."""
 
-import ctypes
 
 import numpy as np
 import pytest
