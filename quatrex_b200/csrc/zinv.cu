@@ -541,6 +541,65 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         cp_async_commit();
       };
+      const int ntiles = row_tiles * col_tiles;
+      // Accumulator start values of a tile: output position i starts from
+      // X[sigma(i)].  Rows with sigma(i) == i load straight from X under one
+      // predicate each (no branch between global and shared memory), so the
+      // 32 loads of a thread are in flight together; the few rows displaced
+      // by a pivot swap are then patched from the staged rows D.
+      auto load_own = [&](int tile, int c0, double (&are)[2][4][4], double (&aim)[2][4][4]) {
+        const int row0 = (tile / col_tiles) * 32, col0 = (tile % col_tiles) * 32;
+        bool own[2][2];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int i = row0 + mi * 16 + g + 8 * h;
+            own[mi][h] = i < n && !(i >= k0 && i < k0 + w) && pos2row[i] == i;
+          }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int i = row0 + mi * 16 + g + ((q >> 1) << 3);
+              const int c = c0 + col0 + ni * 8 + 2 * t + (q & 1);
+              are[mi][ni][q] = 0.0;
+              aim[mi][ni][q] = 0.0;
+              if (own[mi][q >> 1] && c < n) {
+                const cplx y = X[(int64_t)i * ldx + c];
+                are[mi][ni][q] = y.x;
+                aim[mi][ni][q] = y.y;
+              }
+            }
+      };
+      auto patch_displaced = [&](int tile, int c0, const cplx* D, double (&are)[2][4][4],
+                                 double (&aim)[2][4][4]) {
+        const int row0 = (tile / col_tiles) * 32, col0 = (tile % col_tiles) * 32;
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int i = row0 + mi * 16 + g + 8 * h;
+            if (i < n && !(i >= k0 && i < k0 + w)) {
+              const int src = pos2row[i];
+              if (src != i) {
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                  for (int q2 = 0; q2 < 2; ++q2) {
+                    const int cc = col0 + ni * 8 + 2 * t + q2;
+                    if (c0 + cc < n) {
+                      const cplx y = D[(src - k0) * LDR + cc];
+                      are[mi][ni][2 * h + q2] = y.x;
+                      aim[mi][ni][2 * h + q2] = y.y;
+                    }
+                  }
+              }
+            }
+          }
+      };
       int slab = next_slab(0);
       int buf = 0;
       if (slab < nslab) stage(slab, 0);
@@ -555,27 +614,12 @@ __global__ void __launch_bounds__(THREADS, 1)
         __syncthreads();
         cplx* R = Rs + (size_t)buf * 2 * W * LDR;  // pivot rows p_j      (w x CW)
         cplx* D = R + (size_t)W * LDR;             // rows k0 + j         (w x CW)
-        for (int tile = warp; tile < row_tiles * col_tiles; tile += NWARPS) {
+        for (int tile = warp; tile < ntiles; tile += NWARPS) {
           const int rt = tile / col_tiles, ct = tile % col_tiles;
           const int row0 = rt * 32, col0 = ct * 32;
           double acc_re[2][4][4], acc_im[2][4][4];
-#pragma unroll
-          for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                int i = row0 + mi * 16 + g + ((q >> 1) << 3);
-                int cc = col0 + ni * 8 + 2 * t + (q & 1);
-                int c = c0 + cc;
-                cplx y = cmk(0, 0);
-                if (i < n && c < n && !(i >= k0 && i < k0 + w)) {
-                  int src = pos2row[i];
-                  y = (src == i) ? X[(int64_t)i * ldx + c] : D[(src - k0) * LDR + cc];
-                }
-                acc_re[mi][ni][q] = y.x;
-                acc_im[mi][ni][q] = y.y;
-              }
+          load_own(tile, c0, acc_re, acc_im);
+          patch_displaced(tile, c0, D, acc_re, acc_im);
           int prow_idx[2][2];
 #pragma unroll
           for (int mi = 0; mi < 2; ++mi) {
@@ -806,33 +850,63 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2)
       cp_async16(&D[j * SPLIT_LDR + cc], ok ? &de[(int64_t)j * n + c0 + cc] : de, ok);
     }
     cp_async_commit();
-    cp_async_wait<0>();
-    __syncthreads();
     // one 32 x 32 tile per warp: rows r0 + 32 warp .., columns c0 ..
+    // Output position i starts from row sigma(i): itself, or a row of
+    // [k0, k0 + w) displaced by a pivot swap; positions inside the panel start
+    // from zero.  The rows that start from themselves load while the staged
+    // copies are in flight (only this CTA writes these positions of X); the
+    // displaced rows are patched from the staged D after the barrier.
     const int lrow0 = warp * 32;
-    if (r0 + lrow0 < n) {
-      double acc_re[2][4][4], acc_im[2][4][4];
+    const bool has_tile = r0 + lrow0 < n;
+    double acc_re[2][4][4], acc_im[2][4][4];
+    int src_of[2][2];  // sigma(i), or -1 where position i starts from zero
+    if (has_tile) {
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
         for (int hq = 0; hq < 2; ++hq) {
           const int li = lrow0 + mi * 16 + g + hq * 8;
           const int i = r0 + li;
-          // output position i starts from row sigma(i): itself, or a row of
-          // [k0, k0 + w) displaced by a pivot swap; positions inside the
-          // panel start from zero
           const bool rv = i < n && !(i >= k0 && i < k0 + w);
-          const int src = rv ? srow[li] : 0;
+          const int src = rv ? srow[li] : -1;
+          src_of[mi][hq] = src;
 #pragma unroll
           for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
             for (int ql = 0; ql < 2; ++ql) {
               const int cc = ni * 8 + 2 * t + ql;
-              cplx y = cmk(0, 0);
-              if (rv && c0 + cc < n) y = (src == i) ? X[(int64_t)i * ldx + c0 + cc] : D[(src - k0) * SPLIT_LDR + cc];
-              acc_re[mi][ni][hq * 2 + ql] = y.x;
-              acc_im[mi][ni][hq * 2 + ql] = y.y;
+              acc_re[mi][ni][hq * 2 + ql] = 0.0;
+              acc_im[mi][ni][hq * 2 + ql] = 0.0;
+              if (src == i && c0 + cc < n) {
+                const cplx y = X[(int64_t)i * ldx + c0 + cc];
+                acc_re[mi][ni][hq * 2 + ql] = y.x;
+                acc_im[mi][ni][hq * 2 + ql] = y.y;
+              }
             }
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    if (has_tile) {
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int hq = 0; hq < 2; ++hq) {
+          const int i = r0 + lrow0 + mi * 16 + g + hq * 8;
+          const int src = src_of[mi][hq];
+          if (src >= 0 && src != i) {
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+              for (int ql = 0; ql < 2; ++ql) {
+                const int cc = ni * 8 + 2 * t + ql;
+                if (c0 + cc < n) {
+                  const cplx y = D[(src - k0) * SPLIT_LDR + cc];
+                  acc_re[mi][ni][hq * 2 + ql] = y.x;
+                  acc_im[mi][ni][hq * 2 + ql] = y.y;
+                }
+              }
+          }
         }
       for (int kk = 0; kk < w; kk += 4) {
         const int kc = kk + t;
