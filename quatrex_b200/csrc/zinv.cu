@@ -87,6 +87,24 @@ __device__ __forceinline__ int pidx(int r, int c, int wp) {
   return r * wp + (c ^ sw);
 }
 
+// Two adjacent complex elements in one 32-byte access.  The caller guarantees
+// 32-byte alignment: pair_access_ok() for the matrix and an even column.
+__device__ __forceinline__ void ld_pair(const cplx* p, cplx& a, cplx& b) {
+  asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];\n"
+               : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+               : "l"(p));
+}
+__device__ __forceinline__ void st_pair(cplx* p, cplx a, cplx b) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};\n" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
+               : "memory");
+}
+// Element (i, c) of X with c even starts on a 32-byte boundary, and the pair
+// (c, c + 1) lies on one side of every even column boundary (n, panel edges
+// k0 and k0 + w, which are even when n is).
+__device__ __forceinline__ bool pair_access_ok(const cplx* X, int64_t ldx, int n) {
+  return (reinterpret_cast<uintptr_t>(X) & 31) == 0 && (ldx & 1) == 0 && (n & 1) == 0;
+}
+
 __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
   asm volatile(
       "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
@@ -831,6 +849,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2)
   for (int64_t e = blockIdx.y; e < batch; e += gridDim.y) {
     if (active && !active[e]) continue;
     cplx* X = x_base + e * sx;
+    const bool pairs = pair_access_ok(X, ldx, n);
     const int* sig = sc.sigma + e * n;
     const cplx* pe = sc.p + e * (int64_t)n * W;
     const cplx* re = sc.r + e * (int64_t)W * n;
@@ -871,18 +890,23 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2)
           const int src = rv ? srow[li] : -1;
           src_of[mi][hq] = src;
 #pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int ql = 0; ql < 2; ++ql) {
-              const int cc = ni * 8 + 2 * t + ql;
-              acc_re[mi][ni][hq * 2 + ql] = 0.0;
-              acc_im[mi][ni][hq * 2 + ql] = 0.0;
-              if (src == i && c0 + cc < n) {
-                const cplx y = X[(int64_t)i * ldx + c0 + cc];
-                acc_re[mi][ni][hq * 2 + ql] = y.x;
-                acc_im[mi][ni][hq * 2 + ql] = y.y;
+          for (int ni = 0; ni < 4; ++ni) {
+            const int c = c0 + ni * 8 + 2 * t;  // even
+            cplx y0 = cmk(0, 0), y1 = cmk(0, 0);
+            if (src == i) {
+              const cplx* p = X + (int64_t)i * ldx + c;
+              if (pairs) {
+                if (c < n) ld_pair(p, y0, y1);
+              } else {
+                if (c < n) y0 = p[0];
+                if (c + 1 < n) y1 = p[1];
               }
             }
+            acc_re[mi][ni][hq * 2] = y0.x;
+            acc_im[mi][ni][hq * 2] = y0.y;
+            acc_re[mi][ni][hq * 2 + 1] = y1.x;
+            acc_im[mi][ni][hq * 2 + 1] = y1.y;
+          }
         }
     }
     cp_async_wait<0>();
@@ -940,13 +964,18 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2)
           const int i = r0 + lrow0 + mi * 16 + g + hq * 8;
           if (i >= n) continue;
 #pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int ql = 0; ql < 2; ++ql) {
-              const int c = c0 + ni * 8 + 2 * t + ql;
-              if (c < n && !(c >= k0 && c < k0 + w))
-                X[(int64_t)i * ldx + c] = cmk(acc_re[mi][ni][hq * 2 + ql], acc_im[mi][ni][hq * 2 + ql]);
+          for (int ni = 0; ni < 4; ++ni) {
+            const int c = c0 + ni * 8 + 2 * t;  // even
+            const cplx v0 = cmk(acc_re[mi][ni][hq * 2], acc_im[mi][ni][hq * 2]);
+            const cplx v1 = cmk(acc_re[mi][ni][hq * 2 + 1], acc_im[mi][ni][hq * 2 + 1]);
+            cplx* p = X + (int64_t)i * ldx + c;
+            if (pairs) {
+              if (c < n && !(c >= k0 && c < k0 + w)) st_pair(p, v0, v1);
+            } else {
+              if (c < n && !(c >= k0 && c < k0 + w)) p[0] = v0;
+              if (c + 1 < n && !(c + 1 >= k0 && c + 1 < k0 + w)) p[1] = v1;
             }
+          }
         }
     }
     __syncthreads();
