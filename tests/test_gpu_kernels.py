@@ -109,6 +109,29 @@ def test_inverse_split_and_fused_paths_agree(n):
     assert _rel(small, np.linalg.inv(a[:5])) < 1e-10
 
 
+@pytest.mark.parametrize("n", [200, 256])
+@pytest.mark.parametrize("batch", [5, 130], ids=["split", "fused"])
+def test_inverse_output_sixteen_bytes_off(n, batch):
+    """The split path reads and writes adjacent column pairs in one 32-byte
+    access only when the matrices start 32-byte aligned; an output batch that
+    starts one complex element (16 bytes) into its buffer takes the 16-byte
+    accesses and returns the same bits as an aligned one."""
+    rng = np.random.default_rng(n + batch)
+    a = rng.standard_normal((batch, n, n)) + 1j * rng.standard_normal((batch, n, n))
+    a[:, np.arange(n), np.arange(n)] += np.sqrt(n)
+    ta = torch.from_numpy(a).cuda()
+    aligned = torch.empty_like(ta)
+    buf = torch.empty(batch * n * n + 1, dtype=torch.complex128, device="cuda")
+    off = buf[1:].view(batch, n, n)
+    assert off.data_ptr() % 32 == 16
+    lib = _lib.load()
+    ctx = _lib.context(0)
+    _lib.check(lib.qtx_inv(ctx, n, batch, ta.data_ptr(), n * n, aligned.data_ptr(), n * n, 0), ctx, "inv")
+    _lib.check(lib.qtx_inv(ctx, n, batch, ta.data_ptr(), n * n, off.data_ptr(), n * n, 0), ctx, "inv")
+    assert torch.equal(off, aligned)
+    assert _rel(aligned[:3], np.linalg.inv(a[:3])) < 1e-10
+
+
 def test_inverse_needs_pivoting():
     # zero leading diagonal entries: fails without row interchanges
     a = np.array([[0, 1, 2], [1, 0, 3], [4, 5, 0]], dtype=np.complex128)[None]
