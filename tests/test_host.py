@@ -265,3 +265,24 @@ def test_host_batched_factorisations_equal_numpy():
     a = rng.standard_normal((37, 8, 8)) + 1j * rng.standard_normal((37, 8, 8))
     w, v = _host_batched(lambda x: np.linalg.eig(x), a, 2)
     assert np.allclose(a @ v, v * w[..., None, :], atol=1e-11)
+
+
+def test_autotuner_cache_and_keys(tmp_path):
+    """Autotuner keys bucket the batch to a power of two; a cached choice is
+    returned without measuring anything (no device needed), and the table
+    survives a save/load round trip."""
+    from quatrex_b200.autotune import Autotuner
+
+    assert Autotuner.key(256, 100, "fp64") == "b256-n128-fp64"
+    assert Autotuner.key(64, 148, "mixed") == "b64-n256-mixed"
+    assert Autotuner.key(32, 1, "fp64") == "b32-n1-fp64"
+    path = tmp_path / "sub" / "autotune.json"
+    t = Autotuner(cache_path=str(path))
+    choice = {"energies_per_call": 148, "gemm_path": "fp64", "graph": False, "probe_solves_per_s": 1.0}
+    t.table[Autotuner.key(256, 148, "fp64")] = choice
+    t.save()
+    assert path.exists() and not (tmp_path / "sub" / "autotune.json.tmp").exists()
+    t2 = Autotuner(cache_path=str(path))
+    # 130 .. 256 energies share the bucket of 148
+    assert t2.best(256, 200, "fp64") == choice
+    assert t2.lookup(256, 100, "fp64") is None
