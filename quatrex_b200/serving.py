@@ -85,13 +85,9 @@ class TransportServer:
             return fut
         energies = np.asarray(energies, dtype=np.float64)
         choice = self.tuner.best(device.block_size, len(energies), self.precision)
-        ne_call = min(int(choice["energies_per_call"]), len(energies))
         path = choice.get("gemm_path", self.precision)
-        # the tuned call size is chosen on a short probe device: a long device
-        # takes smaller calls, so that one call's work space fits the budget
-        while ne_call > 1 and self._lib.qtx_transport_footprint(device.num_blocks, device.block_size, ne_call,
-                                                                _PRECISIONS[path]) > self.budget:
-            ne_call = max(1, ne_call // 2)
+        ne_call = call_size(self._lib, device.num_blocks, device.block_size, len(energies),
+                            int(choice["energies_per_call"]), path, self.budget)
         dev = f"cuda:{self.cuda}"
         nb, b, ne = device.num_blocks, device.block_size, len(energies)
         with torch.cuda.stream(self._copy_stream):
@@ -163,6 +159,19 @@ class TransportServer:
             res = {k: v.cpu().numpy() for k, v in out.items()}
             res["latency_s"] = lat.value
             fut.set_result(res)
+
+
+def call_size(lib, num_blocks: int, block_size: int, num_energies: int, tuned: int, path: str,
+              budget: int) -> int:
+    """Energies per device call of one request: the tuned size (chosen on a
+    short probe device), at most the request's energies, halved until one
+    call's work space (``qtx_transport_footprint``) fits the budget, never
+    below one; a request that does not fit even then is refused at
+    submission by the native server."""
+    ne_call = max(1, min(int(tuned), int(num_energies)))
+    while ne_call > 1 and lib.qtx_transport_footprint(num_blocks, block_size, ne_call, _PRECISIONS[path]) > budget:
+        ne_call = max(1, ne_call // 2)
+    return ne_call
 
 
 def poisson_arrivals(count: int, rate_hz: float, seed: int = 0) -> np.ndarray:

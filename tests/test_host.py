@@ -123,6 +123,24 @@ def test_transport_footprint_is_host_arithmetic():
     assert lib.qtx_transport_footprint(1, 64, 8, _lib.QTX_PREC_FP64) == 0
 
 
+def test_serving_call_size_fits_the_budget():
+    """A request's energies per call: the tuned size capped by the request's
+    energies, halved until one call's footprint fits the server budget; one
+    energy per call is the floor (the native server refuses the rest)."""
+    from quatrex_b200.serving import call_size
+
+    lib = _lib.load()
+    fp = lambda ne, prec="fp64": lib.qtx_transport_footprint(64, 256, ne, _lib.QTX_PREC_FP64 if prec == "fp64"
+                                                             else _lib.QTX_PREC_MIXED)
+    assert call_size(lib, 64, 256, 1024, 148, "fp64", 10 ** 15) == 148
+    assert call_size(lib, 64, 256, 20, 148, "fp64", 10 ** 15) == 20
+    budget = fp(40)
+    got = call_size(lib, 64, 256, 1024, 148, "fp64", budget)
+    assert got == 37 and fp(got) <= budget < fp(2 * got)  # 148 -> 74 -> 37
+    assert call_size(lib, 64, 256, 1024, 148, "mixed", fp(37)) <= 37
+    assert call_size(lib, 64, 256, 1024, 148, "fp64", 1) == 1
+
+
 def test_grouped_footprint_is_host_arithmetic():
     """Work space of a grouped launch: one (3 nb_max + 20)-block work space per
     resident CTA (never more CTAs than pairs), plus descriptors; block sizes
