@@ -8,10 +8,12 @@
 //
 // Algorithm for an n x n matrix X (a copy of A), panel width w:
 //   for each panel of columns [k0, k0 + w):
-//     1. stage the n x w panel in shared memory (rows in the current order of
-//        X) and eliminate it column by column without moving rows: pick the
-//        pivot row among the rows not yet used, eliminate the column from all
-//        other rows, scale the pivot row (two barriers per column);
+//     1. stage the n x w panel (rows in the current order of X) into the
+//        threads' registers through shared memory and eliminate it column by
+//        column without moving rows: pick the pivot row among the rows not
+//        yet used, eliminate the column from all other rows, scale the pivot
+//        row (one barrier per column: every warp publishes its candidate row
+//        before it);
 //     2. turn the pivot sequence into the row permutation sigma that the
 //        classic row-swapping Gauss-Jordan would apply (position k0 + j takes
 //        pivot row p_j, the displaced row goes to p_j's position), and record
@@ -20,7 +22,9 @@
 //        rank-w update on DMMA (mma.sync m16n8k4 f64) tiles:
 //          X[i, c] <- [i not in panel] X[sigma(i), c]
 //                     + sum_j P[sigma(i), j] X[p_j, c]
-//        in column slabs of CW, the k0 + j pivot rows staged in shared memory;
+//        in column slabs of CW, the k0 + j pivot rows staged in shared memory
+//        (for small batches the updates of one panel run as a separate launch
+//        spread over the GPU, the split path below);
 //   finally undo the row interchanges as column interchanges in reverse order.
 // The matrix itself stays in global memory (L2 resident for a wave of
 // matrices); shared memory holds the panel (n x Wp, XOR-swizzled so that both
